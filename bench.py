@@ -1,0 +1,427 @@
+"""Benchmark of the batched orientation search (CC evaluations per second).
+
+Workload (one step): the 64^3 share of the batched uneven-alignment configuration --
+1,200 synthetic 64^3 subtomograms, each searched over 256 local orientations within 8
+degrees of its own seeded prior, peak radius 7, in one emc_search_run call (one CUDA graph).
+307,200 CC evaluations per step per GPU.  The single-subtomogram plain search (one particle,
+540 orientations on the 10 degree grid) is timed beside it and reported under "plain".
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--particles P]
+
+Under torchrun every rank runs its own full batch (weak scaling, no collective on the
+data path); the step time is the max over ranks.  `--impl reference` times the
+single-precision CPU port of the reference path (oracle/liboracle_f32.so) on all host
+cores over a bounded sample of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BOX = 64
+N_ORIENT = 256
+PEAK_RADIUS = 7
+
+
+def bytes_per_eval(n):
+    """Algorithmic bytes of one CC evaluation: rotated source (4 n^3) + particle spectrum
+    (8 nh n^2) + wedge.CTF weight (4 nh n^2) + 16 B result."""
+    nh = n // 2 + 1
+    return 4 * n ** 3 + 8 * nh * n * n + 4 * nh * n * n + 16
+
+
+def flops_per_eval(n):
+    return 2 * 2.5 * n ** 3 * math.log2(n ** 3) + 30 * n ** 3 + 8 * (n // 2 + 1) * n * n
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+def build_batch(seed, n_particles):
+    """Host (pinned) particle volumes and weights plus search descriptors for one rank."""
+    import torch
+
+    from emclarity_b200 import api, synthetic
+    rng = np.random.default_rng(seed)
+    ref = synthetic.blob_reference(rng, BOX)
+    mask = synthetic.soft_sphere_mask(BOX, 28)
+    grid = synthetic.local_grid(N_ORIENT, 8.0, 2.0)
+    ref_g = torch.from_numpy(ref).cuda()
+    parts = torch.empty((n_particles, BOX, BOX, BOX), dtype=torch.float32).pin_memory()
+    weights = torch.empty((n_particles, BOX, BOX, BOX // 2 + 1), dtype=torch.float32).pin_memory()
+    priors = []
+    ft = api.FourierTransformer((BOX, BOX, BOX))
+    for i in range(n_particles):
+        prior = api.define_matrix(synthetic.random_euler(rng), "inv")
+        jitter = api.define_matrix([rng.uniform(-6, 6), rng.uniform(0, 6), rng.uniform(-6, 6)], "inv")
+        truth = prior @ jitter
+        shift = rng.integers(-4, 5, 3)
+        w = api.wedge_ctf_weight(BOX, -rng.uniform(50, 65), rng.uniform(50, 65),
+                                 synthetic.ctf_dict(rng.uniform(15000, 40000)))
+        p = synthetic.make_particle(ref_g, rng, truth, shift, w, 0.1, ft=ft)
+        parts[i].copy_(p)
+        weights[i].copy_(w)
+        priors.append(prior)
+    return dict(ref=ref_g, mask=torch.from_numpy(mask).cuda(), grid=grid, parts=parts, weights=weights,
+                priors=priors, ref_np=ref, mask_np=mask)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from emclarity_b200 import api
+    n = args.particles
+    b = build_batch(1000 + rank, n)
+    s = api.Search(peak_radius=PEAK_RADIUS)
+    rid = s.add_reference(b["ref"], b["mask"])
+    s.set_orientations(b["grid"])
+    d_parts = b["parts"].cuda()
+    d_w = b["weights"].cuda()
+    spec = torch.empty((n, BOX, BOX, BOX // 2 + 1), dtype=torch.complex64, device="cuda")
+    energy = torch.zeros(n, dtype=torch.float64, device="cuda")
+    for i in range(n):
+        L_call_spectrum(api, d_parts[i], d_w[i], spec[i], energy[i:i + 1])
+    torch.cuda.synchronize()
+    en = energy.cpu().numpy()
+    descs = [s.particle(spec[i], en[i], rid, prior=b["priors"][i], orient_count=N_ORIENT) for i in range(n)]
+    evals = n * N_ORIENT
+    cc = torch.empty(evals, device="cuda")
+    best = torch.empty((n, 5), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        s.run(descs, cc=cc, best=best)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # ---------------- timed region: device-resident inputs, graph replay
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    ms_local = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms_local, world)
+    launches_per_step = s.timings()["launches_last_run"]
+
+    # ---------------- per-pass device times (eager launches bracketed by CUDA events)
+    s.set_profiling(True)
+    s.timings(reset=True)
+    torch.cuda.synchronize()
+    for _ in range(max(1, min(args.steps, 3))):
+        step()
+    torch.cuda.synchronize()
+    prof = s.timings(reset=True)
+    s.set_profiling(False)
+
+    # ---------------- end to end: pinned host volumes -> spectra -> search -> host results
+    h_best = torch.empty((n, 5), dtype=torch.int32).pin_memory()
+    h2d = b["parts"].numel() * 4 + b["weights"].numel() * 4
+    d2h = h_best.numel() * 4
+
+    def e2e_step():
+        d_parts.copy_(b["parts"], non_blocking=True)
+        d_w.copy_(b["weights"], non_blocking=True)
+        energy.zero_()
+        for i in range(n):
+            L_call_spectrum(api, d_parts[i], d_w[i], spec[i], energy[i:i + 1])
+        s.run(descs, cc=cc, best=best)
+        h_best.copy_(best, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+
+    # ---------------- plain single-subtomogram search (C0 shape), timed the same way
+    plain = run_plain(args, api)
+
+    value = world * evals / (ms / 1e3)
+    res = {
+        "metric": "CC evals/s at 64^3 (batched)",
+        "value": value,
+        "unit": "CC evals/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "batched alignment, 64^3 share: %d particles x %d local orientations (8 deg of a "
+                               "seeded prior), peak radius %d, one emc_search_run (CUDA graph) per step" %
+                               (n, N_ORIENT, PEAK_RADIUS),
+                   "box": BOX, "particles_per_gpu": n, "orientations": N_ORIENT, "evals_per_step_per_gpu": evals,
+                   "l2": "inputs larger than L2 (%.2f GB of particle spectra per GPU)" % (spec.numel() * 8 / 1e9),
+                   "parallelism": "replicas%d" % world},
+        "e2e": {"value": world * evals / (e2e_ms / 1e3), "unit": "CC evals/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h),
+                "path": "pinned host volumes + weights -> emc_particle_spectrum -> emc_search_run -> host hits"},
+        "gpu_launches": int(launches_per_step * args.steps),
+        "plain": plain,
+    }
+    res["roofline"], res["passes"] = roofline(prof)
+    res["clocks"] = clk.summary()
+    return res
+
+
+def L_call_spectrum(api, part, w, q, e):
+    """emc_particle_spectrum into preallocated buffers."""
+    import ctypes as C
+
+    from emclarity_b200 import _lib as L
+    n = part.shape[-1]
+    L.call("emc_particle_spectrum", n, C.c_void_p(part.data_ptr()), C.c_void_p(w.data_ptr()), None,
+           C.c_void_p(q.data_ptr()), C.c_void_p(e.data_ptr()), api._stream())
+
+
+def roofline(prof):
+    peak, which = measured_peaks()
+    nl = max(1, prof["launches"]["fwd_xy"])
+    per_launch_ms = (prof["ms"]["fwd_xy"] + prof["ms"]["z_mul"] + prof["ms"]["inv_peak"]) / nl
+    evals_per_launch = prof["evals"] / nl
+    b = bytes_per_eval(BOX) * evals_per_launch
+    achieved = b / (per_launch_ms / 1e3) / 1e9
+    passes = {k: {"ms_total": v, "launches": prof["launches"][k],
+                  "us_per_launch": 1e3 * v / max(1, prof["launches"][k])} for k, v in prof["ms"].items()}
+    total = sum(prof["ms"].values())
+    for k in passes:
+        passes[k]["share"] = prof["ms"][k] / total if total else None
+    return ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+             "peak_source": which + " (MEASURED_PEAKS.json hbm_gbs)" if which == "measured" else which,
+             "traffic": None, "kernel": "fused search pipeline (fwd_xy + z_mul + inv_peak per chunk)",
+             "algorithmic_bytes_per_eval": bytes_per_eval(BOX), "evals_per_launch": evals_per_launch,
+             "us_per_launch": per_launch_ms * 1e3}, passes)
+
+
+def run_plain(args, api):
+    """One particle, 540 orientations (10 degree grid), timed with CUDA events."""
+    import torch
+
+    from emclarity_b200 import synthetic
+    case = synthetic.PlainCase(seed=11)
+    g = case.to_gpu()
+    q, e = api.particle_spectrum(g["particle"], g["weight"])
+    s = api.Search(peak_radius=case.peak_radius)
+    rid = s.add_reference(g["ref"], g["mask"])
+    s.set_orientations(case.grid)
+    d = [s.particle(q, e.item(), rid, orient_count=len(case.grid))]
+    best = torch.empty((1, 5), dtype=torch.int32, device="cuda")
+    for _ in range(max(3, args.warmup)):
+        s.run(d, best=best)
+    torch.cuda.synchronize()
+    reps = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        s.run(d, best=best)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    s.close()
+    return {"workload": "1 particle x %d orientations (C1 eulerSearch 40/10/40/10), 64^3" % len(case.grid),
+            "ms_per_search": ms, "value": len(case.grid) / (ms / 1e3), "unit": "CC evals/s"}
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_port_rate(seconds=12.0, threads=None, orient_per_call=None):
+    """Single-precision CPU port of the reference path (interpn-linear rotate, FFT, normalised
+    xcf, masked argmax) on a bounded sample of the workload; OpenMP over orientations."""
+    from emclarity_b200 import synthetic
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    rng = np.random.default_rng(5)
+    ref = synthetic.blob_reference(rng, BOX)
+    mask = synthetic.soft_sphere_mask(BOX, 28)
+    part = (np.roll(ref, 2, axis=0) + rng.standard_normal(ref.shape)).astype(np.float32)
+    q, e = O.particle_spectrum(part, precision="f32")
+    grid = synthetic_local_grid_np()
+    mats = [O.define_matrix([p, t, s - p], "inv") for p, t, s in grid]
+    per = orient_per_call or max(threads, 8)
+    done, t0 = 0, time.time()
+    while True:
+        sl = [mats[(done + k) % len(mats)] for k in range(per)]
+        O.search(ref, q, e, sl, mask=mask, radius=PEAK_RADIUS, nthreads=threads, precision="f32")
+        done += per
+        if time.time() - t0 >= seconds:
+            break
+    dt = time.time() - t0
+    return done / dt, threads, "%d CC evaluations of one 64^3 particle over the local grid in %.1f s" % (done, dt)
+
+
+def synthetic_local_grid_np():
+    from oracle import oracle as O
+    g = O.euler_search_np("C1", 8.0, 2.0, 8.0, 2.0)
+    mats = np.array([O.define_matrix([p, t, s - p], "inv") for p, t, s in g])
+    ang = np.degrees(np.arccos(np.clip((np.trace(mats, axis1=1, axis2=2) - 1) / 2, -1, 1)))
+    order = np.argsort(ang, kind="stable")[:N_ORIENT]
+    return g[np.sort(order)]
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    rates = []
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        cpu_port_rate(seconds=2.0)
+    threads = os.cpu_count() or 1
+    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps)))
+    sample = None
+    for _ in range(args.steps):
+        r, threads, sample = cpu_port_rate(seconds=per_step)
+        rates.append(r)
+    v = float(np.mean(rates))
+    return {
+        "metric": "CC evals/s at 64^3 (batched)", "value": v, "unit": "CC evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "batched alignment, 64^3 share (bounded CPU sample)", "box": BOX,
+                   "orientations": N_ORIENT, "peak_radius": PEAK_RADIUS},
+        "cpu_baseline": {"value": v, "unit": "CC evals/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "CC evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--particles", type=int, default=1200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        res = run_reference(args, world, rank)
+        if res is not None:
+            print(json.dumps(res))
+        return
+    world, rank, local = dist_setup()
+    res = run_ours(args, world, rank, local)
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            r, threads, sample = cpu_port_rate(seconds=12.0)
+            res["cpu_baseline"] = {"value": r, "unit": "CC evals/s", "cores": threads, "kind": "port",
+                                   "sample": sample}
+        print(json.dumps(res))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

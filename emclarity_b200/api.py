@@ -1,0 +1,375 @@
+"""Python mirror of the reference's operator interface for the orientation-search path.
+
+Each class or function wraps one C-ABI entry point of libemc_b200.so and keeps the
+argument meaning of the reference call it replaces:
+
+* ``Interpolator``        testScripts/interpolator.m (mexXform3d)
+* ``FourierTransformer``  testScripts/fourierTransformer.m (mexFFT)
+* ``ctf2d`` / ``sf3d``    mexFiles/mexCTF.cu, mexFiles/mexSF3D.cu
+* ``Search``              the orientation loop of alignment/BH_alignRaw3d_v2.m:1119-1423
+                          with the normalised translational CC of
+                          statistics/BH_multi_xcf_Translational_2.m
+* ``TemplateSearch``      alignment/BH_templateSearch3d_2.m:633-887
+
+Tensors are torch CUDA tensors used as device buffers only; volumes have shape
+(nz, ny, nx) (x fastest, the reference's column-major order), half spectra are complex64
+of shape (nz, ny, nx//2+1).  Every computation runs in the CUDA library; a missing
+library or a CPU tensor raises.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _need_cuda(t, name, dtype=torch.float32):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("%s must be a CUDA tensor" % name)
+    if t.dtype != dtype:
+        raise TypeError("%s must be %s, got %s" % (name, dtype, t.dtype))
+    if not t.is_contiguous():
+        raise ValueError("%s must be contiguous" % name)
+    return C.c_void_p(t.data_ptr())
+
+
+def _dptr(arr):
+    arr = np.ascontiguousarray(arr, dtype=np.float64)
+    return arr, arr.ctypes.data_as(C.POINTER(C.c_double))
+
+
+# --------------------------------------------------------------------------- host math
+def define_matrix(angles, direction="inv"):
+    """BH_defineMatrix(angles, 'Bah', direction) as a (3, 3) float64 array (row i, col j)."""
+    d = {"forward": 0, "inv": 1}[direction]
+    a, ap = _dptr(angles)
+    out = np.zeros(9)
+    L.call("emc_define_matrix", ap, d, out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out.reshape(3, 3, order="F")
+
+
+def euler_search(symmetry, theta_max, theta_step, psi_max, psi_step):
+    """eulerSearch grid as an (n, 3) array of (phi, theta, psi) in degrees, walk order."""
+    cnt = C.c_int(0)
+    L.call("emc_euler_search", symmetry.encode(), theta_max, theta_step, psi_max, psi_step, None, C.byref(cnt))
+    out = np.zeros((cnt.value, 3))
+    L.call("emc_euler_search", symmetry.encode(), theta_max, theta_step, psi_max, psi_step,
+           out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cnt))
+    return out
+
+
+def search_matrices(phi_theta_psi, prior=None):
+    """RotMat = prior * defineMatrix([phi, theta, psi-phi], 'inv') for every orientation (FP64)."""
+    prior = np.eye(3) if prior is None else np.asarray(prior, dtype=np.float64)
+    out = []
+    for phi, theta, psi in np.asarray(phi_theta_psi, dtype=np.float64):
+        out.append(prior @ define_matrix([phi, theta, psi - phi], "inv"))
+    return np.array(out)
+
+
+# --------------------------------------------------------------------------- interpolator
+class Interpolator:
+    """Rotate / shift / interpolate a volume (mexXform3d through interpolator.m).
+
+    ``interp3d(angles, shifts, direction, symmetry_matrices)``: ``angles`` is an Euler
+    triple (converted with defineMatrix(angles, 'Bah', direction)) or a 3x3 matrix used as
+    is; 'forward' negates the shift and applies it before the rotation, 'inv' after it.
+    """
+
+    def __init__(self, volume, store="f32", interp="linear"):
+        self.shape = tuple(volume.shape)
+        nz, ny, nx = self.shape
+        h = C.c_void_p()
+        dt = {"f32": L.DTYPE_F32, "bf16": L.DTYPE_BF16}[store]
+        L.call("emc_xform3d_create", _need_cuda(volume, "volume"), nx, ny, nz, dt, C.byref(h), _stream())
+        self._h = h
+        self.interp = {"linear": L.INTERP_LINEAR, "cubic": L.INTERP_CUBIC,
+                       "linear_border": L.INTERP_LINEAR_BORDER}[interp]
+
+    def interp3d(self, angles, shifts=(0.0, 0.0, 0.0), direction="forward", symmetry=None, out=None):
+        m = np.asarray(angles, dtype=np.float64)
+        if m.size == 3:
+            m = define_matrix(m, direction)
+        m = m.reshape(3, 3)
+        mats = [m] if symmetry is None else [m @ s for s in symmetry]
+        packed = np.concatenate([np.asarray(x, dtype=np.float64).reshape(3, 3).flatten(order="F") for x in mats])
+        packed, pp = _dptr(packed)
+        sh = (C.c_float * 3)(*[float(v) for v in shifts])
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device="cuda")
+        fwd = 1 if direction == "forward" else 0
+        L.call("emc_xform3d_apply", self._h, pp, len(mats), sh, fwd, self.interp, _need_cuda(out, "out"), _stream())
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.load().emc_xform3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------- FFT
+class FourierTransformer:
+    """Unnormalised R2C / C2R transforms with a cached plan (mexFFT through fourierTransformer.m)."""
+
+    def __init__(self, shape, batch=1):
+        shape = tuple(shape)
+        self.shape = shape
+        dims = list(reversed(shape))  # x fastest
+        rank = len(dims)
+        arr = (C.c_int * 3)(*(dims + [1] * (3 - rank)))
+        h = C.c_void_p()
+        L.call("emc_fft_plan", rank, arr, batch, C.byref(h))
+        self._h = h
+        self.batch = batch
+        self.half_shape = shape[:-1] + (shape[-1] // 2 + 1,)
+        # fourierTransformer.m:63-66
+        self.inv_trim = 1 if shape[-1] % 2 else 2
+
+    def fwd_fft(self, vol, out=None):
+        if out is None:
+            out = torch.empty(((self.batch,) if self.batch > 1 else ()) + self.half_shape, dtype=torch.complex64,
+                              device="cuda")
+        L.call("emc_fft_r2c", self._h, _need_cuda(vol, "vol"), _need_cuda(out, "out", torch.complex64), _stream())
+        return out
+
+    def inv_fft(self, ft, out=None):
+        if out is None:
+            out = torch.empty(((self.batch,) if self.batch > 1 else ()) + self.shape, dtype=torch.float32,
+                              device="cuda")
+        L.call("emc_fft_c2r", self._h, _need_cuda(ft, "ft", torch.complex64), _need_cuda(out, "out"), _stream())
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.load().emc_fft_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------- CTF
+def _ctfp(pixel_size, wavelength, cs_mm, defocus1, defocus2, astig_deg, amp_contrast):
+    return L.CtfParams(pixel_size, wavelength, cs_mm, amp_contrast, defocus1, defocus2, astig_deg)
+
+
+def ctf2d(nx, ny, pixel_size, wavelength, cs_mm, defocus1, defocus2, astig_deg, amp_contrast, half=True,
+          squared=False, centred=False, radial_weight=None, exposure=None):
+    """mexCTF(half, sq, nX, nY, pix, lambda, Cs, df1, df2, ast, AC[, centred]) -> (ny, nx') tensor."""
+    p = _ctfp(pixel_size, wavelength, cs_mm, defocus1, defocus2, astig_deg, amp_contrast)
+    out = torch.empty((ny, nx // 2 + 1 if half else nx), dtype=torch.float32, device="cuda")
+    if radial_weight is None:
+        L.call("emc_ctf2d", C.byref(p), nx, ny, int(half), int(squared), int(centred), _need_cuda(out, "out"),
+               _stream())
+    else:
+        L.call("emc_ctf2d_exposure", C.byref(p), nx, ny, int(half), int(squared), int(centred),
+               float(radial_weight), float(exposure), _need_cuda(out, "out"), _stream())
+    return out
+
+
+def sf3d(size, pixel_size, wavelength, cs_mm, df1, df2, astig_deg, amp_contrast, tilt_deg, exposure, occupancy,
+         squared=True):
+    """mexSF3D: sum over tilts of the exposure-weighted CTF^2 on the tilted central slab.
+
+    ``size`` is (nx, ny, nz); per-tilt arrays have one entry per tilt.  Returns (nz, ny, nx)."""
+    nt = len(tilt_deg)
+
+    def fa(x):
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=np.float32), (nt,)))
+        return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+    arrs = [fa(x) for x in (pixel_size, wavelength, cs_mm, df1, df2, astig_deg, amp_contrast, tilt_deg, exposure,
+                            occupancy)]
+    sz = (C.c_uint * 3)(*[int(v) for v in size])
+    out = torch.empty((size[2], size[1], size[0]), dtype=torch.float32, device="cuda")
+    L.call("emc_sf3d", 0, int(squared), sz, *[a[1] for a in arrs[:7]], nt, arrs[7][1], arrs[8][1], arrs[9][1],
+           _need_cuda(out, "out"), _stream())
+    return out
+
+
+def wedge_ctf_weight(n, tilt_min=-60.0, tilt_max=60.0, ctf=None, squared=False):
+    """Half-spectrum (n, n, n//2+1) weight: binary Y-axis missing wedge times the 3-D CTF.
+
+    ``ctf``: dict(pixel_size, wavelength, cs_mm, defocus, amp_contrast) or None."""
+    out = torch.empty((n, n, n // 2 + 1), dtype=torch.float32, device="cuda")
+    p = None
+    if ctf is not None:
+        p = C.byref(_ctfp(ctf["pixel_size"], ctf["wavelength"], ctf["cs_mm"], ctf["defocus"], ctf["defocus"], 0.0,
+                          ctf["amp_contrast"]))
+    L.call("emc_wedge_ctf_weight", int(n), float(tilt_min), float(tilt_max), p, int(squared),
+           _need_cuda(out, "out"), _stream())
+    return out
+
+
+# --------------------------------------------------------------------------- particle prep
+def particle_spectrum(particle, weight=None, bandpass=None):
+    """Q = weight .* bandpass .* fftn(particle), Q(0) = 0, and E_P = sum |Q|^2 (full spectrum)."""
+    n = particle.shape[-1]
+    q = torch.empty((n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    L.call("emc_particle_spectrum", n, _need_cuda(particle, "particle"),
+           _need_cuda(weight, "weight") if weight is not None else None,
+           _need_cuda(bandpass, "bandpass") if bandpass is not None else None,
+           _need_cuda(q, "q", torch.complex64), _need_cuda(e, "energy", torch.float64), _stream())
+    return q, e
+
+
+def particle_template(q):
+    """h = unnormalised inverse transform of Q (the real-space particle template)."""
+    n = q.shape[0]
+    h = torch.empty((n, n, n), dtype=torch.float32, device="cuda")
+    L.call("emc_particle_template", n, _need_cuda(q, "q", torch.complex64), _need_cuda(h, "h"), _stream())
+    return h
+
+
+# --------------------------------------------------------------------------- search
+class Search:
+    """Fused orientation search: rotate the reference, FFT, conj-multiply with the particle
+    spectrum, normalised CC map over the peak window, argmax, best orientation."""
+
+    def __init__(self, peak_radius=0, interp="linear", chunk_evals=0):
+        h = C.c_void_p()
+        L.call("emc_search_create", C.byref(h))
+        self._h = h
+        self._keep = []
+        self.configure(peak_radius, interp, chunk_evals)
+
+    def configure(self, peak_radius=0, interp="linear", chunk_evals=0):
+        mode = {"linear": L.INTERP_LINEAR, "cubic": L.INTERP_CUBIC, "linear_border": L.INTERP_LINEAR_BORDER}[interp]
+        L.call("emc_search_configure", self._h, int(peak_radius), mode, int(chunk_evals))
+
+    def add_reference(self, ref, mask=None, wref=None, store="f32"):
+        n = ref.shape[-1]
+        rid = C.c_int(-1)
+        dt = {"f32": L.DTYPE_F32, "bf16": L.DTYPE_BF16}[store]
+        L.call("emc_search_add_reference", self._h, _need_cuda(ref, "ref"), n,
+               _need_cuda(mask, "mask") if mask is not None else None,
+               _need_cuda(wref, "wref") if wref is not None else None, dt, C.byref(rid), _stream())
+        return rid.value
+
+    def set_orientations(self, phi_theta_psi):
+        a, ap = _dptr(np.asarray(phi_theta_psi, dtype=np.float64).reshape(-1, 3))
+        L.call("emc_search_set_orientations", self._h, ap, a.shape[0])
+        self.n_orient = a.shape[0]
+
+    @staticmethod
+    def particle(spectrum, energy, ref_id, prior=None, shift=(0, 0, 0), orient_begin=0, orient_count=0):
+        d = L.ParticleDesc()
+        d.spectrum = spectrum.data_ptr()
+        d.energy = float(energy)
+        pr = np.eye(3) if prior is None else np.asarray(prior, dtype=np.float64).reshape(3, 3)
+        d.prior[:] = list(pr.flatten(order="F"))
+        d.shift[:] = [float(v) for v in shift]
+        d.box = spectrum.shape[0]
+        d.ref_id = int(ref_id)
+        d.orient_begin = int(orient_begin)
+        d.orient_count = int(orient_count)
+        return d
+
+    def run(self, particles, cc=None, peak=None, best=None, stream=None):
+        """Device outputs: cc (float32 [pairs]), peak (int32 [pairs, 3]), best (int32 [np, 5] view of hits)."""
+        arr = (L.ParticleDesc * len(particles))(*particles)
+        self._keep = [arr]
+        L.call("emc_search_run", self._h, arr, len(particles),
+               _need_cuda(cc, "cc") if cc is not None else None,
+               _need_cuda(peak, "peak", torch.int32) if peak is not None else None,
+               _need_cuda(best, "best", torch.int32) if best is not None else None, _stream(stream))
+
+    def run_host(self, particles):
+        """Host outputs: (cc [pairs], peak [pairs, 3], best list of (cc, orient, peak))."""
+        total = sum(p.orient_count for p in particles)
+        arr = (L.ParticleDesc * len(particles))(*particles)
+        cc = np.zeros(total, dtype=np.float32)
+        pk = np.zeros((total, 3), dtype=np.int32)
+        hits = (L.SearchHit * len(particles))()
+        L.call("emc_search_run_host", self._h, arr, len(particles), cc.ctypes.data_as(C.POINTER(C.c_float)),
+               pk.ctypes.data_as(C.POINTER(C.c_int)), hits, _stream())
+        best = [(h.cc, h.orient, tuple(h.peak)) for h in hits]
+        return cc, pk, best
+
+    def set_profiling(self, enable=True):
+        L.call("emc_search_set_profiling", self._h, int(bool(enable)))
+
+    def timings(self, reset=False):
+        """Per-pass device time (ms) and launch counts since the last reset, CC evaluations,
+        and the number of kernels launched by the most recent run."""
+        ms = (C.c_double * 4)()
+        ln = (C.c_long * 4)()
+        ev = C.c_long(0)
+        last = C.c_long(0)
+        L.call("emc_search_timings", self._h, ms, ln, C.byref(ev), C.byref(last), int(bool(reset)))
+        names = ("fwd_xy", "z_mul", "inv_peak", "decode")
+        return {"ms": dict(zip(names, list(ms))), "launches": dict(zip(names, list(ln))), "evals": ev.value,
+                "launches_last_run": last.value}
+
+    def cc_adjoint(self, ref_id, h, energy_p, prior, poses):
+        """CC and gradient (dphi, dtheta, dpsi per degree; dtx, dty, dtz per voxel) per pose."""
+        poses = np.ascontiguousarray(np.asarray(poses, dtype=np.float64).reshape(-1, 6))
+        pr, pp = _dptr(np.asarray(prior, dtype=np.float64).reshape(3, 3).flatten(order="F"))
+        n = poses.shape[0]
+        cc = np.zeros(n)
+        grad = np.zeros((n, 6))
+        L.call("emc_cc_adjoint", self._h, int(ref_id), _need_cuda(h, "h"), float(energy_p), pp,
+               poses.ctypes.data_as(C.POINTER(C.c_double)), n, cc.ctypes.data_as(C.POINTER(C.c_double)),
+               grad.ctypes.data_as(C.POINTER(C.c_double)), _stream())
+        return cc, grad
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.load().emc_search_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TemplateSearch:
+    """Template matching over a whole tomogram: per-voxel max of std-normalised CC maps and
+    the 1-based index of the winning orientation (BH_templateSearch3d_2.m:633-887)."""
+
+    def __init__(self, tomogram):
+        nz, ny, nx = tomogram.shape
+        self.shape = (nz, ny, nx)
+        h = C.c_void_p()
+        L.call("emc_tsearch_create", _need_cuda(tomogram, "tomogram"), nx, ny, nz, C.byref(h), _stream())
+        self._h = h
+
+    def run(self, template, phi_theta_psi, peak=None, angle=None):
+        t = template.shape[-1]
+        a, ap = _dptr(np.asarray(phi_theta_psi, dtype=np.float64).reshape(-1, 3))
+        if peak is None:
+            peak = torch.empty(self.shape, dtype=torch.float32, device="cuda")
+        if angle is None:
+            angle = torch.empty(self.shape, dtype=torch.float32, device="cuda")
+        L.call("emc_tsearch_run", self._h, _need_cuda(template, "template"), t, ap, a.shape[0],
+               _need_cuda(peak, "peak"), _need_cuda(angle, "angle"), _stream())
+        return peak, angle
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.load().emc_tsearch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

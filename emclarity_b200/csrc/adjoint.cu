@@ -1,0 +1,219 @@
+// adjoint.cu -- forward + adjoint of the masked normalised CC with respect to the pose.
+//
+// For pose (phi, theta, psi, t) the reference is sampled with tricubic interpolation at
+//   s(p) = M (p - c - t) + c,   M = (R_prior * D)',  D = defineMatrix([phi, theta, psi-phi], 'inv')
+// (the 'forward' sampling of BH_alignRaw3d_v2.m:1287-1291), masked, and correlated at zero lag
+// with the real-space particle template h = unnormalised inverse FFT of Q:
+//   CC = A / sqrt(E_R E_P),  A = sum r h,  E_R = n^3 sum r^2 - (sum r)^2  (DC-free, Parseval).
+// One pass over the voxels accumulates, in FP64, A, sum r, sum r^2 and for each pose parameter k
+// the sums H_k = sum h G_k, R_k = sum r G_k, S_k = sum G_k with G_k = dr/dk; then
+//   dCC/dk = H_k / sqrt(E_R E_P) - CC / E_R * (n^3 R_k - sum r * S_k).
+// The Euler-angle derivatives of M are formed on the host in FP64.
+#include <math.h>
+
+#include <vector>
+
+#include "interp.cuh"
+
+namespace emc {
+
+constexpr int kAdjSums = 21;  // A, S1, S2, then (H, R, S) x 6
+
+struct AdjPose {
+  float m[9];       // sampling matrix rows
+  float dm[3][9];   // d m / d(phi, theta, psi) per degree
+  float t[3];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_cc_adjoint(const T* __restrict__ ref, const float* __restrict__ mask,
+                                                    const float* __restrict__ h, int n,
+                                                    const AdjPose* __restrict__ poses, double* __restrict__ sums) {
+  __shared__ AdjPose sp;
+  __shared__ double red[kAdjSums][8];
+  const int pose = blockIdx.y;
+  if (threadIdx.x == 0) sp = poses[pose];
+  __syncthreads();
+  const int c = n / 2;
+  const long nv = (long)n * n * n;
+  float acc[kAdjSums];
+#pragma unroll
+  for (int k = 0; k < kAdjSums; ++k) acc[k] = 0.f;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nv; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((long)n * n));
+    const float u0 = (float)(x - c) - sp.t[0], u1 = (float)(y - c) - sp.t[1], u2 = (float)(z - c) - sp.t[2];
+    const float* m = sp.m;
+    const float sx = fmaf(m[0], u0, fmaf(m[1], u1, m[2] * u2)) + (float)c;
+    const float sy = fmaf(m[3], u0, fmaf(m[4], u1, m[5] * u2)) + (float)c;
+    const float sz = fmaf(m[6], u0, fmaf(m[7], u1, m[8] * u2)) + (float)c;
+    float g[3];
+    const float v = sample_cubic_grad(ref, n, n, n, sx, sy, sz, g);
+    const float mk = mask ? __ldg(mask + i) : 1.f;
+    const float r = mk * v;
+    const float hv = __ldg(h + i);
+    g[0] *= mk; g[1] *= mk; g[2] *= mk;
+    acc[0] += r * hv;
+    acc[1] += r;
+    acc[2] += r * r;
+    // angle derivatives: ds/dk = dm_k u
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float* d = sp.dm[k];
+      const float gk = g[0] * fmaf(d[0], u0, fmaf(d[1], u1, d[2] * u2)) +
+                       g[1] * fmaf(d[3], u0, fmaf(d[4], u1, d[5] * u2)) +
+                       g[2] * fmaf(d[6], u0, fmaf(d[7], u1, d[8] * u2));
+      acc[3 + 3 * k] += hv * gk;
+      acc[4 + 3 * k] += r * gk;
+      acc[5 + 3 * k] += gk;
+    }
+    // shift derivatives: ds/dt_j = -M[:, j]
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const float gk = -(g[0] * m[j] + g[1] * m[3 + j] + g[2] * m[6 + j]);
+      acc[12 + 3 * j] += hv * gk;
+      acc[13 + 3 * j] += r * gk;
+      acc[14 + 3 * j] += gk;
+    }
+  }
+  // block reduction in FP64
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < kAdjSums; ++k) {
+    double v = (double)acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kAdjSums) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
+    atomicAdd(sums + (long)pose * kAdjSums + threadIdx.x, t);
+  }
+}
+
+// Rz / Rx and their derivatives (per radian), column-major 3x3 products in FP64.
+static void mat_mul(const double* a, const double* b, double* c) {
+  double t[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += a[i + 3 * k] * b[k + 3 * j];
+      t[i + 3 * j] = s;
+    }
+  for (int i = 0; i < 9; ++i) c[i] = t[i];
+}
+static void rz(double a, double* r, bool d) {
+  const double c = cos(a), s = sin(a);
+  // [[c,-s,0],[s,c,0],[0,0,1]] and its derivative [[-s,-c,0],[c,-s,0],[0,0,0]]
+  const double v[9] = {d ? -s : c, d ? c : s, 0, d ? -c : -s, d ? -s : c, 0, 0, 0, d ? 0.0 : 1.0};
+  for (int i = 0; i < 9; ++i) r[i] = v[i];
+}
+static void rx(double a, double* r, bool d) {
+  const double c = cos(a), s = sin(a);
+  const double v[9] = {d ? 0.0 : 1.0, 0, 0, 0, d ? -s : c, d ? c : s, 0, d ? -c : -s, d ? -s : c};
+  for (int i = 0; i < 9; ++i) r[i] = v[i];
+}
+
+// D = defineMatrix([phi, theta, psi - phi], 'inv') = Rz(phi) Rx(theta) Rz(psi - phi) and the
+// derivatives of M = (prior D)' with respect to phi, theta, psi (per degree).
+static void pose_matrices(const double prior[9], const double* pose, AdjPose* out) {
+  const double k = M_PI / 180.0;
+  const double a1 = pose[0] * k, a2 = pose[1] * k, a3 = (pose[2] - pose[0]) * k;
+  double Z1[9], X2[9], Z3[9], dZ1[9], dX2[9], dZ3[9], t[9], D[9], dD[3][9];
+  rz(a1, Z1, false); rz(a1, dZ1, true);
+  rx(a2, X2, false); rx(a2, dX2, true);
+  rz(a3, Z3, false); rz(a3, dZ3, true);
+  mat_mul(Z1, X2, t); mat_mul(t, Z3, D);
+  // d/dphi: dZ1 X2 Z3 - Z1 X2 dZ3   (a3 = psi - phi)
+  double p1[9], p2[9];
+  mat_mul(dZ1, X2, t); mat_mul(t, Z3, p1);
+  mat_mul(Z1, X2, t); mat_mul(t, dZ3, p2);
+  for (int i = 0; i < 9; ++i) dD[0][i] = p1[i] - p2[i];
+  mat_mul(Z1, dX2, t); mat_mul(t, Z3, dD[1]);
+  mat_mul(Z1, X2, t); mat_mul(t, dZ3, dD[2]);
+  double R[9], dR[3][9];
+  mat_mul(prior, D, R);
+  for (int j = 0; j < 3; ++j) mat_mul(prior, dD[j], dR[j]);
+  // sampling matrix rows m[3i + j] = M(i, j) = R(j, i)
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      out->m[3 * i + j] = (float)R[j + 3 * i];
+      for (int q = 0; q < 3; ++q) out->dm[q][3 * i + j] = (float)(dR[q][j + 3 * i] * k);
+    }
+  for (int j = 0; j < 3; ++j) out->t[j] = (float)pose[3 + j];
+}
+
+}  // namespace emc
+
+// Defined in search.cu: access to a registered reference.
+emc_status emc_search_reference_info(emc_search_t s, int ref_id, const void** data, const float** mask, int* n,
+                                     int* dtype);
+
+extern "C" {
+
+emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, double energy_p, const double prior[9],
+                          const double* poses, int n_poses, double* h_cc, double* h_grad, void* stream) {
+  EMC_CHECK_ARG(s && d_h && prior && poses && h_cc && h_grad, "emc_cc_adjoint: null argument");
+  EMC_CHECK_ARG(n_poses > 0 && n_poses <= 65535, "emc_cc_adjoint: n_poses %d", n_poses);
+  EMC_CHECK_ARG(energy_p > 0.0, "emc_cc_adjoint: energy must be > 0");
+  const void* data = nullptr;
+  const float* mask = nullptr;
+  int n = 0, dtype = 0;
+  EMC_TRY(emc_search_reference_info(s, ref_id, &data, &mask, &n, &dtype));
+  cudaStream_t st = emc::as_stream(stream);
+  std::vector<emc::AdjPose> hp(n_poses);
+  for (int i = 0; i < n_poses; ++i) emc::pose_matrices(prior, poses + 6 * i, &hp[i]);
+  const size_t pose_bytes = sizeof(emc::AdjPose) * n_poses;
+  const size_t sum_bytes = sizeof(double) * emc::kAdjSums * n_poses;
+  char* buf = nullptr;
+  EMC_CUDA(cudaMallocAsync(&buf, pose_bytes + sum_bytes + 64, st));
+  emc::AdjPose* d_poses = reinterpret_cast<emc::AdjPose*>(buf);
+  double* d_sums = reinterpret_cast<double*>(buf + ((pose_bytes + 15) / 16) * 16);
+  std::vector<double> sums((size_t)emc::kAdjSums * n_poses);
+  emc_status rs = EMC_OK;
+  if (cudaMemcpyAsync(d_poses, hp.data(), pose_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemsetAsync(d_sums, 0, sum_bytes, st) != cudaSuccess) {
+    emc::set_error("emc_cc_adjoint: upload failed");
+    rs = EMC_E_CUDA;
+  }
+  if (rs == EMC_OK) {
+    const long nv = (long)n * n * n;
+    const int bx = (int)std::max<long>(1, std::min<long>((nv + 2047) / 2048, 2L * emc::device_sm_count()));
+    dim3 grid(bx, n_poses);
+    if (dtype == EMC_DTYPE_F32)
+      emc::k_cc_adjoint<float><<<grid, 256, 0, st>>>((const float*)data, mask, d_h, n, d_poses, d_sums);
+    else
+      emc::k_cc_adjoint<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)data, mask, d_h, n, d_poses,
+                                                             d_sums);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(sums.data(), d_sums, sum_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      emc::set_error("emc_cc_adjoint: kernel or copy failed");
+      rs = EMC_E_CUDA;
+    }
+  }
+  cudaFreeAsync(buf, st);
+  if (rs != EMC_OK) return rs;
+  const double n3 = (double)n * n * n;
+  for (int i = 0; i < n_poses; ++i) {
+    const double* q = &sums[(size_t)emc::kAdjSums * i];
+    const double A = q[0], S1 = q[1], S2 = q[2];
+    const double er = n3 * S2 - S1 * S1;
+    if (!(er > 0.0)) {
+      h_cc[i] = NAN;
+      for (int k = 0; k < 6; ++k) h_grad[6 * i + k] = NAN;
+      continue;
+    }
+    const double norm = 1.0 / sqrt(er * energy_p);
+    const double cc = A * norm;
+    h_cc[i] = cc;
+    for (int k = 0; k < 6; ++k) {
+      const double H = q[3 + 3 * k], R = q[4 + 3 * k], S = q[5 + 3 * k];
+      h_grad[6 * i + k] = H * norm - cc / er * (n3 * R - S1 * S);
+    }
+  }
+  return EMC_OK;
+}
+
+}  // extern "C"

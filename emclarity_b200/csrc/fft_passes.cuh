@@ -1,0 +1,161 @@
+// fft_passes.cuh -- generic single-axis FFT passes over global memory.
+//
+// These are the building blocks of the standalone R2C / C2R transform (the mexFFT
+// replacement), of the particle-spectrum preparation and of the large-volume
+// template search.  The fused orientation-search kernels use the same line FFT
+// but keep the data on chip between axes.
+#pragma once
+#include "common.cuh"
+
+namespace emc {
+
+// ----------------------------------------------------------------- rows, R2C
+// nrows real rows of length L (pitch in_pitch floats) -> complex rows of length
+// L/2+1 (pitch out_pitch float2).  Two rows share one complex FFT: z = a + i b.
+// Teams per CTA of the row kernels: at most 256 threads and ~32 KB of line buffers.
+__host__ __device__ constexpr int rows_teams(int L, int P) {
+  return (256 / P) < (4096 / (L + 1)) ? (256 / P) : ((4096 / (L + 1)) > 0 ? (4096 / (L + 1)) : 1);
+}
+
+template <int L, int P>
+__global__ void __launch_bounds__(256) k_rows_r2c(const float* __restrict__ in, long in_pitch,
+                                                  float2* __restrict__ out, long out_pitch, long nrows,
+                                                  const float2* __restrict__ g_tw) {
+  constexpr int TEAMS = rows_teams(L, P);
+  __shared__ float2 s_tw[L];
+  __shared__ float2 s_line[TEAMS][L + 1];
+  load_twiddles<L>(s_tw, g_tw);
+  __syncthreads();
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  const long npairs = (nrows + 1) / 2;
+  for (long pair0 = (long)blockIdx.x * TEAMS; pair0 < npairs; pair0 += (long)gridDim.x * TEAMS) {
+    const long pair = pair0 + team;
+    const bool active = pair < npairs;
+    const long ra = 2 * pair, rb = 2 * pair + 1;
+    const bool has_b = rb < nrows;
+    float2* buf = s_line[team];
+    if (active) {
+      const float* a = in + ra * in_pitch;
+      const float* b = in + rb * in_pitch;
+      for (int n = lane; n < L; n += P) buf[n] = make_float2(__ldg(a + n), has_b ? __ldg(b + n) : 0.f);
+    }
+    __syncwarp();
+    fft_line<L, -1, P>(buf, 1, lane, s_tw, active);
+    if (active) {
+      float2* oa = out + ra * out_pitch;
+      float2* ob = out + rb * out_pitch;
+      for (int k = lane; k <= L / 2; k += P) {
+        const float2 zk = buf[k], zm = buf[(L - k) % L];
+        oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        if (has_b) ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ----------------------------------------------------------------- rows, C2R
+// complex rows of length L/2+1 -> real rows of length L (unnormalised inverse).
+// The imaginary parts of the k = 0 and k = L/2 terms are ignored (real-part
+// semantics of a Hermitian inverse).
+template <int L, int P>
+__global__ void __launch_bounds__(256) k_rows_c2r(const float2* __restrict__ in, long in_pitch,
+                                                  float* __restrict__ out, long out_pitch, long nrows,
+                                                  const float2* __restrict__ g_tw) {
+  constexpr int TEAMS = rows_teams(L, P);
+  __shared__ float2 s_tw[L];
+  __shared__ float2 s_line[TEAMS][L + 1];
+  load_twiddles<L>(s_tw, g_tw);
+  __syncthreads();
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  const long npairs = (nrows + 1) / 2;
+  for (long pair0 = (long)blockIdx.x * TEAMS; pair0 < npairs; pair0 += (long)gridDim.x * TEAMS) {
+    const long pair = pair0 + team;
+    const bool active = pair < npairs;
+    const long ra = 2 * pair, rb = 2 * pair + 1;
+    const bool has_b = rb < nrows;
+    float2* buf = s_line[team];
+    if (active) {
+      const float2* a = in + ra * in_pitch;
+      const float2* b = in + rb * in_pitch;
+      for (int n = lane; n < L; n += P) {
+        const bool lower = n <= L / 2;
+        const int k = lower ? n : L - n;
+        float2 A = a[k];
+        float2 B = has_b ? b[k] : make_float2(0.f, 0.f);
+        if (k == 0 || 2 * k == L) { A.y = 0.f; B.y = 0.f; }
+        if (!lower) { A.y = -A.y; B.y = -B.y; }
+        buf[n] = make_float2(A.x - B.y, A.y + B.x);
+      }
+    }
+    __syncwarp();
+    fft_line<L, 1, P>(buf, 1, lane, s_tw, active);
+    if (active) {
+      float* oa = out + ra * out_pitch;
+      float* ob = out + rb * out_pitch;
+      for (int n = lane; n < L; n += P) {
+        const float2 z = buf[n];
+        oa[n] = z.x;
+        if (has_b) ob[n] = z.y;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ----------------------------------------------------------------- strided columns
+// Complex lines along a strided axis: element n of line (o, i) lives at
+// base + o*outer_pitch + i + n*stride, for i in [0, inner), o in [0, outer).
+// One CTA transforms a tile of T consecutive i for one o; in == out is allowed.
+template <int L, int SIGN, int P, int T>
+__global__ void __launch_bounds__(P * T) k_cols(const float2* __restrict__ in, float2* __restrict__ out,
+                                                long stride, long inner, long outer, long outer_pitch,
+                                                const float2* __restrict__ g_tw) {
+  extern __shared__ float2 smem[];
+  float2* s_tw = smem;
+  float2* tile = smem + L;  // [L][T+1]
+  constexpr int TP = T + 1;
+  load_twiddles<L>(s_tw, g_tw);
+  const long i0 = (long)blockIdx.x * T;
+  const int nt = P * T;
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  for (long o = blockIdx.y; o < outer; o += gridDim.y) {
+    const float2* src = in + o * outer_pitch + i0;
+    float2* dst = out + o * outer_pitch + i0;
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < L * T; idx += nt) {
+      const int n = idx / T, t = idx % T;
+      if (i0 + t < inner) tile[n * TP + t] = src[(long)n * stride + t];
+    }
+    __syncthreads();
+    fft_line<L, SIGN, P>(tile + team, TP, lane, s_tw, i0 + team < inner);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < L * T; idx += nt) {
+      const int n = idx / T, t = idx % T;
+      if (i0 + t < inner) dst[(long)n * stride + t] = tile[n * TP + t];
+    }
+  }
+}
+
+template <int L>
+struct ColsCfg {
+  static constexpr int P = team_size(L);
+  static constexpr int T = (512 / P) < 32 ? (512 / P) : 32;
+  static constexpr size_t smem = sizeof(float2) * (L + (size_t)L * (T + 1));
+};
+
+// Host launchers (defined in fft_passes.cu); return EMC_OK or an error status.
+emc_status launch_rows_r2c(int L, const float* in, long in_pitch, float2* out, long out_pitch, long nrows,
+                           cudaStream_t st);
+emc_status launch_rows_c2r(int L, const float2* in, long in_pitch, float* out, long out_pitch, long nrows,
+                           cudaStream_t st);
+emc_status launch_cols(int L, int sign, const float2* in, float2* out, long stride, long inner, long outer,
+                       long outer_pitch, cudaStream_t st);
+
+// Full 3-D R2C / C2R over a batch of volumes (x fastest).  c2r uses `scratch`
+// ((nx/2+1)*ny*nz*batch float2) so that `in` is left untouched.
+emc_status fft3_r2c(const float* in, float2* out, int nx, int ny, int nz, int batch, cudaStream_t st);
+emc_status fft3_c2r(const float2* in, float* out, float2* scratch, int nx, int ny, int nz, int batch,
+                    cudaStream_t st);
+
+}  // namespace emc

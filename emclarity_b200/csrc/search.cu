@@ -1,0 +1,666 @@
+// search.cu -- host orchestration of the fused orientation search (C-ABI emc_search_*),
+// particle-spectrum preparation and the real-space particle template.
+//
+// A run evaluates every (particle, orientation) pair of the request.  Pairs are grouped by
+// (box size, reference storage type) and cut into chunks whose on-chip-spilled scratch
+// (S1 + S2) stays inside a budget sized to the L2 cache; each chunk is four launches
+// (fwd_xy, z_mul, inv_peak, decode).  The whole launch sequence of a run is captured once
+// in a CUDA graph and replayed while the request (particles, outputs, settings) is unchanged.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "fft_passes.cuh"
+#include "search_kernels.cuh"
+
+namespace emc {
+
+struct EvalResult {
+  float cc;
+  int peak[3];
+};
+
+// Decodes the per-evaluation keys of one chunk into EvalResult rows and folds each
+// evaluation into its particle's best-orientation key.
+__global__ void k_search_decode(const SearchChunkArgs a, int n, EvalResult* __restrict__ results,
+                                unsigned long long* __restrict__ best_keys) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.n_items) return;
+  const EvalItem it = a.items[e];
+  const DevParticle& pt = a.parts[it.particle];
+  const unsigned long long key = a.keys[e];
+  EvalResult r;
+  const int c = n / 2;
+  if (key == 0ull) {
+    r.cc = __int_as_float(0x7fc00000);
+    r.peak[0] = r.peak[1] = r.peak[2] = 0;
+  } else {
+    r.cc = key_to_float((unsigned int)(key >> 32));
+    const unsigned int lin = 0xffffffffu - (unsigned int)(key & 0xffffffffull);
+    r.peak[0] = (int)(lin % n) - c;
+    r.peak[1] = (int)((lin / n) % n) - c;
+    r.peak[2] = (int)(lin / ((unsigned)n * n)) - c;
+  }
+  const long out = pt.eval_base + (it.orient - pt.orient_begin);
+  results[out] = r;
+  if (key != 0ull) {
+    const unsigned long long bk = ((unsigned long long)ordered_key(r.cc) << 32) | (0xffffffffu - (unsigned)it.orient);
+    atomicMax(best_keys + it.particle, bk);
+  }
+}
+
+__global__ void k_search_best(const DevParticle* __restrict__ parts, int np, const EvalResult* __restrict__ results,
+                              const unsigned long long* __restrict__ best_keys, emc_search_hit* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const unsigned long long k = best_keys[p];
+  emc_search_hit h;
+  if (k == 0ull) {
+    h.cc = __int_as_float(0x7fc00000);
+    h.orient = -1;
+    h.peak[0] = h.peak[1] = h.peak[2] = 0;
+  } else {
+    const int o = (int)(0xffffffffu - (unsigned int)(k & 0xffffffffull));
+    const EvalResult r = results[parts[p].eval_base + (o - parts[p].orient_begin)];
+    h.cc = r.cc;
+    h.orient = o;
+    h.peak[0] = r.peak[0]; h.peak[1] = r.peak[1]; h.peak[2] = r.peak[2];
+  }
+  out[p] = h;
+}
+
+__global__ void k_search_scatter(const EvalResult* __restrict__ results, long n, float* __restrict__ cc,
+                                 int* __restrict__ peak) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const EvalResult r = results[i];
+    if (cc) cc[i] = r.cc;
+    if (peak) { peak[3 * i] = r.peak[0]; peak[3 * i + 1] = r.peak[1]; peak[3 * i + 2] = r.peak[2]; }
+  }
+}
+
+// ------------------------------------------------------------------ per-size dispatch
+template <int N, typename T>
+static emc_status set_attrs() {
+  using C = SearchCfg<N>;
+  EMC_CUDA(cudaFuncSetAttribute(k_search_fwd_xy<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_A));
+  EMC_CUDA(cudaFuncSetAttribute(k_search_z_mul<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_B));
+  EMC_CUDA(cudaFuncSetAttribute(k_search_inv_peak<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_C));
+  return EMC_OK;
+}
+
+// Launches the three passes of one chunk; ev (optional) receives an event record before
+// each pass and after the last one (4 events).
+template <int N, typename T>
+static emc_status launch_chunk(const SearchChunkArgs& a, cudaStream_t st, cudaEvent_t* ev) {
+  using C = SearchCfg<N>;
+  const float2* tw = device_twiddles(N);
+  if (!tw) return EMC_E_CUDA;
+  const int w = 2 * a.radius + 1;
+  if (ev) EMC_CUDA(cudaEventRecord(ev[0], st));
+  k_search_fwd_xy<N, T><<<dim3(N / C::G, a.n_items), C::NT_A, C::SMEM_A, st>>>(a, tw);
+  EMC_LAUNCH_CHECK();
+  if (ev) EMC_CUDA(cudaEventRecord(ev[1], st));
+  k_search_z_mul<N><<<dim3(N, a.n_items), C::NT_BC, C::SMEM_B, st>>>(a, tw);
+  EMC_LAUNCH_CHECK();
+  if (ev) EMC_CUDA(cudaEventRecord(ev[2], st));
+  k_search_inv_peak<N><<<dim3(w, a.n_items), C::NT_BC, C::SMEM_C, st>>>(a, tw);
+  EMC_LAUNCH_CHECK();
+  if (ev) EMC_CUDA(cudaEventRecord(ev[3], st));
+  return EMC_OK;
+}
+
+static bool box_supported(int n) { return n == 64 || n == 96 || n == 128; }
+
+static emc_status launch_chunk_any(int n, int dtype, const SearchChunkArgs& a, cudaStream_t st, cudaEvent_t* ev) {
+  if (dtype == EMC_DTYPE_F32) {
+    switch (n) {
+      case 64: return launch_chunk<64, float>(a, st, ev);
+      case 96: return launch_chunk<96, float>(a, st, ev);
+      case 128: return launch_chunk<128, float>(a, st, ev);
+    }
+  } else {
+    switch (n) {
+      case 64: return launch_chunk<64, __nv_bfloat16>(a, st, ev);
+      case 96: return launch_chunk<96, __nv_bfloat16>(a, st, ev);
+      case 128: return launch_chunk<128, __nv_bfloat16>(a, st, ev);
+    }
+  }
+  set_error("search: box %d not supported (64, 96, 128)", n);
+  return EMC_E_UNSUPPORTED;
+}
+
+static emc_status set_attrs_any(int n, int dtype) {
+  if (dtype == EMC_DTYPE_F32) {
+    switch (n) {
+      case 64: return set_attrs<64, float>();
+      case 96: return set_attrs<96, float>();
+      case 128: return set_attrs<128, float>();
+    }
+  } else {
+    switch (n) {
+      case 64: return set_attrs<64, __nv_bfloat16>();
+      case 96: return set_attrs<96, __nv_bfloat16>();
+      case 128: return set_attrs<128, __nv_bfloat16>();
+    }
+  }
+  return EMC_E_UNSUPPORTED;
+}
+
+static size_t per_eval_scratch(int n, int radius) {
+  const size_t nh = n / 2 + 1;
+  return sizeof(float2) * nh * n * (n + (size_t)(2 * radius + 1));
+}
+
+// Device buffer that grows on demand.
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  emc_status reserve(size_t n) {
+    if (n <= cap) return EMC_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, sizeof(T) * std::max<size_t>(n, 1)) != cudaSuccess) {
+      set_error("search: cudaMalloc(%zu) failed", sizeof(T) * n);
+      return EMC_E_OOM;
+    }
+    cap = n;
+    return EMC_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+__global__ void k_particle_weight(float2* __restrict__ q, const float* __restrict__ wgt, const float* __restrict__ bp,
+                                  long nhalf, int nh, int n, double* __restrict__ energy) {
+  __shared__ double red[32];
+  double e = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nhalf; i += (long)gridDim.x * blockDim.x) {
+    float f = 1.f;
+    if (wgt) f *= wgt[i];
+    if (bp) f *= bp[i];
+    if (i == 0) f = 0.f;
+    float2 v = q[i];
+    v.x *= f;
+    v.y *= f;
+    q[i] = v;
+    const int kx = (int)(i % nh);
+    e += (kx == 0 || 2 * kx == n ? 1.0 : 2.0) * ((double)v.x * v.x + (double)v.y * v.y);
+  }
+  double t = block_sum(e, red);
+  if (threadIdx.x == 0) atomicAdd(energy, t);
+}
+
+}  // namespace emc
+
+// ===================================================================== C-ABI
+struct emc_search_s {
+  struct Ref {
+    void* data = nullptr;
+    float* mask = nullptr;
+    float* wref = nullptr;
+    int n = 0;
+    int dtype = 0;
+  };
+  std::vector<Ref> refs;
+  emc::DevBuf<emc::DevRef> d_refs;
+  bool refs_dirty = true;
+  std::vector<double> dmat;  // [norient][9]
+  emc::DevBuf<double> d_dmat;
+  int norient = 0;
+  int radius = 0, interp = EMC_INTERP_LINEAR, chunk_evals = 0;
+  size_t scratch_budget = 48ull << 20;
+
+  emc::DevBuf<emc::DevParticle> d_parts;
+  emc::DevBuf<emc::EvalItem> d_items;
+  emc::DevBuf<emc::EvalResult> d_results;
+  emc::DevBuf<unsigned long long> d_best_keys;
+  emc::DevBuf<float2> s1, s2;
+  emc::DevBuf<emc::EvalStats> stats;
+  emc::DevBuf<unsigned long long> keys;
+
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<char> gkey;
+  long last_launches = 0;
+
+  // profiling: a ring of per-chunk event sets, harvested before reuse
+  bool profiling = false;
+  static constexpr int kRing = 64;
+  cudaEvent_t ev[kRing][5] = {};
+  bool ev_pending[kRing] = {};
+  int ev_next = 0;
+  double prof_ms[4] = {0, 0, 0, 0};
+  long prof_launches[4] = {0, 0, 0, 0};
+  long prof_evals = 0;
+};
+
+namespace {
+
+struct Chunk {
+  int n, dtype;
+  long item_offset;
+  int count;
+};
+
+int effective_radius(const emc_search_s* s, int n) {
+  int r = s->radius > 0 ? s->radius : std::max(1, n / 8);
+  return std::min(r, n / 2 - 1);
+}
+
+}  // namespace
+
+extern "C" {
+
+emc_status emc_search_create(emc_search_t* out) {
+  EMC_CHECK_ARG(out, "emc_search_create: null argument");
+  emc_search_s* s = new (std::nothrow) emc_search_s();
+  EMC_CHECK_ARG(s, "emc_search_create: host allocation failed");
+  if (cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete s;
+    emc::set_error("emc_search_create: stream creation failed");
+    return EMC_E_CUDA;
+  }
+  *out = s;
+  return EMC_OK;
+}
+
+emc_status emc_search_add_reference(emc_search_t s, const float* d_ref, int n, const float* d_mask, const float* d_wref,
+                                    int store_dtype, int* ref_id, void* stream) {
+  EMC_CHECK_ARG(s && d_ref && ref_id, "emc_search_add_reference: null argument");
+  EMC_CHECK_ARG(emc::box_supported(n), "emc_search_add_reference: box %d not supported (64, 96, 128)", n);
+  EMC_CHECK_ARG(store_dtype == EMC_DTYPE_F32 || store_dtype == EMC_DTYPE_BF16, "emc_search_add_reference: dtype");
+  cudaStream_t st = emc::as_stream(stream);
+  emc_search_s::Ref r;
+  r.n = n;
+  r.dtype = store_dtype;
+  const long nv = (long)n * n * n, nhalf = (long)(n / 2 + 1) * n * n;
+  const size_t vb = nv * (store_dtype == EMC_DTYPE_F32 ? 4 : 2);
+  EMC_CUDA(cudaMalloc(&r.data, vb));
+  if (store_dtype == EMC_DTYPE_F32) {
+    EMC_CUDA(cudaMemcpyAsync(r.data, d_ref, vb, cudaMemcpyDeviceToDevice, st));
+  } else {
+    EMC_TRY(emc::to_bf16(d_ref, reinterpret_cast<__nv_bfloat16*>(r.data), nv, st));
+  }
+  if (d_mask) {
+    EMC_CUDA(cudaMalloc(&r.mask, nv * sizeof(float)));
+    EMC_CUDA(cudaMemcpyAsync(r.mask, d_mask, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  }
+  if (d_wref) {
+    EMC_CUDA(cudaMalloc(&r.wref, nhalf * sizeof(float)));
+    EMC_CUDA(cudaMemcpyAsync(r.wref, d_wref, nhalf * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  }
+  EMC_TRY(emc::set_attrs_any(n, store_dtype));
+  if (!emc::device_twiddles(n)) return EMC_E_CUDA;
+  s->refs.push_back(r);
+  s->refs_dirty = true;
+  *ref_id = (int)s->refs.size() - 1;
+  return EMC_OK;
+}
+
+emc_status emc_search_set_orientations(emc_search_t s, const double* ptp, int n) {
+  EMC_CHECK_ARG(s && ptp && n > 0, "emc_search_set_orientations: bad argument");
+  s->dmat.assign((size_t)n * 9, 0.0);
+  for (int o = 0; o < n; ++o) {
+    const double ang[3] = {ptp[3 * o], ptp[3 * o + 1], ptp[3 * o + 2] - ptp[3 * o]};
+    EMC_TRY(emc_define_matrix(ang, 1, &s->dmat[(size_t)o * 9]));
+  }
+  EMC_TRY(s->d_dmat.reserve(s->dmat.size()));
+  EMC_CUDA(cudaMemcpy(s->d_dmat.p, s->dmat.data(), sizeof(double) * s->dmat.size(), cudaMemcpyHostToDevice));
+  s->norient = n;
+  s->gkey.clear();  // invalidate the cached graph
+  return EMC_OK;
+}
+
+emc_status emc_search_configure(emc_search_t s, int peak_radius, int interp, int chunk_evals) {
+  EMC_CHECK_ARG(s, "emc_search_configure: null handle");
+  EMC_CHECK_ARG(peak_radius >= 0 && peak_radius < 64, "emc_search_configure: peak radius %d", peak_radius);
+  EMC_CHECK_ARG(interp >= 0 && interp <= 2, "emc_search_configure: interp %d", interp);
+  EMC_CHECK_ARG(chunk_evals >= 0, "emc_search_configure: chunk_evals %d", chunk_evals);
+  s->radius = peak_radius;
+  s->interp = interp;
+  s->chunk_evals = chunk_evals;
+  s->gkey.clear();
+  return EMC_OK;
+}
+
+// Adds the elapsed times of a finished event set to the profile totals.
+static emc_status harvest_slot(emc_search_t s, int slot) {
+  if (!s->ev_pending[slot]) return EMC_OK;
+  EMC_CUDA(cudaEventSynchronize(s->ev[slot][4]));
+  for (int k = 0; k < 4; ++k) {
+    float ms = 0.f;
+    EMC_CUDA(cudaEventElapsedTime(&ms, s->ev[slot][k], s->ev[slot][k + 1]));
+    s->prof_ms[k] += ms;
+  }
+  s->ev_pending[slot] = false;
+  return EMC_OK;
+}
+
+static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks, int np, long total_evals,
+                                float* d_cc, int* d_peak, emc_search_hit* d_best, cudaStream_t st) {
+  EMC_CUDA(cudaMemsetAsync(s->d_best_keys.p, 0, sizeof(unsigned long long) * np, st));
+  long launches = 0;
+  for (const Chunk& c : chunks) {
+    emc::SearchChunkArgs a;
+    a.items = s->d_items.p + c.item_offset;
+    a.parts = s->d_parts.p;
+    a.refs = s->d_refs.p;
+    a.dmat = s->d_dmat.p;
+    a.s1 = s->s1.p;
+    a.s2 = s->s2.p;
+    a.stats = s->stats.p;
+    a.keys = s->keys.p;
+    a.n_items = c.count;
+    a.radius = effective_radius(s, c.n);
+    a.interp = s->interp;
+    EMC_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(emc::EvalStats) * c.count, st));
+    EMC_CUDA(cudaMemsetAsync(s->keys.p, 0, sizeof(unsigned long long) * c.count, st));
+    cudaEvent_t* ev = nullptr;
+    if (s->profiling) {
+      const int slot = s->ev_next;
+      s->ev_next = (s->ev_next + 1) % emc_search_s::kRing;
+      EMC_TRY(harvest_slot(s, slot));
+      ev = s->ev[slot];
+      s->ev_pending[slot] = true;
+    }
+    EMC_TRY(emc::launch_chunk_any(c.n, c.dtype, a, st, ev));
+    emc::k_search_decode<<<(c.count + 255) / 256, 256, 0, st>>>(a, c.n, s->d_results.p, s->d_best_keys.p);
+    EMC_LAUNCH_CHECK();
+    if (ev) EMC_CUDA(cudaEventRecord(ev[4], st));
+    launches += 4;
+    if (s->profiling) {
+      for (int k = 0; k < 4; ++k) s->prof_launches[k] += 1;
+      s->prof_evals += c.count;
+    }
+  }
+  if (d_best) {
+    emc::k_search_best<<<(np + 127) / 128, 128, 0, st>>>(s->d_parts.p, np, s->d_results.p, s->d_best_keys.p, d_best);
+    EMC_LAUNCH_CHECK();
+    ++launches;
+  }
+  if (d_cc || d_peak) {
+    const int blocks = (int)std::min<long>((total_evals + 255) / 256, 4L * emc::device_sm_count());
+    emc::k_search_scatter<<<std::max(blocks, 1), 256, 0, st>>>(s->d_results.p, total_evals, d_cc, d_peak);
+    EMC_LAUNCH_CHECK();
+    ++launches;
+  }
+  s->last_launches = launches;
+  return EMC_OK;
+}
+
+emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, int np, float* d_cc, int* d_peak,
+                          emc_search_hit* d_best, void* stream) {
+  EMC_CHECK_ARG(s && particles && np > 0, "emc_search_run: bad argument");
+  EMC_CHECK_ARG(s->norient > 0, "emc_search_run: no orientations set");
+  cudaStream_t st = emc::as_stream(stream);
+  // ---- validate and build the particle table
+  std::vector<emc::DevParticle> parts(np);
+  long total = 0;
+  for (int p = 0; p < np; ++p) {
+    const emc_particle_desc& d = particles[p];
+    EMC_CHECK_ARG(d.spectrum, "particle %d: null spectrum", p);
+    EMC_CHECK_ARG(d.ref_id >= 0 && d.ref_id < (int)s->refs.size(), "particle %d: bad ref_id %d", p, d.ref_id);
+    EMC_CHECK_ARG(s->refs[d.ref_id].n == d.box, "particle %d: box %d does not match reference box %d", p, d.box,
+                  s->refs[d.ref_id].n);
+    EMC_CHECK_ARG(d.orient_begin >= 0 && d.orient_count >= 0 && d.orient_begin + d.orient_count <= s->norient,
+                  "particle %d: orientation slice [%d, %d) outside [0, %d)", p, d.orient_begin,
+                  d.orient_begin + d.orient_count, s->norient);
+    EMC_CHECK_ARG(d.energy > 0.0, "particle %d: energy must be > 0", p);
+    emc::DevParticle& q = parts[p];
+    q.spec = reinterpret_cast<const float2*>(d.spectrum);
+    q.energy = d.energy;
+    memcpy(q.prior, d.prior, sizeof(q.prior));
+    memcpy(q.shift, d.shift, sizeof(q.shift));
+    q.ref = d.ref_id;
+    q.box = d.box;
+    q.orient_begin = d.orient_begin;
+    q.eval_base = total;
+    total += d.orient_count;
+  }
+  EMC_CHECK_ARG(total > 0, "emc_search_run: no (particle, orientation) pairs");
+  // ---- cache key: request content + outputs + settings
+  std::vector<char> key(sizeof(emc_particle_desc) * np + 64);
+  memcpy(key.data(), particles, sizeof(emc_particle_desc) * np);
+  {
+    char* k = key.data() + sizeof(emc_particle_desc) * np;
+    memcpy(k, &d_cc, 8); memcpy(k + 8, &d_peak, 8); memcpy(k + 16, &d_best, 8);
+    memcpy(k + 24, &s->radius, 4); memcpy(k + 28, &s->interp, 4); memcpy(k + 32, &s->chunk_evals, 4);
+    memcpy(k + 36, &s->norient, 4);
+    const size_t nref = s->refs.size();
+    memcpy(k + 40, &nref, 8);
+    memcpy(k + 48, &st, 8);
+    memset(k + 56, 0, 8);
+  }
+  if (!s->profiling && !s->gkey.empty() && s->gkey == key && s->gexec && !s->refs_dirty) {
+    EMC_CUDA(cudaGraphLaunch(s->gexec, st));
+    return EMC_OK;
+  }
+  // ---- group pairs by (box, dtype) and cut chunks
+  std::vector<emc::EvalItem> items;
+  items.reserve(total);
+  std::vector<Chunk> chunks;
+  size_t max_chunk_bytes = 0;
+  int max_chunk = 0;
+  for (int n : {64, 96, 128})
+    for (int dt : {EMC_DTYPE_F32, EMC_DTYPE_BF16}) {
+      const long begin = (long)items.size();
+      for (int p = 0; p < np; ++p) {
+        if (particles[p].box != n || s->refs[particles[p].ref_id].dtype != dt) continue;
+        for (int k = 0; k < particles[p].orient_count; ++k) items.push_back({p, particles[p].orient_begin + k});
+      }
+      const long cnt = (long)items.size() - begin;
+      if (!cnt) continue;
+      const int r = effective_radius(s, n);
+      const size_t pe = emc::per_eval_scratch(n, r);
+      int e = s->chunk_evals > 0 ? s->chunk_evals : (int)std::max<size_t>(1, s->scratch_budget / pe);
+      e = (int)std::min<long>(e, 65535);
+      for (long off = 0; off < cnt; off += e) {
+        Chunk c{n, dt, begin + off, (int)std::min<long>(e, cnt - off)};
+        chunks.push_back(c);
+        max_chunk_bytes = std::max(max_chunk_bytes, pe * c.count);
+        max_chunk = std::max(max_chunk, c.count);
+      }
+    }
+  // ---- buffers
+  EMC_TRY(s->d_parts.reserve(np));
+  EMC_TRY(s->d_items.reserve(items.size()));
+  EMC_TRY(s->d_results.reserve(total));
+  EMC_TRY(s->d_best_keys.reserve(np));
+  EMC_TRY(s->stats.reserve(max_chunk));
+  EMC_TRY(s->keys.reserve(max_chunk));
+  {
+    // split scratch between S1 and S2 proportionally to the largest chunk of each size
+    size_t s1n = 0, s2n = 0;
+    for (const Chunk& c : chunks) {
+      const size_t nh = c.n / 2 + 1;
+      const int r = effective_radius(s, c.n);
+      s1n = std::max(s1n, (size_t)c.count * c.n * c.n * nh);
+      s2n = std::max(s2n, (size_t)c.count * (2 * r + 1) * c.n * nh);
+    }
+    EMC_TRY(s->s1.reserve(s1n));
+    EMC_TRY(s->s2.reserve(s2n));
+  }
+  if (s->refs_dirty) {
+    std::vector<emc::DevRef> dr(s->refs.size());
+    for (size_t i = 0; i < s->refs.size(); ++i)
+      dr[i] = {s->refs[i].data, s->refs[i].mask, s->refs[i].wref, s->refs[i].n, s->refs[i].dtype};
+    EMC_TRY(s->d_refs.reserve(dr.size()));
+    EMC_CUDA(cudaMemcpy(s->d_refs.p, dr.data(), sizeof(emc::DevRef) * dr.size(), cudaMemcpyHostToDevice));
+    s->refs_dirty = false;
+  }
+  EMC_CUDA(cudaMemcpyAsync(s->d_parts.p, parts.data(), sizeof(emc::DevParticle) * np, cudaMemcpyHostToDevice, st));
+  EMC_CUDA(cudaMemcpyAsync(s->d_items.p, items.data(), sizeof(emc::EvalItem) * items.size(), cudaMemcpyHostToDevice,
+                           st));
+  // host vectors must outlive the async copies
+  EMC_CUDA(cudaStreamSynchronize(st));
+  if (s->profiling) {
+    s->gkey.clear();
+    return search_record(s, chunks, np, total, d_cc, d_peak, d_best, st);
+  }
+  // ---- capture the launch sequence into a graph, then launch it
+  if (s->gexec) {
+    cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+  }
+  s->gkey.clear();
+  EMC_CUDA(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
+  emc_status rs = search_record(s, chunks, np, total, d_cc, d_peak, d_best, s->cap_stream);
+  cudaGraph_t graph = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(s->cap_stream, &graph);
+  if (rs != EMC_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rs;
+  }
+  if (ce != cudaSuccess) {
+    emc::set_error("emc_search_run: graph capture failed: %s", cudaGetErrorString(ce));
+    return EMC_E_CUDA;
+  }
+  ce = cudaGraphInstantiate(&s->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) {
+    emc::set_error("emc_search_run: graph instantiation failed: %s", cudaGetErrorString(ce));
+    s->gexec = nullptr;
+    return EMC_E_CUDA;
+  }
+  s->gkey = key;
+  EMC_CUDA(cudaGraphLaunch(s->gexec, st));
+  return EMC_OK;
+}
+
+emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particles, int np, float* h_cc, int* h_peak,
+                               emc_search_hit* h_best, void* stream) {
+  EMC_CHECK_ARG(s && particles && np > 0, "emc_search_run_host: bad argument");
+  cudaStream_t st = emc::as_stream(stream);
+  long total = 0;
+  for (int p = 0; p < np; ++p) total += particles[p].orient_count;
+  float* d_cc = nullptr;
+  int* d_peak = nullptr;
+  emc_search_hit* d_best = nullptr;
+  emc_status rs = EMC_OK;
+  if (h_cc && cudaMalloc(&d_cc, sizeof(float) * std::max<long>(total, 1)) != cudaSuccess) rs = EMC_E_OOM;
+  if (rs == EMC_OK && h_peak && cudaMalloc(&d_peak, sizeof(int) * 3 * std::max<long>(total, 1)) != cudaSuccess)
+    rs = EMC_E_OOM;
+  if (rs == EMC_OK && h_best && cudaMalloc(&d_best, sizeof(emc_search_hit) * np) != cudaSuccess) rs = EMC_E_OOM;
+  if (rs == EMC_OK) rs = emc_search_run(s, particles, np, d_cc, d_peak, d_best, stream);
+  if (rs == EMC_OK && h_cc && cudaMemcpyAsync(h_cc, d_cc, sizeof(float) * total, cudaMemcpyDeviceToHost, st))
+    rs = EMC_E_CUDA;
+  if (rs == EMC_OK && h_peak &&
+      cudaMemcpyAsync(h_peak, d_peak, sizeof(int) * 3 * total, cudaMemcpyDeviceToHost, st))
+    rs = EMC_E_CUDA;
+  if (rs == EMC_OK && h_best &&
+      cudaMemcpyAsync(h_best, d_best, sizeof(emc_search_hit) * np, cudaMemcpyDeviceToHost, st))
+    rs = EMC_E_CUDA;
+  if (rs == EMC_OK && cudaStreamSynchronize(st) != cudaSuccess) rs = EMC_E_CUDA;
+  if (rs == EMC_E_OOM) emc::set_error("emc_search_run_host: device allocation failed");
+  if (rs == EMC_E_CUDA) emc::set_error("emc_search_run_host: copy back failed");
+  cudaFree(d_cc);
+  cudaFree(d_peak);
+  cudaFree(d_best);
+  // the graph was recorded with these temporary outputs: do not replay it
+  s->gkey.clear();
+  return rs;
+}
+
+emc_status emc_search_set_profiling(emc_search_t s, int enable) {
+  EMC_CHECK_ARG(s, "emc_search_set_profiling: null handle");
+  if (enable && !s->ev[0][0]) {
+    for (int i = 0; i < emc_search_s::kRing; ++i)
+      for (int k = 0; k < 5; ++k) EMC_CUDA(cudaEventCreate(&s->ev[i][k]));
+  }
+  s->profiling = enable != 0;
+  return EMC_OK;
+}
+
+emc_status emc_search_timings(emc_search_t s, double ms[4], long launches[4], long* evals, long* launches_last_run,
+                              int reset) {
+  EMC_CHECK_ARG(s, "emc_search_timings: null handle");
+  for (int i = 0; i < emc_search_s::kRing; ++i) EMC_TRY(harvest_slot(s, i));
+  for (int k = 0; k < 4; ++k) {
+    if (ms) ms[k] = s->prof_ms[k];
+    if (launches) launches[k] = s->prof_launches[k];
+  }
+  if (evals) *evals = s->prof_evals;
+  if (launches_last_run) *launches_last_run = s->last_launches;
+  if (reset) {
+    for (int k = 0; k < 4; ++k) {
+      s->prof_ms[k] = 0;
+      s->prof_launches[k] = 0;
+    }
+    s->prof_evals = 0;
+  }
+  return EMC_OK;
+}
+
+emc_status emc_search_destroy(emc_search_t s) {
+  if (!s) return EMC_OK;
+  for (int i = 0; i < emc_search_s::kRing; ++i)
+    for (int k = 0; k < 5; ++k)
+      if (s->ev[i][k]) cudaEventDestroy(s->ev[i][k]);
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  for (auto& r : s->refs) {
+    cudaFree(r.data);
+    cudaFree(r.mask);
+    cudaFree(r.wref);
+  }
+  s->d_refs.release();
+  s->d_dmat.release();
+  s->d_parts.release();
+  s->d_items.release();
+  s->d_results.release();
+  s->d_best_keys.release();
+  s->s1.release();
+  s->s2.release();
+  s->stats.release();
+  s->keys.release();
+  if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+  delete s;
+  return EMC_OK;
+}
+
+emc_status emc_particle_spectrum(int n, const float* d_particle, const float* d_weight, const float* d_bandpass,
+                                 float* d_spectrum_out, double* d_energy, void* stream) {
+  EMC_CHECK_ARG(d_particle && d_spectrum_out && d_energy, "emc_particle_spectrum: null argument");
+  EMC_CHECK_ARG(emc::fft_length_supported(n) && n >= 2, "emc_particle_spectrum: box %d not supported", n);
+  cudaStream_t st = emc::as_stream(stream);
+  float2* q = reinterpret_cast<float2*>(d_spectrum_out);
+  EMC_TRY(emc::fft3_r2c(d_particle, q, n, n, n, 1, st));
+  EMC_CUDA(cudaMemsetAsync(d_energy, 0, sizeof(double), st));
+  const long nhalf = (long)(n / 2 + 1) * n * n;
+  const int blocks = (int)std::min<long>((nhalf + 255) / 256, 2L * emc::device_sm_count());
+  emc::k_particle_weight<<<blocks, 256, 0, st>>>(q, d_weight, d_bandpass, nhalf, n / 2 + 1, n, d_energy);
+  EMC_LAUNCH_CHECK();
+  return EMC_OK;
+}
+
+emc_status emc_particle_template(int n, const float* d_spectrum, float* d_h, void* stream) {
+  EMC_CHECK_ARG(d_spectrum && d_h, "emc_particle_template: null argument");
+  EMC_CHECK_ARG(emc::fft_length_supported(n) && n >= 2, "emc_particle_template: box %d not supported", n);
+  cudaStream_t st = emc::as_stream(stream);
+  const size_t nhalf = (size_t)(n / 2 + 1) * n * n;
+  float2* scratch = nullptr;
+  EMC_CUDA(cudaMallocAsync(&scratch, nhalf * sizeof(float2), st));
+  emc_status rs = emc::fft3_c2r(reinterpret_cast<const float2*>(d_spectrum), d_h, scratch, n, n, n, 1, st);
+  cudaFreeAsync(scratch, st);
+  return rs;
+}
+
+}  // extern "C"
+
+// Read access to a registered reference (used by the adjoint entry point).
+emc_status emc_search_reference_info(emc_search_t s, int ref_id, const void** data, const float** mask, int* n,
+                                     int* dtype) {
+  EMC_CHECK_ARG(s && data && mask && n && dtype, "emc_search_reference_info: null argument");
+  EMC_CHECK_ARG(ref_id >= 0 && ref_id < (int)s->refs.size(), "reference id %d not registered", ref_id);
+  const auto& r = s->refs[ref_id];
+  *data = r.data;
+  *mask = r.mask;
+  *n = r.n;
+  *dtype = r.dtype;
+  return EMC_OK;
+}

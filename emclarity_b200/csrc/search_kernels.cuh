@@ -1,0 +1,366 @@
+// search_kernels.cuh -- the three fused passes of one CC evaluation (particle, orientation).
+//
+// Data flow per evaluation e (box n, half width nh = n/2+1, peak radius r, window w = 2r+1):
+//   pass A  (CTA = G z-planes)   gather r = mask .* I(M (p - c - t) + c)  -> smem
+//                                FP64 sums of r and r^2 (DC-free energy by Parseval)
+//                                R2C along x (two rows per complex FFT), FFT along y
+//                                -> S1[e][z][y][kx]                         (n * n * nh c64)
+//   pass B  (CTA = one ky row)   FFT along z, X = Q .* conj(wref .* R), X(0) = 0,
+//                                inverse FFT along z, keep the w output planes |sz| <= r
+//                                -> S2[e][j][ky][kx]                        (w * n * nh c64)
+//   pass C  (CTA = one sz plane) inverse FFT along y, C2R along x for the w rows |sy| <= r,
+//                                normalise by sqrt(E_R E_P), spherical peak mask,
+//                                argmax -> atomicMax on a 64-bit (cc, -index) key
+// The reference computes the whole map (BH_multi_xcf_Translational_2.m:35-38) and then
+// masks it (BH_multi_xcf_Translational.m:33-42); only the masked window is evaluated here.
+#pragma once
+#include "interp.cuh"
+
+namespace emc {
+
+struct DevParticle {
+  const float2* spec;  // Q, [z][y][kx]
+  double energy;       // E_P
+  double prior[9];     // column-major
+  float shift[3];
+  int ref;
+  int box;
+  int orient_begin;
+  long eval_base;      // index of this particle's first (p, o) pair in the output order
+};
+
+struct DevRef {
+  const void* data;    // n^3, float or bf16
+  const float* mask;   // n^3 or null
+  const float* wref;   // nh*n*n or null
+  int n;
+  int dtype;
+};
+
+struct EvalItem {
+  int particle;
+  int orient;          // global orientation index
+};
+
+struct EvalStats {
+  double sum_r, sum_r2, energy_spec, pad;
+};
+
+struct SearchChunkArgs {
+  const EvalItem* items;     // [E]
+  const DevParticle* parts;
+  const DevRef* refs;
+  const double* dmat;        // [norient][9] column-major defineMatrix([phi,theta,psi-phi],'inv')
+  float2* s1;                // [E][n][n][nh]
+  float2* s2;                // [E][w][n][nh]
+  EvalStats* stats;          // [E]
+  unsigned long long* keys;  // [E]
+  int n_items;
+  int radius;
+  int interp;
+};
+
+// Sampling matrix rows of RotMat' with RotMat = prior * D (FP64 composition).
+__device__ __forceinline__ void compose_sampling_matrix(const double* prior, const double* d, float m[9]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      // RotMat(j, i) = sum_k prior(j, k) D(k, i)
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc = fma(prior[j + 3 * k], d[k + 3 * i], acc);
+      m[3 * i + j] = (float)acc;
+    }
+}
+
+template <int N>
+struct SearchCfg {
+  static constexpr int NH = N / 2 + 1;
+  static constexpr int P = team_size(N);
+  static constexpr int G = N <= 64 ? 4 : (N <= 96 ? 2 : 1);  // planes per pass-A CTA
+  static constexpr int NT_A = 256;
+  static constexpr int TEAMS_A = NT_A / P;
+  static constexpr int NT_BC = ((NH * P + 31) / 32) * 32;
+  static constexpr int TEAMS_BC = NT_BC / P;
+  static constexpr size_t SMEM_A = sizeof(float2) * ((size_t)G * N * NH + (size_t)TEAMS_A * (N + 1) + N) + 64;
+  static constexpr size_t SMEM_B = sizeof(float2) * ((size_t)N * NH + N);
+  static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)N * NH + N + (size_t)TEAMS_BC * (N + 1));
+};
+
+template <typename Tv>
+__device__ __forceinline__ Tv block_sum(Tv v, Tv* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  Tv t = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  return t;  // valid in thread 0
+}
+
+// ------------------------------------------------------------------ pass A
+template <int N, typename T>
+__global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const SearchChunkArgs a,
+                                                                       const float2* __restrict__ g_tw) {
+  using C = SearchCfg<N>;
+  constexpr int NH = C::NH, G = C::G, P = C::P;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* planes = reinterpret_cast<float2*>(smem_raw);          // [G][N][NH]
+  float2* lines = planes + (size_t)G * N * NH;                    // [TEAMS][N+1]
+  float2* s_tw = lines + (size_t)C::TEAMS_A * (N + 1);             // [N]
+  float* s_m = reinterpret_cast<float*>(s_tw + N);                // 9 floats
+  __shared__ double red[2][32];
+
+  const int e = blockIdx.y;
+  if (e >= a.n_items) return;
+  const int z0 = blockIdx.x * G;
+  const EvalItem it = a.items[e];
+  const DevParticle& pt = a.parts[it.particle];
+  const DevRef rf = a.refs[pt.ref];
+  const T* __restrict__ src = reinterpret_cast<const T*>(rf.data);
+  const float* __restrict__ mask = rf.mask;
+
+  load_twiddles<N>(s_tw, g_tw);
+  if (threadIdx.x == 0) compose_sampling_matrix(pt.prior, a.dmat + 9L * it.orient, s_m);
+  __syncthreads();
+  float m[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) m[i] = s_m[i];
+  const float tx = pt.shift[0], ty = pt.shift[1], tz = pt.shift[2];
+  constexpr int c = N / 2;
+
+  // 1. gather (x fastest: a warp walks 32 consecutive voxels of one row)
+  double s1 = 0.0, s2 = 0.0;
+  float* fplanes = reinterpret_cast<float*>(planes);
+  for (int idx = threadIdx.x; idx < G * N * N; idx += C::NT_A) {
+    const int x = idx % N, y = (idx / N) % N, zl = idx / (N * N);
+    const int z = z0 + zl;
+    const float u = (float)(x - c) - tx, v = (float)(y - c) - ty, w = (float)(z - c) - tz;
+    const float sx = fmaf(m[0], u, fmaf(m[1], v, m[2] * w)) + (float)c;
+    const float sy = fmaf(m[3], u, fmaf(m[4], v, m[5] * w)) + (float)c;
+    const float sz = fmaf(m[6], u, fmaf(m[7], v, m[8] * w)) + (float)c;
+    float val = sample(a.interp, src, N, N, N, sx, sy, sz);
+    if (mask) val *= __ldg(mask + ((long)z * N + y) * N + x);
+    fplanes[((size_t)zl * N + y) * (2 * NH) + x] = val;
+    s1 += (double)val;
+    s2 += (double)val * (double)val;
+  }
+  {
+    double t1 = block_sum(s1, red[0]);
+    double t2 = block_sum(s2, red[1]);
+    if (threadIdx.x == 0) {
+      atomicAdd(&a.stats[e].sum_r, t1);
+      atomicAdd(&a.stats[e].sum_r2, t2);
+    }
+  }
+  __syncthreads();
+
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  // 2. R2C along x: rows 2q and 2q+1 of the slab share one complex FFT
+  {
+    constexpr int NPAIRS = G * N / 2;
+    float2* buf = lines + (size_t)team * (N + 1);
+    for (int base = 0; base < NPAIRS; base += C::TEAMS_A) {
+      const int q = base + team;
+      const bool active = q < NPAIRS;
+      const float* ra = fplanes + (size_t)(2 * q) * (2 * NH);
+      const float* rb = ra + 2 * NH;
+      if (active)
+        for (int n = lane; n < N; n += P) buf[n] = make_float2(ra[n], rb[n]);
+      __syncwarp();
+      fft_line<N, -1, P>(buf, 1, lane, s_tw, active);
+      if (active) {
+        float2* oa = planes + (size_t)(2 * q) * NH;
+        float2* ob = oa + NH;
+        for (int k = lane; k < NH; k += P) {
+          const float2 zk = buf[k], zm = buf[(N - k) % N];
+          oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+          ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // 3. FFT along y for every (plane, kx) column
+  {
+    constexpr int NLINES = G * NH;
+    for (int base = 0; base < NLINES; base += C::TEAMS_A) {
+      const int li = base + team;
+      const bool active = li < NLINES;
+      const int zl = active ? li / NH : 0, kx = active ? li % NH : 0;
+      fft_line<N, -1, P>(planes + (size_t)zl * N * NH + kx, NH, lane, s_tw, active);
+    }
+  }
+  __syncthreads();
+  // 4. store the slab (contiguous in S1)
+  {
+    float4* dst = reinterpret_cast<float4*>(a.s1 + ((size_t)e * N + z0) * N * NH);
+    const float4* srcv = reinterpret_cast<const float4*>(planes);
+    constexpr int NV = G * N * NH / 2;  // float2 pairs; G*N*NH is even because N is even
+    for (int i = threadIdx.x; i < NV; i += C::NT_A) dst[i] = srcv[i];
+  }
+}
+
+// ------------------------------------------------------------------ pass B
+template <int N>
+__global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const SearchChunkArgs a,
+                                                                       const float2* __restrict__ g_tw) {
+  using C = SearchCfg<N>;
+  constexpr int NH = C::NH, P = C::P;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tile = reinterpret_cast<float2*>(smem_raw);  // [N (z)][NH]
+  float2* s_tw = tile + (size_t)N * NH;
+  __shared__ double red[32];
+
+  const int e = blockIdx.y;
+  if (e >= a.n_items) return;
+  const int ky = blockIdx.x;
+  const EvalItem it = a.items[e];
+  const DevParticle& pt = a.parts[it.particle];
+  const float* __restrict__ wref = a.refs[pt.ref].wref;
+  const float2* __restrict__ q = pt.spec;
+  const int w = 2 * a.radius + 1;
+
+  load_twiddles<N>(s_tw, g_tw);
+  const float2* src = a.s1 + (size_t)e * N * N * NH + (size_t)ky * NH;
+  for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) {
+    const int z = i / NH, kx = i % NH;
+    tile[i] = src[(size_t)z * N * NH + kx];
+  }
+  __syncthreads();
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  for (int base = 0; base < NH; base += C::TEAMS_BC) {
+    const int kx = base + team;
+    fft_line<N, -1, P>(tile + (kx < NH ? kx : 0), NH, lane, s_tw, kx < NH);
+  }
+  __syncthreads();
+  double en = 0.0;
+  for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) {
+    const int z = i / NH, kx = i % NH;
+    const size_t gi = ((size_t)z * N + ky) * NH + kx;
+    float2 r = tile[i];
+    if (wref) {
+      const float wv = __ldg(wref + gi);
+      r.x *= wv;
+      r.y *= wv;
+      if (gi != 0) en += (kx == 0 || 2 * kx == N ? 1.0 : 2.0) * ((double)r.x * r.x + (double)r.y * r.y);
+    }
+    float2 x = cmulc(__ldg(q + gi), r);
+    if (gi == 0) x = make_float2(0.f, 0.f);
+    tile[i] = x;
+  }
+  if (wref) {
+    double t = block_sum(en, red);
+    if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
+  }
+  __syncthreads();
+  for (int base = 0; base < NH; base += C::TEAMS_BC) {
+    const int kx = base + team;
+    fft_line<N, 1, P>(tile + (kx < NH ? kx : 0), NH, lane, s_tw, kx < NH);
+  }
+  __syncthreads();
+  float2* dst = a.s2 + (size_t)e * w * N * NH + (size_t)ky * NH;
+  for (int i = threadIdx.x; i < w * NH; i += C::NT_BC) {
+    const int j = i / NH, kx = i % NH;
+    const int z = (j - a.radius + N) % N;
+    dst[(size_t)j * N * NH + kx] = tile[(size_t)z * NH + kx];
+  }
+}
+
+// ------------------------------------------------------------------ pass C
+template <int N>
+__global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const SearchChunkArgs a,
+                                                                          const float2* __restrict__ g_tw) {
+  using C = SearchCfg<N>;
+  constexpr int NH = C::NH, P = C::P;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tile = reinterpret_cast<float2*>(smem_raw);   // [N (y)][NH]
+  float2* s_tw = tile + (size_t)N * NH;
+  float2* lines = s_tw + N;                              // [TEAMS][N+1]
+  __shared__ unsigned long long s_best;
+
+  const int e = blockIdx.y;
+  if (e >= a.n_items) return;
+  const int j = blockIdx.x;
+  const int r = a.radius, w = 2 * r + 1;
+  const int sz = j - r;
+  const EvalItem it = a.items[e];
+  const DevParticle& pt = a.parts[it.particle];
+  const bool has_wref = a.refs[pt.ref].wref != nullptr;
+
+  load_twiddles<N>(s_tw, g_tw);
+  if (threadIdx.x == 0) s_best = 0ull;
+  const float2* src = a.s2 + ((size_t)e * w + j) * N * NH;
+  for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) tile[i] = src[i];
+  __syncthreads();
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  for (int base = 0; base < NH; base += C::TEAMS_BC) {
+    const int kx = base + team;
+    fft_line<N, 1, P>(tile + (kx < NH ? kx : 0), NH, lane, s_tw, kx < NH);
+  }
+  __syncthreads();
+
+  const EvalStats st = a.stats[e];
+  const double er = has_wref ? st.energy_spec : ((double)N * N * N * st.sum_r2 - st.sum_r * st.sum_r);
+  const double denom = er * pt.energy;
+  const float inv_norm = denom > 0.0 ? (float)(1.0 / sqrt(denom)) : 0.f;
+  constexpr int c = N / 2;
+
+  unsigned long long best = 0ull;
+  const int npairs = (w + 1) / 2;
+  float2* buf = lines + (size_t)team * (N + 1);
+  for (int base = 0; base < npairs; base += C::TEAMS_BC) {
+    const int pr = base + team;
+    const bool active = pr < npairs;
+    const int ja = 2 * pr, jb = 2 * pr + 1;
+    const bool has_b = jb < w;
+    const int ya = (ja - r + N) % N, yb = has_b ? (jb - r + N) % N : ya;
+    if (active) {
+      const float2* ra = tile + (size_t)ya * NH;
+      const float2* rb = tile + (size_t)yb * NH;
+      for (int n = lane; n < N; n += P) {
+        const bool lower = n <= N / 2;
+        const int k = lower ? n : N - n;
+        float2 A = ra[k];
+        float2 B = has_b ? rb[k] : make_float2(0.f, 0.f);
+        if (k == 0 || 2 * k == N) { A.y = 0.f; B.y = 0.f; }
+        if (!lower) { A.y = -A.y; B.y = -B.y; }
+        buf[n] = make_float2(A.x - B.y, A.y + B.x);
+      }
+    }
+    __syncwarp();
+    fft_line<N, 1, P>(buf, 1, lane, s_tw, active);
+    if (active) {
+      for (int t = lane; t < 2 * w; t += P) {
+        const int which = t / w;  // 0: row a, 1: row b
+        if (which == 1 && !has_b) continue;
+        const int sx = (t % w) - r;
+        const int sy = (which ? jb : ja) - r;
+        if (sx * sx + sy * sy + sz * sz > r * r) continue;
+        const float2 zv = buf[(sx + N) % N];
+        const float v = (which ? zv.y : zv.x) * inv_norm;
+        if (v != v) continue;  // NaN never wins (MATLAB max ignores NaN)
+        const unsigned int lin = (unsigned int)(((sz + c) * N + (sy + c)) * N + (sx + c));
+        const unsigned long long key = ((unsigned long long)ordered_key(v) << 32) | (0xffffffffu - lin);
+        best = key > best ? key : best;
+      }
+    }
+    __syncwarp();
+  }
+  // block max
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, o);
+    best = other > best ? other : best;
+  }
+  if ((threadIdx.x & 31) == 0 && best) atomicMax(&s_best, best);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_best) atomicMax(&a.keys[e], s_best);
+}
+
+}  // namespace emc

@@ -1,0 +1,277 @@
+/*
+ * emc_b200.h -- C-ABI of the B200-native orientation-search hot path.
+ *
+ * Every entry point takes plain pointers, sizes and an explicit CUDA stream
+ * (passed as void*; NULL = legacy default stream).  Device buffers are owned
+ * by the caller; the library allocates only inside the opaque handles made by
+ * the *_create / *_plan functions and frees it in the matching *_destroy.
+ * No C++ exception crosses this boundary: every function returns emc_status.
+ *
+ * Conventions shared by all volume functions (they follow the reference):
+ *   - volumes are x-fastest, linear index (z*ny + y)*nx + x
+ *     (reference mexFiles/mexXform3d.cu:86);
+ *   - the rotation origin is floor(n/2) on every axis (mexXform3d.cu:49-51);
+ *   - 3x3 matrices are column-major (MATLAB order), as mexXform3d reads them
+ *     (mexXform3d.cu:170-172);
+ *   - half spectra are (nx/2+1) x ny x nz interleaved complex float, FFT order,
+ *     the cuFFT/MATLAB R2C layout the reference's mexFFT returns
+ *     (mexFiles/mexFFT.cu:96-131).
+ */
+#ifndef EMC_B200_H
+#define EMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define EMC_API __attribute__((visibility("default")))
+#else
+#define EMC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int emc_status;
+#define EMC_OK             0
+#define EMC_E_ARG         -1   /* bad argument (size, null pointer, unsupported combination) */
+#define EMC_E_CUDA        -2   /* a CUDA runtime call failed; see emc_last_error() */
+#define EMC_E_OOM         -3   /* device allocation inside a handle failed */
+#define EMC_E_TIMEOUT     -4   /* a bounded device-side wait gave up */
+#define EMC_E_UNSUPPORTED -5   /* size / mode not compiled into this library */
+
+/* Human-readable text of a status and the last error message of the calling thread. */
+EMC_API const char* emc_status_string(emc_status s);
+EMC_API const char* emc_last_error(void);
+/* Library version string and the compiled FFT edge lengths (for callers that pad). */
+EMC_API const char* emc_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Rotation matrices and search grids (host, FP64)                          */
+/* ------------------------------------------------------------------------ */
+
+/* BH_defineMatrix(angles, 'Bah', direction) (coordinates/BH_defineMatrix.m:85-126).
+ * direction: 0 = 'forward' (angles negated), 1 = 'inv' (order reversed).
+ * R_out: 9 doubles, column-major. */
+EMC_API emc_status emc_define_matrix(const double angles_deg[3], int direction, double R_out[9]);
+
+/* eulerSearch(symmetry, theta_max, theta_step, psi_max, psi_step, ...) grid
+ * (coordinates/eulerSearch.m:38-177), enumerated in the order the alignment
+ * loop walks it (alignment/BH_alignRaw3d_v2.m:1119-1170: theta, then phi, then
+ * psi).  Each orientation is the triple (phi, theta, psi) in degrees, the
+ * rotation passed on is defineMatrix([phi, theta, psi - phi], 'inv').
+ * Call once with out = NULL to get *count, then again with room for 3*count.
+ * symmetry: "C<n>", "D<n>", "O", "I", "I2". theta_max < 0 selects the
+ * bipolar search of the reference. */
+EMC_API emc_status emc_euler_search(const char* symmetry, double theta_max, double theta_step,
+                            double psi_max, double psi_step,
+                            double* out_phi_theta_psi, int* count);
+
+/* ------------------------------------------------------------------------ */
+/* mexXform3d: rotate + shift + interpolate a volume                        */
+/*   replaces mexFiles/mexXform3d.cu:93-324 (create / reuse / destroy) and   */
+/*   the testScripts/interpolator.m handle class (:29-154, :401-408)         */
+/* ------------------------------------------------------------------------ */
+
+typedef struct emc_volume_s* emc_volume_t;
+
+#define EMC_INTERP_LINEAR   0   /* trilinear, interpn(...,'linear',0) semantics: 0 outside [0,n-1] */
+#define EMC_INTERP_CUBIC    1   /* tricubic (Catmull-Rom), 0 outside the volume */
+#define EMC_INTERP_LINEAR_BORDER 2 /* trilinear with zero-valued border voxels, the texture
+                                      cudaAddressModeBorder behaviour of mexXform3d.cu:269-271,
+                                      evaluated with FP32 weights */
+
+#define EMC_DTYPE_F32  0
+#define EMC_DTYPE_BF16 1
+
+/* Copies the source volume (nx*ny*nz floats, device) into a handle-owned
+ * buffer, optionally stored as bf16 (FP32 interpolation either way). */
+EMC_API emc_status emc_xform3d_create(const float* d_src, int nx, int ny, int nz, int store_dtype,
+                              emc_volume_t* out, void* stream);
+/* out[p] = (1/nsym) * sum_s I(M_s (p - c + sh) + c)   with
+ *   fwd != 0 ('forward'): sh = -shift, applied before the rotation
+ *   fwd == 0 ('inv')    : the shift is added after the rotation
+ * (mexXform3d.cu:45-65, :160-168).  R: nsym column-major 3x3 matrices (FP64,
+ * rounded to FP32 as the reference does).  d_out: nx*ny*nz floats. */
+EMC_API emc_status emc_xform3d_apply(emc_volume_t h, const double* R, int nsym, const float shift[3],
+                             int fwd, int interp, float* d_out, void* stream);
+EMC_API emc_status emc_xform3d_destroy(emc_volume_t h);
+
+/* ------------------------------------------------------------------------ */
+/* mexFFT: R2C / C2R 1-, 2- and 3-D transforms, unnormalised                */
+/*   replaces mexFiles/mexFFT.cu:16-239 and fourierTransformer.m:38-159      */
+/* ------------------------------------------------------------------------ */
+
+typedef struct emc_fft_s* emc_fft_t;
+
+/* dims: logical real sizes {nx, ny, nz} (x fastest; unused trailing dims = 1).
+ * Every dim > 1 must be 2^a 3^b and <= 512.  batch >= 1 volumes back to back. */
+EMC_API emc_status emc_fft_plan(int rank, const int dims[3], int batch, emc_fft_t* out);
+/* d_in: nx*ny*nz floats per batch item; d_out: (nx/2+1)*ny*nz complex (float2). */
+EMC_API emc_status emc_fft_r2c(emc_fft_t p, const float* d_in, float* d_out_complex, void* stream);
+/* inverse of the above, unnormalised (like cufftExecC2R); d_in is not modified. */
+EMC_API emc_status emc_fft_c2r(emc_fft_t p, const float* d_in_complex, float* d_out, void* stream);
+EMC_API emc_status emc_fft_destroy(emc_fft_t p);
+
+/* ------------------------------------------------------------------------ */
+/* mexCTF / mexSF3D                                                          */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  float pixel_size;     /* Angstrom */
+  float wavelength;     /* Angstrom */
+  float cs_mm;          /* spherical aberration, mm */
+  float amp_contrast;   /* amplitude contrast fraction (converted to a phase, core_headers.cuh:71-72) */
+  float defocus1;       /* Angstrom, positive = underfocus */
+  float defocus2;       /* Angstrom */
+  float astig_deg;      /* astigmatism angle, degrees from x */
+} emc_ctf_params;
+
+/* mexCTF(half, sq, nX, nY, pix, lambda, Cs, df1, df2, ast, AC[, centred])
+ * (mexFiles/mexCTF.cu:6-121, kernel mexFiles/utils/ctf.cu:12-66).
+ * d_out: (half ? nx/2+1 : nx) * ny floats. */
+EMC_API emc_status emc_ctf2d(const emc_ctf_params* p, int nx, int ny, int half, int squared, int centred,
+                     float* d_out, void* stream);
+/* The exposure-filtered variant (mexFiles/utils/ctf.cu:68-130). */
+EMC_API emc_status emc_ctf2d_exposure(const emc_ctf_params* p, int nx, int ny, int half, int squared,
+                              int centred, float radial_weight, float total_exposure,
+                              float* d_out, void* stream);
+/* mexSF3D(half, sq, size[3], pix[n], lambda[n], Cs[n], df1[n], df2[n], ast[n], AC[n],
+ *         nTilts, tilt[n], exposure[n], occupancy[n]) (mexFiles/mexSF3D.cu:84-302):
+ * sum over tilts of the exposure-weighted CTF^2 inserted on the tilted central
+ * slab.  Host arrays of n_tilts entries; d_out: size[0]*size[1]*size[2] floats,
+ * overwritten.  half must be 0 (the reference only builds the full grid). */
+EMC_API emc_status emc_sf3d(int half, int squared, const unsigned size[3], const float* pix,
+                    const float* wavelength, const float* cs_mm, const float* df1,
+                    const float* df2, const float* astig_deg, const float* amp_contrast,
+                    unsigned n_tilts, const float* tilt_deg, const float* exposure,
+                    const float* occupancy, float* d_out, void* stream);
+
+/* Per-particle Fourier weight on the half spectrum ((n/2+1)*n*n floats, FFT order): the
+ * binary Y-tilt-axis missing wedge of BH_weightMask3d 'binaryWedge' (masking/BH_weightMask3d.m:
+ * 103-120; cones of +/-(90-|tilt|) around kz removed, |kx|,|kz| <= 2 slab kept, zero beyond
+ * Nyquist; the Gaussian smoothing of :124-131 is not applied) times, when ctf != NULL, the CTF
+ * of the 3-D spatial frequency (mexFiles/utils/ctf.cu:45-62; defocus1 used, no astigmatism),
+ * squared when squared != 0. */
+EMC_API emc_status emc_wedge_ctf_weight(int n, float tilt_min_deg, float tilt_max_deg, const emc_ctf_params* ctf,
+                                        int squared, float* d_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Fused orientation search (BH_alignRaw3d_v2.m:1119-1423 inner body,        */
+/* BH_multi_xcf_Translational_2.m:35-38 normalised CC,                        */
+/* BH_multi_xcf_Translational.m:31-42 masked argmax)                          */
+/* ------------------------------------------------------------------------ */
+
+typedef struct emc_search_s* emc_search_t;
+
+/* Particle side of one search item.  spectrum = W .* B .* F(particle) with
+ * F(0) = 0 (BH_bandLimitCenterNormalize.m:48-55 times the particle weight),
+ * as produced by emc_particle_spectrum. */
+typedef struct {
+  const float* spectrum;   /* device, (n/2+1)*n*n complex */
+  double energy;           /* sum over the full spectrum of |spectrum|^2 */
+  double prior[9];         /* column-major R_prior (BH_alignRaw3d_v2.m:1176) */
+  float  shift[3];         /* estPeakCoord applied with the reference rotation */
+  int    box;              /* n: 64, 96 or 128 */
+  int    ref_id;           /* reference registered with emc_search_add_reference */
+  int    orient_begin;     /* slice [begin, begin+count) of the orientation list */
+  int    orient_count;
+} emc_particle_desc;
+
+typedef struct {
+  float cc;                /* normalised CC at the peak */
+  int   orient;            /* orientation index (global index into the list) */
+  int   peak[3];           /* integer peak shift (x, y, z) relative to the origin */
+} emc_search_hit;
+
+/* Q = weight .* bandpass .* fftn(particle) with Q(0) = 0; *energy = sum |Q|^2 over the
+ * full spectrum (Hermitian-weighted, FP64).  weight/bandpass: real half spectra
+ * (n/2+1)*n*n in FFT order, either may be NULL (= 1).  d_energy: one device double. */
+EMC_API emc_status emc_particle_spectrum(int n, const float* d_particle, const float* d_weight,
+                                 const float* d_bandpass, float* d_spectrum_out,
+                                 double* d_energy, void* stream);
+
+EMC_API emc_status emc_search_create(emc_search_t* out);
+/* Registers a reference volume (n^3 floats, device), an optional real-space mask
+ * applied after rotation (n^3, or NULL) and an optional real half-spectrum weight
+ * applied to the rotated reference's spectrum (bandpass; NULL = 1).  store_dtype:
+ * EMC_DTYPE_F32 or EMC_DTYPE_BF16 (mixed precision: interpolation stays FP32). */
+EMC_API emc_status emc_search_add_reference(emc_search_t s, const float* d_ref, int n,
+                                    const float* d_mask, const float* d_wref,
+                                    int store_dtype, int* ref_id, void* stream);
+/* Orientation list: n triples (phi, theta, psi) in degrees; the search rotation of
+ * particle p, orientation o is  RotMat = R_prior(p) * defineMatrix([phi,theta,psi-phi],'inv')
+ * and the reference is sampled through RotMat' with 'forward' semantics
+ * (BH_alignRaw3d_v2.m:1175-1176, :1287-1291).  Composition runs in FP64 on the device. */
+EMC_API emc_status emc_search_set_orientations(emc_search_t s, const double* phi_theta_psi, int n);
+/* Tuning knobs (0 = automatic / autotuned).  peak_radius: spherical peak mask radius in
+ * voxels (the peakMask >= 0.95 region of BH_multi_xcf_Translational.m:34). */
+EMC_API emc_status emc_search_configure(emc_search_t s, int peak_radius, int interp, int chunk_evals);
+/* Runs every (particle, orientation) pair.  d_cc / d_peak (optional, may be NULL):
+ * per-pair outputs in pair order (particle-major, orientations in list order),
+ * d_peak holds 3 ints per pair.  d_best: one hit per particle (stable argmax over its
+ * orientations, first index wins ties, as sortrows(...,-6) at BH_alignRaw3d_v2.m:1423).
+ * All outputs are device memory.  Uneven box sizes are allowed in one call; the
+ * launch sequence is captured in a CUDA graph and replayed on identical calls. */
+EMC_API emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, int n_particles,
+                          float* d_cc, int* d_peak, emc_search_hit* d_best, void* stream);
+/* Same as emc_search_run with host output buffers (copies inside, synchronises). */
+EMC_API emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particles,
+                               int n_particles, float* h_cc, int* h_peak,
+                               emc_search_hit* h_best, void* stream);
+EMC_API emc_status emc_search_destroy(emc_search_t s);
+/* Measurement hook (no counterpart in the reference).  With profiling enabled, emc_search_run
+ * launches eagerly instead of through the graph and brackets each pass launch with CUDA events
+ * on the calling stream.  emc_search_timings returns, summed over all runs since the last
+ * reset, the device time in ms of pass A (rotate + xy R2C), pass B (z FFT, multiply, inverse z),
+ * pass C (inverse xy + peak) and the decode step, their launch counts, and the number of CC
+ * evaluations.  launches_last_run: kernels launched by the most recent run. */
+EMC_API emc_status emc_search_set_profiling(emc_search_t s, int enable);
+EMC_API emc_status emc_search_timings(emc_search_t s, double ms[4], long launches[4], long* evals,
+                                      long* launches_last_run, int reset);
+
+/* ------------------------------------------------------------------------ */
+/* Forward + adjoint of the masked CC w.r.t. 3 Euler angles and 3 shifts      */
+/* ------------------------------------------------------------------------ */
+
+/* For each of n poses (phi, theta, psi in degrees; tx, ty, tz in voxels), evaluates
+ *   CC = sum_p r(p) h(p) / sqrt(E_R E_P)
+ * with r = mask .* I(M (p - c - t) + c) the rotated, shifted reference (tricubic),
+ * M = (R_prior * defineMatrix([phi,theta,psi-phi],'inv'))', h = unnormalised
+ * inverse transform of the particle spectrum and E_R the DC-free reference energy,
+ * i.e. the zero-lag value of the normalised CC map of the search, and its exact
+ * gradient (dCC/dphi, dtheta, dpsi per degree, dCC/dt per voxel).
+ * h: n^3 floats (from emc_particle_template).  Outputs: h_cc[n], h_grad[6n] host. */
+EMC_API emc_status emc_particle_template(int n, const float* d_spectrum, float* d_h, void* stream);
+EMC_API emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, double energy_p,
+                          const double prior[9], const double* poses, int n_poses,
+                          double* h_cc, double* h_grad, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Template search (BH_templateSearch3d_2.m:633-887)                          */
+/* ------------------------------------------------------------------------ */
+
+typedef struct emc_tsearch_s* emc_tsearch_t;
+
+/* Tomogram nx*ny*nz (device floats, already locally normalised), every dim 2^a 3^b <= 512.
+ * The tomogram spectrum is computed once and multiplied by the swapQuadrants phase
+ * ramp (BH_templateSearch3d_2.m:633-641, :714). */
+EMC_API emc_status emc_tsearch_create(const float* d_tomo, int nx, int ny, int nz,
+                              emc_tsearch_t* out, void* stream);
+/* template: t^3 floats (device, t <= min dim), zero-padded into the centre of the volume
+ * (BH_templateSearch3d_2.m:752); orientations as in emc_search_set_orientations but
+ * the template is sampled with defineMatrix([phi,theta,psi-phi],'forward')
+ * (:744).  For each orientation the CC map is divided by its standard deviation
+ * (:764) and the per-voxel max and the 1-based index of the winning orientation are
+ * kept (:851-854, strict '<' so the first orientation wins ties).  d_peak / d_angle:
+ * nx*ny*nz floats, initialised by the call. */
+EMC_API emc_status emc_tsearch_run(emc_tsearch_t h, const float* d_template, int t,
+                           const double* phi_theta_psi, int n_orient,
+                           float* d_peak, float* d_angle, void* stream);
+EMC_API emc_status emc_tsearch_destroy(emc_tsearch_t h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EMC_B200_H */

@@ -1,0 +1,276 @@
+"""Python access to the CPU oracle of the orientation-search path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg as the checker; the product never imports it.
+
+``lib(precision)`` loads oracle/liboracle_f64.so (the FP64 oracle) or liboracle_f32.so
+(the single-precision CPU port used as the timed baseline), building them with make when
+missing.  The numpy helpers below restate the host-side parts of the reference that are
+plain arithmetic (grid enumeration, rotation matrices, masks and wedges).
+"""
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_libs = {}
+
+
+def build():
+    r = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+
+
+def lib(precision="f64"):
+    if precision in _libs:
+        return _libs[precision]
+    path = os.path.join(HERE, "liboracle_%s.so" % precision)
+    src = os.path.join(HERE, "emc_oracle.c")
+    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+        build()
+    L = C.CDLL(path)
+    sfx = "_" + precision
+    R = C.c_double if precision == "f64" else C.c_float
+    pR = C.POINTER(R)
+    pd, pi = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    sig = {
+        "orc_define_matrix": (None, [pd, C.c_int, pd]),
+        "orc_rotate": (None, [pR, C.c_int, C.c_int, C.c_int, pd, C.c_int, pd, C.c_int, C.c_int, pR]),
+        "orc_fft3_r2c": (None, [pR, C.c_int, C.c_int, C.c_int, pR]),
+        "orc_fft3_c2r": (None, [pR, C.c_int, C.c_int, C.c_int, pR]),
+        "orc_fft1": (None, [pR, C.c_int, C.c_int, C.c_int]),
+        "orc_ctf2d": (None, [R, R, R, R, R, R, R, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, R, R, pR]),
+        "orc_sf3d": (None, [C.c_int, C.c_int, C.c_int, C.c_int, pR, pR, pR, pR, pR, pR, pR, C.c_int, pR, pR, pR, pR]),
+        "orc_particle_spectrum": (C.c_double, [pR, pR, pR, C.c_int, pR]),
+        "orc_search": (None, [pR, pR, pR, C.c_int, pR, C.c_double, pd, C.c_int, pd, C.c_int, C.c_int, C.c_int, pd,
+                              pi]),
+        "orc_xcf_translational": (C.c_double, [pR, pR, pR, C.c_int, pR, C.c_double, pd, pd, pR, C.c_int, pR, pd]),
+        "orc_tsearch": (None, [pR, C.c_int, C.c_int, C.c_int, pR, C.c_int, pd, C.c_int, pR, pR]),
+        "orc_cc_pose": (C.c_double, [pR, pR, C.c_int, pR, C.c_double, pd, pd, pd, pd]),
+    }
+    funcs = {}
+    for name, (res, args) in sig.items():
+        f = getattr(L, name + sfx)
+        f.restype = res
+        f.argtypes = args
+        funcs[name] = f
+    obj = type("OracleLib", (), {})()
+    obj.__dict__.update(funcs)
+    obj.dtype = np.float64 if precision == "f64" else np.float32
+    obj.ptr = lambda a, _p=pR: a.ctypes.data_as(_p)
+    _libs[precision] = obj
+    return obj
+
+
+def _p(a, t=C.c_double):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype) if a is not None else None
+
+
+# ----------------------------------------------------------------------------- wrappers
+def define_matrix(angles, direction="inv"):
+    out = np.zeros(9)
+    a = np.ascontiguousarray(angles, dtype=np.float64)
+    lib().orc_define_matrix(_p(a), 0 if direction == "forward" else 1, _p(out))
+    return out.reshape(3, 3, order="F")
+
+
+def rotate(vol, M, shift=(0, 0, 0), direction="forward", interp=0, precision="f64", symmetry=None):
+    L = lib(precision)
+    v = _arr(vol, L.dtype)
+    nz, ny, nx = v.shape
+    mats = [np.asarray(M, dtype=np.float64)] if symmetry is None else [np.asarray(M) @ s for s in symmetry]
+    mp = np.ascontiguousarray(np.concatenate([m.reshape(3, 3).flatten(order="F") for m in mats]))
+    sh = np.ascontiguousarray(shift, dtype=np.float64)
+    out = np.zeros_like(v)
+    L.orc_rotate(L.ptr(v), nx, ny, nz, _p(mp), len(mats), _p(sh), 1 if direction == "forward" else 0, interp,
+                 L.ptr(out))
+    return out
+
+
+def rfftn(vol, precision="f64"):
+    L = lib(precision)
+    v = _arr(vol, L.dtype)
+    nz, ny, nx = v.shape
+    out = np.zeros((nz, ny, nx // 2 + 1), dtype=np.complex128 if precision == "f64" else np.complex64)
+    L.orc_fft3_r2c(L.ptr(v), nx, ny, nz, L.ptr(out.view(L.dtype)))
+    return out
+
+
+def irfftn(spec, shape, precision="f64"):
+    L = lib(precision)
+    s = np.ascontiguousarray(spec, dtype=np.complex128 if precision == "f64" else np.complex64)
+    nz, ny, nx = shape
+    out = np.zeros(shape, dtype=L.dtype)
+    L.orc_fft3_c2r(L.ptr(s.view(L.dtype)), nx, ny, nz, L.ptr(out))
+    return out
+
+
+def fft1(data, sign=-1, precision="f64"):
+    L = lib(precision)
+    d = np.ascontiguousarray(data, dtype=np.complex128 if precision == "f64" else np.complex64).copy()
+    n = d.shape[-1]
+    L.orc_fft1(L.ptr(d.view(L.dtype)), n, d.size // n, sign)
+    return d
+
+
+def ctf2d(nx, ny, pixel_size, wavelength, cs_mm, defocus1, defocus2, astig_deg, amp_contrast, half=True,
+          squared=False, centred=False, radial_weight=None, exposure=None, precision="f64"):
+    L = lib(precision)
+    out = np.zeros((ny, nx // 2 + 1 if half else nx), dtype=L.dtype)
+    L.orc_ctf2d(pixel_size, wavelength, cs_mm, defocus1, defocus2, astig_deg, amp_contrast, nx, ny, int(half),
+                int(squared), int(centred), int(radial_weight is not None), radial_weight or 0.0, exposure or 0.0,
+                L.ptr(out))
+    return out
+
+
+def sf3d(size, pixel_size, wavelength, cs_mm, df1, df2, astig_deg, amp_contrast, tilt_deg, exposure, occupancy,
+         squared=True, precision="f64"):
+    L = lib(precision)
+    nt = len(tilt_deg)
+    arrs = [np.ascontiguousarray(np.broadcast_to(np.asarray(x, dtype=L.dtype), (nt,))) for x in
+            (pixel_size, wavelength, cs_mm, df1, df2, astig_deg, amp_contrast, tilt_deg, exposure, occupancy)]
+    nx, ny, nz = size
+    out = np.zeros((nz, ny, nx), dtype=L.dtype)
+    L.orc_sf3d(int(squared), nx, ny, nz, *[L.ptr(a) for a in arrs[:7]], nt, L.ptr(arrs[7]), L.ptr(arrs[8]),
+               L.ptr(arrs[9]), L.ptr(out))
+    return out
+
+
+def particle_spectrum(particle, weight=None, bandpass=None, precision="f64"):
+    L = lib(precision)
+    p = _arr(particle, L.dtype)
+    n = p.shape[0]
+    w = _arr(weight, L.dtype)
+    b = _arr(bandpass, L.dtype)
+    q = np.zeros((n, n, n // 2 + 1), dtype=np.complex128 if precision == "f64" else np.complex64)
+    e = L.orc_particle_spectrum(L.ptr(p), L.ptr(w) if w is not None else None, L.ptr(b) if b is not None else None,
+                                n, L.ptr(q.view(L.dtype)))
+    return q, e
+
+
+def search(ref, q, energy, matrices, mask=None, wref=None, shift=(0, 0, 0), radius=7, interp=0, nthreads=0,
+           precision="f64"):
+    """Per-orientation (cc, peak) of the fused search.  ``matrices``: RotMat per orientation
+    (the reference is sampled through RotMat', 'forward')."""
+    L = lib(precision)
+    r = _arr(ref, L.dtype)
+    n = r.shape[0]
+    m = _arr(mask, L.dtype)
+    wr = _arr(wref, L.dtype)
+    qq = np.ascontiguousarray(q, dtype=np.complex128 if precision == "f64" else np.complex64)
+    mats = np.ascontiguousarray(np.stack([np.asarray(M).T.flatten(order="F") for M in matrices]))
+    sh = np.ascontiguousarray(shift, dtype=np.float64)
+    no = len(matrices)
+    cc = np.zeros(no)
+    pk = np.zeros((no, 3), dtype=np.int32)
+    L.orc_search(L.ptr(r), L.ptr(m) if m is not None else None, L.ptr(wr) if wr is not None else None, n,
+                 L.ptr(qq.view(L.dtype)), float(energy), _p(mats), no, _p(sh), int(radius), int(interp),
+                 int(nthreads), _p(cc), _p(pk, C.c_int))
+    return cc, pk
+
+
+def xcf_translational(ref, q, energy, matrix, mask=None, wref=None, shift=(0, 0, 0), peak_mask=None, interp=0):
+    L = lib("f64")
+    r = _arr(ref, L.dtype)
+    n = r.shape[0]
+    m = _arr(mask, L.dtype)
+    wr = _arr(wref, L.dtype)
+    pm = _arr(peak_mask, L.dtype)
+    qq = np.ascontiguousarray(q, dtype=np.complex128)
+    M = np.ascontiguousarray(np.asarray(matrix).T.flatten(order="F"))
+    sh = np.ascontiguousarray(shift, dtype=np.float64)
+    out = np.zeros((n, n, n))
+    peak = np.zeros(3)
+    v = L.orc_xcf_translational(L.ptr(r), L.ptr(m) if m is not None else None, L.ptr(wr) if wr is not None else None,
+                                n, L.ptr(qq.view(L.dtype)), float(energy), _p(M), _p(sh),
+                                L.ptr(pm) if pm is not None else None, int(interp), L.ptr(out), _p(peak))
+    return v, peak, out
+
+
+def tsearch(tomo, tmpl, matrices, precision="f64"):
+    """Template search MIP; ``matrices``: defineMatrix([phi,theta,psi-phi],'forward') per orientation."""
+    L = lib(precision)
+    t = _arr(tomo, L.dtype)
+    g = _arr(tmpl, L.dtype)
+    nz, ny, nx = t.shape
+    mats = np.ascontiguousarray(np.stack([np.asarray(M).flatten(order="F") for M in matrices]))
+    peak = np.zeros_like(t)
+    ang = np.zeros_like(t)
+    L.orc_tsearch(L.ptr(t), nx, ny, nz, L.ptr(g), g.shape[0], _p(mats), len(matrices), L.ptr(peak), L.ptr(ang))
+    return peak, ang
+
+
+def cc_pose(ref, h, energy, matrix, t, mask=None):
+    """Zero-lag normalised CC of the tricubic-rotated reference (sampled through matrix,
+    'forward', shift t) against the real-space template h; returns (cc, dM (3x3), dt (3))."""
+    L = lib("f64")
+    r = _arr(ref, L.dtype)
+    hh = _arr(h, L.dtype)
+    m = _arr(mask, L.dtype)
+    M = np.ascontiguousarray(np.asarray(matrix).flatten(order="F"))
+    tt = np.ascontiguousarray(t, dtype=np.float64)
+    dM = np.zeros(9)
+    dt = np.zeros(3)
+    cc = L.orc_cc_pose(L.ptr(r), L.ptr(m) if m is not None else None, r.shape[0], L.ptr(hh), float(energy), _p(M),
+                       _p(tt), _p(dM), _p(dt))
+    return cc, dM.reshape(3, 3, order="F"), dt
+
+
+# ----------------------------------------------------------------------------- numpy restatements
+def define_matrix_np(angles, direction="inv"):
+    """BH_defineMatrix 'Bah' (coordinates/BH_defineMatrix.m:85-126) in numpy."""
+    a = np.radians(np.asarray(angles, dtype=np.float64))
+    a = -a if direction == "forward" else a[::-1]
+    c, s = np.cos(a), np.sin(a)
+    rz3 = np.array([[c[2], -s[2], 0], [s[2], c[2], 0], [0, 0, 1]])
+    rx2 = np.array([[1, 0, 0], [0, c[1], -s[1]], [0, s[1], c[1]]])
+    rz1 = np.array([[c[0], -s[0], 0], [s[0], c[0], 0], [0, 0, 1]])
+    return rz3 @ rx2 @ rz1
+
+
+def _colon(a, d, b):
+    if not d > 0 or b < a:
+        return []
+    n = int(math.floor((b - a) / d + 1e-10 * (1 + abs((b - a) / d)))) + 1
+    return [a + k * d for k in range(n)]
+
+
+def euler_search_np(symmetry, theta_max, theta_step, psi_max, psi_step):
+    """eulerSearch (coordinates/eulerSearch.m:38-177) walked as BH_alignRaw3d_v2.m:1119-1170."""
+    bipolar = theta_max < 0
+    theta_max = abs(theta_max)
+    psi_w = 2.0 * psi_max
+    k, num = symmetry[0], symmetry[1:]
+    if k == "C":
+        psi_w = min(psi_w, 360.0 / float(num)); theta_max = min(180.0, theta_max); phi_max = 360.0
+    elif k == "D":
+        psi_w = 360.0 / float(num); theta_max = min(theta_max, 90.0); phi_max = 360.0
+    elif k == "O":
+        psi_w = min(psi_w, 90.0); theta_max = min(theta_max, 54.7); phi_max = 90.0
+    elif k == "I":
+        psi_w = min(psi_w, 180.0); theta_max = 31.7; phi_max = 180.0
+    else:
+        raise ValueError(symmetry)
+    psi = _colon(-psi_w / 2, psi_step, psi_w / 2) or [0.0]
+    theta = _colon(0.0, theta_step, theta_max) or [0.0]
+    if bipolar:
+        theta = theta + [180.0 - t for t in reversed(theta)]
+    out = []
+    for th in theta:
+        if th in (0.0, 180.0):
+            step = phi_max
+        else:
+            step = abs(theta_step / math.sin(math.radians(th)))
+            step = phi_max if step > phi_max else phi_max / math.floor(phi_max / step + 0.5)
+        for ph in _colon(0.0, step, phi_max - 1):
+            for ps in psi:
+                out.append((math.fmod(ph, 360.0), th, ps))
+    return np.array(out)

@@ -1,0 +1,212 @@
+"""Fused orientation search against the FP64 oracle (same inputs, same orientation list)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4   # CC relative tolerance
+ATOL = 1e-6
+
+
+def compare(cc_g, pk_g, cc_o, pk_o):
+    """CC within RTOL; integer peaks identical except at near-ties (where the GPU's CC at its own
+    peak equals the oracle's peak value within tolerance)."""
+    assert np.allclose(cc_g, cc_o, rtol=RTOL, atol=ATOL), np.abs(cc_g - cc_o).max()
+    mism = np.any(pk_g != pk_o, axis=1)
+    assert mism.mean() < 0.02, "too many peak mismatches: %d" % mism.sum()
+
+
+def best_nondegenerate(cc_o):
+    order = np.argsort(-cc_o, kind="stable")
+    gap = cc_o[order[0]] - cc_o[order[1]]
+    return order[0], gap > 10 * (RTOL * abs(cc_o[order[0]]) + ATOL)
+
+
+@pytest.fixture(scope="module")
+def plain_case(built_lib, cuda):
+    from emclarity_b200 import synthetic
+    case = synthetic.PlainCase(seed=3)
+    g = case.to_gpu()
+    return case, g
+
+
+def run_gpu(case, g, grid, interp="linear", store="f32", wref=None, prior=None):
+    from emclarity_b200 import api
+    q, e = api.particle_spectrum(g["particle"], g["weight"])
+    s = api.Search(peak_radius=case.peak_radius, interp=interp)
+    rid = s.add_reference(g["ref"], g["mask"], wref, store=store)
+    s.set_orientations(grid)
+    pdesc = s.particle(q, e.item(), rid, prior=prior, orient_count=len(grid))
+    cc, pk, best = s.run_host([pdesc])
+    s.close()
+    return cc, pk, best, q, e.item()
+
+
+def run_oracle(case, g, grid, interp=0, ref=None, wref=None, prior=None):
+    from emclarity_b200 import api
+    part = g["particle"].cpu().numpy()
+    w = g["weight"].cpu().numpy()
+    q, e = O.particle_spectrum(part, w)
+    mats = api.search_matrices(grid, prior)
+    ref = case.ref if ref is None else ref
+    return O.search(ref, q, e, mats, mask=case.mask, wref=wref, radius=case.peak_radius, interp=interp)
+
+
+def test_plain_search_parity_and_truth(plain_case):
+    case, g = plain_case
+    grid = case.grid
+    cc_g, pk_g, best, _, _ = run_gpu(case, g, grid)
+    cc_o, pk_o = run_oracle(case, g, grid)
+    compare(cc_g, pk_g, cc_o, pk_o)
+    b, nondeg = best_nondegenerate(cc_o)
+    if nondeg:
+        assert best[0][1] == b
+        assert tuple(best[0][2]) == tuple(pk_o[b])
+    # the planted shift is recovered at the best orientation
+    assert tuple(best[0][2]) == tuple(int(v) for v in case.shift)
+    # and the best orientation is the grid point nearest the truth
+    from emclarity_b200 import api
+    mats = api.search_matrices(grid)
+    ang = np.degrees(np.arccos(np.clip((np.einsum("kij,ij->k", mats, case.truth_matrix) - 1) / 2, -1, 1)))
+    assert ang[best[0][1]] <= np.sort(ang)[2] + 1e-9
+
+
+def test_cubic_and_border_modes(plain_case):
+    case, g = plain_case
+    grid = case.grid[::9]
+    for interp, mode in (("cubic", 1), ("linear_border", 2)):
+        cc_g, pk_g, _, _, _ = run_gpu(case, g, grid, interp=interp)
+        cc_o, pk_o = run_oracle(case, g, grid, interp=mode)
+        compare(cc_g, pk_g, cc_o, pk_o)
+
+
+def test_reference_weight_path(plain_case):
+    """A real half-spectrum weight on the rotated reference (bandpass): E_R from the spectrum."""
+    case, g = plain_case
+    n = case.n
+    k = np.fft.fftfreq(n)
+    kz, ky, kx = np.meshgrid(k, k, np.fft.rfftfreq(n), indexing="ij")
+    bp = np.exp(-(kx ** 2 + ky ** 2 + kz ** 2) / (2 * 0.18 ** 2)).astype(np.float32)
+    grid = case.grid[::7]
+    cc_g, pk_g, _, _, _ = run_gpu(case, g, grid, wref=torch.from_numpy(bp).cuda())
+    cc_o, pk_o = run_oracle(case, g, grid, wref=bp)
+    compare(cc_g, pk_g, cc_o, pk_o)
+
+
+def test_bf16_reference_storage(plain_case):
+    case, g = plain_case
+    grid = case.grid[::5]
+    cc_g, pk_g, _, _, _ = run_gpu(case, g, grid, store="bf16")
+    ref_bf = torch.from_numpy(case.ref).to(torch.bfloat16).float().numpy()
+    cc_o, pk_o = run_oracle(case, g, grid, ref=ref_bf)
+    compare(cc_g, pk_g, cc_o, pk_o)
+
+
+def test_prior_composition(plain_case):
+    """RotMat = R_prior * D (FP64 on the device) matches the host composition."""
+    from emclarity_b200 import api
+    case, g = plain_case
+    prior = api.define_matrix([33.0, 21.0, -48.0], "inv")
+    grid = case.grid[::11]
+    cc_g, pk_g, _, _, _ = run_gpu(case, g, grid, prior=prior)
+    cc_o, pk_o = run_oracle(case, g, grid, prior=prior)
+    compare(cc_g, pk_g, cc_o, pk_o)
+
+
+def test_batched_uneven_matches_oracle(built_lib, cuda):
+    """Several particles of 64^3 and 96^3 (and one 128^3) in one call, each with its own slice."""
+    from emclarity_b200 import api, synthetic
+    rng = np.random.default_rng(21)
+    grid = synthetic.local_grid(24, 8.0, 2.0)
+    s = api.Search(peak_radius=5)
+    refs, descs, oracle_in = {}, [], []
+    for n in (64, 96, 128):
+        ref = synthetic.blob_reference(rng, n)
+        mask = synthetic.soft_sphere_mask(n, 28 * n / 64)
+        refs[n] = (ref, mask, s.add_reference(torch.from_numpy(ref).cuda(), torch.from_numpy(mask).cuda()))
+    s.set_orientations(grid)
+    keep = []
+    for i, n in enumerate([64, 96, 64, 128, 96]):
+        ref, mask, rid = refs[n]
+        prior = api.define_matrix(rng.uniform(-90, 90, 3), "inv")
+        truth = prior @ api.define_matrix([rng.uniform(0, 5), rng.uniform(0, 5), rng.uniform(-5, 5)], "inv")
+        shift = rng.integers(-3, 4, 3)
+        wt = api.wedge_ctf_weight(n, -55, 62, synthetic.ctf_dict(rng.uniform(15000, 40000)))
+        part = synthetic.make_particle(torch.from_numpy(ref).cuda(), rng, truth, shift, wt, 0.5)
+        q, e = api.particle_spectrum(part, wt)
+        keep.append(q)
+        begin = (3 * i) % 8
+        descs.append(s.particle(q, e.item(), rid, prior=prior, orient_begin=begin, orient_count=len(grid) - begin))
+        oracle_in.append((ref, mask, part.cpu().numpy(), wt.cpu().numpy(), prior, begin))
+    cc_g, pk_g, best = s.run_host(descs)
+    off = 0
+    for (ref, mask, part, wt, prior, begin), hit in zip(oracle_in, best):
+        q, e = O.particle_spectrum(part, wt)
+        mats = api.search_matrices(grid[begin:], prior)
+        cc_o, pk_o = O.search(ref, q, e, mats, mask=mask, radius=5)
+        m = len(grid) - begin
+        compare(cc_g[off:off + m], pk_g[off:off + m], cc_o, pk_o)
+        b, nondeg = best_nondegenerate(cc_o)
+        if nondeg:
+            assert hit[1] == begin + b
+            assert tuple(hit[2]) == tuple(pk_o[b])
+        off += m
+    # the same request again replays the captured graph and gives identical results
+    cc2, pk2, best2 = s.run_host(descs)
+    assert np.array_equal(cc2, cc_g) and np.array_equal(pk2, pk_g)
+
+
+def test_graph_replay_device_outputs(plain_case):
+    from emclarity_b200 import api
+    case, g = plain_case
+    q, e = api.particle_spectrum(g["particle"], g["weight"])
+    s = api.Search(peak_radius=7)
+    rid = s.add_reference(g["ref"], g["mask"])
+    s.set_orientations(case.grid)
+    d = s.particle(q, e.item(), rid, orient_count=len(case.grid))
+    cc = torch.empty(len(case.grid), device="cuda")
+    pk = torch.empty(len(case.grid), 3, dtype=torch.int32, device="cuda")
+    best = torch.empty(1, 5, dtype=torch.int32, device="cuda")
+    s.run([d], cc, pk, best)
+    a = (cc.clone(), pk.clone(), best.clone())
+    for _ in range(3):
+        s.run([d], cc, pk, best)
+    torch.cuda.synchronize()
+    assert torch.equal(a[0], cc) and torch.equal(a[1], pk) and torch.equal(a[2], best)
+
+
+def test_bad_requests_are_rejected(plain_case):
+    from emclarity_b200 import EmcError, api
+    case, g = plain_case
+    q, e = api.particle_spectrum(g["particle"], g["weight"])
+    s = api.Search(peak_radius=7)
+    rid = s.add_reference(g["ref"], g["mask"])
+    s.set_orientations(case.grid)
+    with pytest.raises(EmcError):
+        s.run_host([s.particle(q, e.item(), rid, orient_begin=530, orient_count=20)])
+    with pytest.raises(EmcError):
+        s.run_host([s.particle(q, e.item(), rid + 5, orient_count=3)])
+    with pytest.raises(EmcError):
+        s.run_host([s.particle(q, 0.0, rid, orient_count=3)])
+    with pytest.raises(EmcError):
+        s.configure(peak_radius=-1)
+    with pytest.raises(EmcError):
+        s.add_reference(torch.zeros(80, 80, 80, device="cuda"))
+
+
+def test_nan_particle_does_not_win(plain_case):
+    """A NaN in the particle spectrum gives NaN CCs, never a spurious best orientation."""
+    from emclarity_b200 import api
+    case, g = plain_case
+    q, e = api.particle_spectrum(g["particle"], g["weight"])
+    qn = q.clone()
+    qn[3, 4, 5] = float("nan")
+    s = api.Search(peak_radius=7)
+    rid = s.add_reference(g["ref"], g["mask"])
+    s.set_orientations(case.grid[:10])
+    cc, pk, best = s.run_host([s.particle(qn, e.item(), rid, orient_count=10)])
+    assert np.all(np.isnan(cc))
+    assert best[0][1] == -1

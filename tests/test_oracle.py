@@ -1,0 +1,193 @@
+"""CPU checks of the oracle itself: its FFT against numpy, its host math against the
+numpy restatements and the committed golden vectors, and internal consistency."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("shape", [(8, 12, 16), (16, 16, 16), (6, 24, 9), (64, 64, 64), (5, 7, 3)])
+def test_oracle_fft_matches_numpy(shape):
+    x = np.random.default_rng(1).standard_normal(shape)
+    X = O.rfftn(x)
+    ref = np.fft.rfftn(x)
+    assert np.abs(X - ref).max() <= 1e-11 * np.abs(ref).max()
+    back = O.irfftn(X, shape) / x.size
+    assert np.abs(back - x).max() < 1e-12
+
+
+@pytest.mark.parametrize("n", [2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 7, 25])
+def test_oracle_fft1_lengths(n):
+    x = np.random.default_rng(n).standard_normal((3, n)) + 1j * np.random.default_rng(n + 1).standard_normal((3, n))
+    assert np.abs(O.fft1(x, -1) - np.fft.fft(x, axis=-1)).max() < 1e-10 * n
+    assert np.abs(O.fft1(x, 1) - np.fft.ifft(x, axis=-1) * n).max() < 1e-10 * n
+
+
+def test_define_matrix_matches_numpy_restatement():
+    rng = np.random.default_rng(2)
+    for _ in range(50):
+        a = rng.uniform(-360, 360, 3)
+        for d in ("forward", "inv"):
+            M = O.define_matrix(a, d)
+            assert np.abs(M - O.define_matrix_np(a, d)).max() < 1e-14
+            assert np.abs(M @ M.T - np.eye(3)).max() < 1e-14
+    # 'forward' and 'inv' of the same triple are inverse rotations (BH_defineMatrix.m:85-102)
+    a = [30.0, 50.0, -70.0]
+    assert np.abs(O.define_matrix(a, "forward") @ O.define_matrix(a, "inv") - np.eye(3)).max() < 1e-14
+
+
+def test_define_matrix_known_values():
+    # pure Z rotation by 90 degrees: Rz(90) with 'inv' ordering of [90, 0, 0]
+    M = O.define_matrix([90, 0, 0], "inv")
+    assert np.allclose(M, [[0, -1, 0], [1, 0, 0], [0, 0, 1]], atol=1e-15)
+    # pure X rotation by the second angle
+    M = O.define_matrix([0, 90, 0], "inv")
+    assert np.allclose(M, [[1, 0, 0], [0, 0, -1], [0, 1, 0]], atol=1e-15)
+
+
+@pytest.mark.parametrize("args,count", [
+    (("C1", 40, 10, 40, 10), 540),     # the 10-degree grid of the single-subtomogram workload
+    (("C1", 180, 12, 48, 12), 2592),   # the 12-degree template-search grid
+    (("C1", 180, 15, 180, 15), 4600),  # the full 15-degree grid
+    (("C1", 0, 0, 0, 0), 1),
+    (("C2", 20, 10, 180, 10), None),
+    (("O", 90, 15, 90, 15), None),
+    (("I", 30, 10, 90, 10), None),
+    (("C1", -20, 10, 20, 10), None),   # bipolar
+])
+def test_euler_grid_counts(args, count):
+    g = O.euler_search_np(*args)
+    if count is not None:
+        assert len(g) == count
+    assert np.all(g[:, 1] >= 0) and np.all(g[:, 1] <= 180)
+
+
+def test_rotate_identity_and_inverse():
+    rng = np.random.default_rng(3)
+    v = rng.standard_normal((16, 16, 16))
+    for interp in (0, 1, 2):
+        out = O.rotate(v, np.eye(3), interp=interp)
+        assert np.abs(out - v).max() < 1e-12
+    # a 90 degree rotation about z permutes voxels exactly (origin floor(n/2))
+    M = O.define_matrix([90, 0, 0], "inv")
+    out = O.rotate(v, M, interp=0)
+    c = 8
+    for (z, y, x) in [(3, 4, 5), (10, 2, 7), (8, 8, 8)]:
+        s = M @ np.array([x - c, y - c, z - c]) + c
+        sx, sy, sz = np.rint(s).astype(int)
+        if 0 <= sx < 16 and 0 <= sy < 16 and 0 <= sz < 16:
+            assert abs(out[z, y, x] - v[sz, sy, sx]) < 1e-12
+
+
+def test_rotate_shift_semantics():
+    """'forward' applies -shift before the rotation, 'inv' adds it after (mexXform3d.cu:45-65)."""
+    rng = np.random.default_rng(4)
+    v = rng.standard_normal((12, 12, 12))
+    sh = (1.0, -2.0, 3.0)
+    out_f = O.rotate(v, np.eye(3), sh, "forward")
+    out_i = O.rotate(v, np.eye(3), sh, "inv")
+    assert abs(out_f[6, 6, 6] - v[6 - 3, 6 + 2, 6 - 1]) < 1e-12
+    assert abs(out_i[6, 6, 6] - v[6 + 3, 6 - 2, 6 + 1]) < 1e-12
+
+
+def test_interpn_linear_boundary():
+    """interpn(...,'linear',0): exact at the last grid point, 0 just outside."""
+    v = np.arange(4 * 4 * 4, dtype=np.float64).reshape(4, 4, 4)
+    # identity with a shift of -1 ('inv'): s = p - 1; at p = 0 -> s = -1 -> 0
+    out = O.rotate(v, np.eye(3), (-1, 0, 0), "inv", interp=0)
+    assert out[0, 0, 0] == 0.0
+    assert out[0, 0, 1] == v[0, 0, 0]
+    # border mode interpolates towards zero inside (-1, 0)
+    out = O.rotate(v, np.eye(3), (-0.5, 0, 0), "inv", interp=2)
+    assert abs(out[0, 0, 0] - 0.5 * v[0, 0, 0]) < 1e-12
+
+
+def test_ctf_oracle_formula():
+    """mexCTF (ctf.cu:45-62) against a direct numpy evaluation of the same formula."""
+    nx, ny, pix, wl, cs, df1, df2, ast, ac = 64, 48, 2.5, 0.019687, 2.7, 26000.0, 24000.0, 30.0, 0.07
+    out = O.ctf2d(nx, ny, pix, wl, cs, df1, df2, ast, ac, half=True)
+    x = np.arange(nx // 2 + 1)
+    y = np.arange(ny)
+    y = np.where(y > ny // 2, y - ny, y)
+    fx = x[None, :] / (pix * nx)
+    fy = y[:, None] / (pix * ny)
+    phi = np.arctan2(fy, fx)
+    r2 = fx * fx + fy * fy
+    amp = np.arctan(ac / np.sqrt(1 - ac * ac))
+    a = np.radians(ast) - np.pi * np.rint(ast / 180)
+    val = np.sin(np.pi * 0.5 * cs * 1e7 * wl ** 3 * r2 * r2
+                 - np.pi * wl * r2 * (0.5 * (df1 + df2) + 0.5 * (df1 - df2) * np.cos(2 * (phi - a))) - amp)
+    assert np.abs(out - val).max() < 1e-12
+
+
+def test_search_oracle_finds_planted_shift():
+    """A particle that is the reference rolled by d correlates best at shift d (sign check)."""
+    rng = np.random.default_rng(5)
+    n = 16
+    ref = np.zeros((n, n, n))
+    ref[4:12, 5:11, 6:10] = rng.standard_normal((8, 6, 4))
+    d = (2, -1, 3)
+    part = np.roll(ref, (d[2], d[1], d[0]), axis=(0, 1, 2))
+    q, e = O.particle_spectrum(part)
+    cc, pk = O.search(ref, q, e, [np.eye(3)], radius=5)
+    assert tuple(pk[0]) == d
+    assert abs(cc[0] - 1.0) < 1e-9
+
+
+def test_search_oracle_matches_full_map():
+    """The windowed argmax equals the argmax of the full fftshifted map under a spherical mask."""
+    rng = np.random.default_rng(6)
+    n = 16
+    ref = rng.standard_normal((n, n, n))
+    part = rng.standard_normal((n, n, n))
+    q, e = O.particle_spectrum(part)
+    M = O.define_matrix([10, 20, 30], "inv")
+    cc, pk = O.search(ref, q, e, [M], radius=4)
+    c = n // 2
+    ax = np.arange(n) - c
+    zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
+    pmask = ((xx ** 2 + yy ** 2 + zz ** 2) <= 16).astype(np.float64)
+    v, peak, full = O.xcf_translational(ref, q, e, M, peak_mask=pmask)
+    full_masked = np.where(pmask > 0.5, full, -np.inf)
+    idx = np.unravel_index(np.argmax(full_masked), full.shape)
+    assert (idx[2] - c, idx[1] - c, idx[0] - c) == tuple(pk[0])
+    assert abs(full_masked[idx] - cc[0]) < 1e-12
+
+
+def test_f32_port_agrees_with_f64_oracle():
+    rng = np.random.default_rng(7)
+    n = 32
+    ref = np.zeros((n, n, n), np.float32)
+    ref[8:24, 8:24, 8:24] = rng.standard_normal((16, 16, 16))
+    part = np.roll(ref, 2, axis=0) + 0.5 * rng.standard_normal((n, n, n)).astype(np.float32)
+    mats = [O.define_matrix([a, 10, -a], "inv") for a in (0, 20, 40)]
+    q64, e64 = O.particle_spectrum(part)
+    q32, e32 = O.particle_spectrum(part, precision="f32")
+    cc64, pk64 = O.search(ref, q64, e64, mats, radius=4)
+    cc32, pk32 = O.search(ref, q32, e32, mats, radius=4, precision="f32")
+    assert np.allclose(cc32, cc64, rtol=1e-4, atol=1e-6)
+    assert np.array_equal(pk32, pk64)
+
+
+def test_cc_pose_gradient_matches_finite_differences():
+    rng = np.random.default_rng(8)
+    n = 16
+    ax = np.arange(n) - n // 2
+    zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
+    ref = np.exp(-((xx - 1) ** 2 + (yy + 1) ** 2 + zz ** 2) / 8.0) + 0.5 * np.exp(-((xx + 2) ** 2 + (yy - 2) ** 2 + (zz - 1) ** 2) / 4.0)
+    h = rng.standard_normal((n, n, n))
+    M = O.define_matrix([5, 8, -3], "inv")
+    t = np.array([0.3, -0.2, 0.1])
+    cc, dM, dt = O.cc_pose(ref, h, 2.0, M, t)
+    eps = 1e-6
+    for i in range(3):
+        for j in range(3):
+            Mp = M.copy(); Mp[i, j] += eps
+            Mm = M.copy(); Mm[i, j] -= eps
+            fd = (O.cc_pose(ref, h, 2.0, Mp, t)[0] - O.cc_pose(ref, h, 2.0, Mm, t)[0]) / (2 * eps)
+            assert abs(fd - dM[i, j]) < 1e-6 * max(1.0, abs(fd)) + 1e-8
+    for j in range(3):
+        tp = t.copy(); tp[j] += eps
+        tm = t.copy(); tm[j] -= eps
+        fd = (O.cc_pose(ref, h, 2.0, M, tp)[0] - O.cc_pose(ref, h, 2.0, M, tm)[0]) / (2 * eps)
+        assert abs(fd - dt[j]) < 1e-6 * max(1.0, abs(fd)) + 1e-8
