@@ -59,5 +59,36 @@ def build(verbose=False, extra=()):
     return LIB
 
 
+MEX_DIR = os.path.join(HERE, "mex")
+MEX_OUT = os.path.join(MEX_DIR, "_shim")
+GATEWAYS = ["mexXform3d_b200", "mexFFT_b200", "mexCTF_b200", "mexSF3D_b200", "mexEmcSearch"]
+
+
+def build_mex(verbose=False):
+    """Compiles every MEX gateway against the in-repo MEX stand-in (emclarity_b200/mex/shim) into
+    emclarity_b200/mex/_shim/lib<gateway>.so, linked to libemc_b200.so.  With MATLAB installed the
+    same sources build with `mex` instead (see the integration notes)."""
+    lib = build(verbose=verbose)
+    os.makedirs(MEX_OUT, exist_ok=True)
+    shim = os.path.join(MEX_DIR, "shim", "mex_shim.cpp")
+    outs = []
+    for gw in GATEWAYS:
+        src = os.path.join(MEX_DIR, gw + ".cpp")
+        out = os.path.join(MEX_OUT, "lib%s.so" % gw)
+        deps = [src, shim, os.path.join(MEX_DIR, "mex_common.h"), lib]
+        if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+            outs.append(out)
+            continue
+        cmd = [_nvcc(), "-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-I", os.path.join(MEX_DIR, "shim"),
+               "-I", INCLUDE, "-I", MEX_DIR, src, shim, "-o", out, "-L", HERE, "-lemc_b200", "-lcudart",
+               "-Xlinker", "-rpath=$ORIGIN/../.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("MEX gateway build failed for %s:\n%s\n%s" % (gw, " ".join(cmd), r.stderr[-4000:]))
+        outs.append(out)
+    return outs
+
+
 if __name__ == "__main__":
     build(verbose=True, extra=sys.argv[1:])
+    build_mex(verbose=True)
