@@ -72,6 +72,11 @@ SIGNATURES = {
     "emc_sf3d": (_i, [_i, _i, C.POINTER(C.c_uint), _pf, _pf, _pf, _pf, _pf, _pf, _pf, C.c_uint, _pf, _pf, _pf,
                       _vp, _vp]),
     "emc_wedge_ctf_weight": (_i, [_i, _f, _f, C.POINTER(CtfParams), _i, _vp, _vp]),
+    "emc_pad3d": (_i, [_vp, _i, _i, _i, _pi, _pi, _f, _i, _vp, _vp]),
+    "emc_bandpass3d": (_i, [_i, _i, _i, _f, _f, _f, _f, _vp, _vp]),
+    "emc_band_limit_center_normalize": (_i, [_vp, _i, _i, _i, _pi, _pi, _i, _vp, _vp, _vp]),
+    "emc_xcf_rotational": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _pd, _vp]),
+    "emc_xcf_translational": (_i, [_vp, _vp, _i, _i, _i, _vp, _i, _pd, _pd, _vp, _vp]),
     "emc_particle_spectrum": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "emc_particle_template": (_i, [_i, _vp, _vp, _vp]),
     "emc_search_create": (_i, [C.POINTER(_vp)]),
@@ -83,6 +88,7 @@ SIGNATURES = {
     "emc_search_destroy": (_i, [_vp]),
     "emc_search_set_profiling": (_i, [_vp, _i]),
     "emc_search_timings": (_i, [_vp, _pd, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_long), _i]),
+    "emc_cc_adjoint_batch": (_i, [_vp, _i, _pi, C.POINTER(_vp), _pd, _pd, _pd, _pd, _pd, _vp]),
     "emc_cc_adjoint": (_i, [_vp, _i, _vp, _d, _pd, _pd, _i, _pd, _pd, _vp]),
     "emc_tsearch_create": (_i, [_vp, _i, _i, _i, C.POINTER(_vp), _vp]),
     "emc_tsearch_run": (_i, [_vp, _vp, _i, _pd, _i, _vp, _vp, _vp]),

@@ -373,3 +373,66 @@ class TemplateSearch:
             self.close()
         except Exception:
             pass
+
+
+# --------------------------------------------------------------------------- volume / spectrum operators
+def pad3d(img, pad_low, pad_top, fill=0.0, taper=False):
+    """BH_padZeros3d(img, padLow, padTop, 'GPU', 'single'|'singleTaper', fill); pads given (x, y, z)."""
+    nz, ny, nx = img.shape
+    pl = (C.c_int * 3)(*[int(v) for v in pad_low])
+    pt = (C.c_int * 3)(*[int(v) for v in pad_top])
+    out_shape = tuple(s + l + t for s, l, t in zip((nz, ny, nx), reversed(pad_low), reversed(pad_top)))
+    out = torch.empty(out_shape, dtype=torch.float32, device="cuda")
+    L.call("emc_pad3d", _need_cuda(img, "img"), nx, ny, nz, pl, pt, float(fill), int(bool(taper)),
+           _need_cuda(out, "out"), _stream())
+    return out
+
+
+def bandpass3d(shape_xyz, high_thresh, high_cut, low_cut, pixel_size):
+    """BH_bandpass3d on the half spectrum (z, y, x//2+1); pixel_size 0 -> 'nyquist', < 0 -> 'nyquistHigh'."""
+    nx, ny, nz = shape_xyz
+    out = torch.empty((nz, ny, nx // 2 + 1), dtype=torch.float32, device="cuda")
+    L.call("emc_bandpass3d", nx, ny, nz, float(high_thresh), float(high_cut), float(low_cut), float(pixel_size),
+           _need_cuda(out, "out"), _stream())
+    return out
+
+
+def band_limit_center_normalize(img, pad_low=(0, 0, 0), pad_top=(0, 0, 0), taper=False, bandpass=None):
+    """BH_bandLimitCenterNormalize: half spectrum of the mean-padded image, F(0) = 0, bandpassed,
+    scaled to sqrt(sum |F|^2) / numel = 1."""
+    nz, ny, nx = img.shape
+    od = [s + l + t for s, l, t in zip((nx, ny, nz), pad_low, pad_top)]
+    out = torch.empty((od[2], od[1], od[0] // 2 + 1), dtype=torch.complex64, device="cuda")
+    pl = (C.c_int * 3)(*[int(v) for v in pad_low])
+    pt = (C.c_int * 3)(*[int(v) for v in pad_top])
+    L.call("emc_band_limit_center_normalize", _need_cuda(img, "img"), nx, ny, nz, pl, pt, int(bool(taper)),
+           _need_cuda(bandpass, "bandpass") if bandpass is not None else None,
+           _need_cuda(out, "out", torch.complex64), _stream())
+    return out
+
+
+def xcf_rotational(part_ft, ref_ft_conj, wdg_mask=None, ref_wdg=None, nx=None):
+    """BH_multi_xcf_Rotational on half spectra (z, y, x//2+1)."""
+    nz, ny, nxh = part_ft.shape
+    nx = nx if nx is not None else 2 * (nxh - 1)
+    cc = C.c_double(0)
+    L.call("emc_xcf_rotational", _need_cuda(part_ft, "part_ft", torch.complex64),
+           _need_cuda(ref_ft_conj, "ref_ft", torch.complex64),
+           _need_cuda(wdg_mask, "wdg_mask") if wdg_mask is not None else None,
+           _need_cuda(ref_wdg, "ref_wdg") if ref_wdg is not None else None, nx, ny, nz, C.byref(cc), _stream())
+    return cc.value
+
+
+def xcf_translational(a, b, peak_mask=None, peak_com=3, nx=None, return_map=False):
+    """BH_multi_xcf_Translational(A, B, peakMask, peakCOM): subvoxel peak (x, y, z) of
+    fftshift(real(ifftn(A .* B))) and the peak value (scaled like MATLAB ifftn)."""
+    nz, ny, nxh = a.shape
+    nx = nx if nx is not None else 2 * (nxh - 1)
+    peak = (C.c_double * 3)()
+    mv = C.c_double(0)
+    mp = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda") if return_map else None
+    L.call("emc_xcf_translational", _need_cuda(a, "a", torch.complex64), _need_cuda(b, "b", torch.complex64),
+           nx, ny, nz, _need_cuda(peak_mask, "peak_mask") if peak_mask is not None else None, int(peak_com), peak,
+           C.byref(mv), _need_cuda(mp, "map") if mp is not None else None, _stream())
+    res = (np.array(list(peak)), mv.value)
+    return res + (mp,) if return_map else res

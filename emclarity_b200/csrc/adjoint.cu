@@ -11,6 +11,7 @@
 // The Euler-angle derivatives of M are formed on the host in FP64.
 #include <math.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "interp.cuh"
@@ -25,20 +26,21 @@ struct AdjPose {
   float t[3];
 };
 
+struct AdjItem {
+  const void* ref;      // n^3 reference (float or bf16)
+  const float* mask;    // n^3 or null
+  const float* h;       // n^3 real-space particle template
+  int n;
+  int dtype;
+  AdjPose pose;
+};
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_cc_adjoint(const T* __restrict__ ref, const float* __restrict__ mask,
-                                                    const float* __restrict__ h, int n,
-                                                    const AdjPose* __restrict__ poses, double* __restrict__ sums) {
-  __shared__ AdjPose sp;
-  __shared__ double red[kAdjSums][8];
-  const int pose = blockIdx.y;
-  if (threadIdx.x == 0) sp = poses[pose];
-  __syncthreads();
+__device__ __forceinline__ void adj_accumulate(const T* __restrict__ ref, const float* __restrict__ mask,
+                                               const float* __restrict__ h, int n, const AdjPose& sp,
+                                               float acc[kAdjSums]) {
   const int c = n / 2;
   const long nv = (long)n * n * n;
-  float acc[kAdjSums];
-#pragma unroll
-  for (int k = 0; k < kAdjSums; ++k) acc[k] = 0.f;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nv; i += (long)gridDim.x * blockDim.x) {
     const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((long)n * n));
     const float u0 = (float)(x - c) - sp.t[0], u1 = (float)(y - c) - sp.t[1], u2 = (float)(z - c) - sp.t[2];
@@ -75,7 +77,22 @@ __global__ void __launch_bounds__(256) k_cc_adjoint(const T* __restrict__ ref, c
       acc[14 + 3 * j] += gk;
     }
   }
-  // block reduction in FP64
+}
+
+// One block-row (blockIdx.y) per item; partial sums reduced in FP64 and added atomically.
+__global__ void __launch_bounds__(256) k_cc_adjoint(const AdjItem* __restrict__ items, double* __restrict__ sums) {
+  __shared__ AdjItem it;
+  __shared__ double red[kAdjSums][8];
+  const int item = blockIdx.y;
+  if (threadIdx.x == 0) it = items[item];
+  __syncthreads();
+  float acc[kAdjSums];
+#pragma unroll
+  for (int k = 0; k < kAdjSums; ++k) acc[k] = 0.f;
+  if (it.dtype == EMC_DTYPE_F32)
+    adj_accumulate(reinterpret_cast<const float*>(it.ref), it.mask, it.h, it.n, it.pose, acc);
+  else
+    adj_accumulate(reinterpret_cast<const __nv_bfloat16*>(it.ref), it.mask, it.h, it.n, it.pose, acc);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
   for (int k = 0; k < kAdjSums; ++k) {
@@ -88,7 +105,7 @@ __global__ void __launch_bounds__(256) k_cc_adjoint(const T* __restrict__ ref, c
   if (threadIdx.x < kAdjSums) {
     double t = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
-    atomicAdd(sums + (long)pose * kAdjSums + threadIdx.x, t);
+    atomicAdd(sums + (long)item * kAdjSums + threadIdx.x, t);
   }
 }
 
@@ -152,51 +169,60 @@ emc_status emc_search_reference_info(emc_search_t s, int ref_id, const void** da
 
 extern "C" {
 
-emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, double energy_p, const double prior[9],
-                          const double* poses, int n_poses, double* h_cc, double* h_grad, void* stream) {
-  EMC_CHECK_ARG(s && d_h && prior && poses && h_cc && h_grad, "emc_cc_adjoint: null argument");
-  EMC_CHECK_ARG(n_poses > 0 && n_poses <= 65535, "emc_cc_adjoint: n_poses %d", n_poses);
-  EMC_CHECK_ARG(energy_p > 0.0, "emc_cc_adjoint: energy must be > 0");
-  const void* data = nullptr;
-  const float* mask = nullptr;
-  int n = 0, dtype = 0;
-  EMC_TRY(emc_search_reference_info(s, ref_id, &data, &mask, &n, &dtype));
+emc_status emc_cc_adjoint_batch(emc_search_t s, int n_items, const int* ref_ids, const float* const* d_h,
+                                const double* energy_p, const double* priors, const double* poses, double* h_cc,
+                                double* h_grad, void* stream) {
+  EMC_CHECK_ARG(s && ref_ids && d_h && energy_p && priors && poses && h_cc && h_grad,
+                "emc_cc_adjoint_batch: null argument");
+  EMC_CHECK_ARG(n_items > 0 && n_items <= 65535, "emc_cc_adjoint_batch: n_items %d", n_items);
+  std::vector<emc::AdjItem> items(n_items);
+  int max_n = 0;
+  for (int i = 0; i < n_items; ++i) {
+    EMC_CHECK_ARG(d_h[i], "emc_cc_adjoint_batch: item %d has no template", i);
+    EMC_CHECK_ARG(energy_p[i] > 0.0, "emc_cc_adjoint_batch: item %d energy must be > 0", i);
+    const void* data = nullptr;
+    const float* mask = nullptr;
+    int n = 0, dtype = 0;
+    EMC_TRY(emc_search_reference_info(s, ref_ids[i], &data, &mask, &n, &dtype));
+    items[i].ref = data;
+    items[i].mask = mask;
+    items[i].h = d_h[i];
+    items[i].n = n;
+    items[i].dtype = dtype;
+    emc::pose_matrices(priors + 9 * (size_t)i, poses + 6 * (size_t)i, &items[i].pose);
+    max_n = std::max(max_n, n);
+  }
   cudaStream_t st = emc::as_stream(stream);
-  std::vector<emc::AdjPose> hp(n_poses);
-  for (int i = 0; i < n_poses; ++i) emc::pose_matrices(prior, poses + 6 * i, &hp[i]);
-  const size_t pose_bytes = sizeof(emc::AdjPose) * n_poses;
-  const size_t sum_bytes = sizeof(double) * emc::kAdjSums * n_poses;
+  const size_t item_bytes = sizeof(emc::AdjItem) * n_items;
+  const size_t sum_bytes = sizeof(double) * emc::kAdjSums * n_items;
   char* buf = nullptr;
-  EMC_CUDA(cudaMallocAsync(&buf, pose_bytes + sum_bytes + 64, st));
-  emc::AdjPose* d_poses = reinterpret_cast<emc::AdjPose*>(buf);
-  double* d_sums = reinterpret_cast<double*>(buf + ((pose_bytes + 15) / 16) * 16);
-  std::vector<double> sums((size_t)emc::kAdjSums * n_poses);
+  EMC_CUDA(cudaMallocAsync(&buf, item_bytes + sum_bytes + 64, st));
+  emc::AdjItem* d_items = reinterpret_cast<emc::AdjItem*>(buf);
+  double* d_sums = reinterpret_cast<double*>(buf + ((item_bytes + 15) / 16) * 16);
+  std::vector<double> sums((size_t)emc::kAdjSums * n_items);
   emc_status rs = EMC_OK;
-  if (cudaMemcpyAsync(d_poses, hp.data(), pose_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+  if (cudaMemcpyAsync(d_items, items.data(), item_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemsetAsync(d_sums, 0, sum_bytes, st) != cudaSuccess) {
-    emc::set_error("emc_cc_adjoint: upload failed");
+    emc::set_error("emc_cc_adjoint_batch: upload failed");
     rs = EMC_E_CUDA;
   }
   if (rs == EMC_OK) {
-    const long nv = (long)n * n * n;
-    const int bx = (int)std::max<long>(1, std::min<long>((nv + 2047) / 2048, 2L * emc::device_sm_count()));
-    dim3 grid(bx, n_poses);
-    if (dtype == EMC_DTYPE_F32)
-      emc::k_cc_adjoint<float><<<grid, 256, 0, st>>>((const float*)data, mask, d_h, n, d_poses, d_sums);
-    else
-      emc::k_cc_adjoint<__nv_bfloat16><<<grid, 256, 0, st>>>((const __nv_bfloat16*)data, mask, d_h, n, d_poses,
-                                                             d_sums);
+    const long nv = (long)max_n * max_n * max_n;
+    // enough blocks per item to fill the GPU without starving the reduction
+    const long want = std::max<long>(1, (4L * emc::device_sm_count() + n_items - 1) / n_items);
+    const int bx = (int)std::max<long>(1, std::min<long>((nv + 2047) / 2048, want));
+    emc::k_cc_adjoint<<<dim3(bx, n_items), 256, 0, st>>>(d_items, d_sums);
     if (cudaGetLastError() != cudaSuccess ||
         cudaMemcpyAsync(sums.data(), d_sums, sum_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
-      emc::set_error("emc_cc_adjoint: kernel or copy failed");
+      emc::set_error("emc_cc_adjoint_batch: kernel or copy failed");
       rs = EMC_E_CUDA;
     }
   }
   cudaFreeAsync(buf, st);
   if (rs != EMC_OK) return rs;
-  const double n3 = (double)n * n * n;
-  for (int i = 0; i < n_poses; ++i) {
+  for (int i = 0; i < n_items; ++i) {
+    const double n3 = (double)items[i].n * items[i].n * items[i].n;
     const double* q = &sums[(size_t)emc::kAdjSums * i];
     const double A = q[0], S1 = q[1], S2 = q[2];
     const double er = n3 * S2 - S1 * S1;
@@ -205,7 +231,7 @@ emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, double e
       for (int k = 0; k < 6; ++k) h_grad[6 * i + k] = NAN;
       continue;
     }
-    const double norm = 1.0 / sqrt(er * energy_p);
+    const double norm = 1.0 / sqrt(er * energy_p[i]);
     const double cc = A * norm;
     h_cc[i] = cc;
     for (int k = 0; k < 6; ++k) {
@@ -214,6 +240,18 @@ emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, double e
     }
   }
   return EMC_OK;
+}
+
+emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, double energy_p, const double prior[9],
+                          const double* poses, int n_poses, double* h_cc, double* h_grad, void* stream) {
+  EMC_CHECK_ARG(s && d_h && prior && poses && h_cc && h_grad, "emc_cc_adjoint: null argument");
+  EMC_CHECK_ARG(n_poses > 0 && n_poses <= 65535, "emc_cc_adjoint: n_poses %d", n_poses);
+  std::vector<int> ids(n_poses, ref_id);
+  std::vector<const float*> hs(n_poses, d_h);
+  std::vector<double> en(n_poses, energy_p), pr(9 * (size_t)n_poses);
+  for (int i = 0; i < n_poses; ++i)
+    for (int k = 0; k < 9; ++k) pr[9 * (size_t)i + k] = prior[k];
+  return emc_cc_adjoint_batch(s, n_poses, ids.data(), hs.data(), en.data(), pr.data(), poses, h_cc, h_grad, stream);
 }
 
 }  // extern "C"

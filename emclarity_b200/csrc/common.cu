@@ -19,7 +19,9 @@ void set_error(const char* fmt, ...) {
 
 namespace {
 constexpr int kMaxDevices = 64;
-constexpr int kLengths[] = {2, 3, 4, 6, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512};
+#define EMC_LEN_ITEM(L) L,
+constexpr int kLengths[] = {EMC_FOR_EACH_LENGTH(EMC_LEN_ITEM)};
+#undef EMC_LEN_ITEM
 constexpr int kNumLengths = sizeof(kLengths) / sizeof(kLengths[0]);
 
 struct DeviceTables {

@@ -42,11 +42,19 @@ void set_error(const char* fmt, ...);
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-// True for the FFT edge lengths compiled into this library.
+// FFT edge lengths compiled into this library: 2^a 3^b up to 512 used by the search plus the
+// "nextBest" sizes of coordinates/BH_multi_iterator.m:3-5 (factors 5, 7, 13).
+#define EMC_FOR_EACH_LENGTH(X) \
+  X(2) X(3) X(4) X(6) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(72) X(80) X(84) X(90) X(96) \
+  X(108) X(112) X(120) X(126) X(128) X(144) X(160) X(162) X(168) X(180) X(192) X(216) X(224) X(240) X(252) X(256) \
+  X(270) X(288) X(320) X(324) X(336) X(360) X(378) X(384) X(400) X(416) X(432) X(448) X(480) X(486) X(504) X(512)
+
 inline bool fft_length_supported(int n) {
   switch (n) {
-    case 1: case 2: case 3: case 4: case 6: case 8: case 12: case 16: case 24: case 32: case 48:
-    case 64: case 96: case 128: case 192: case 256: case 384: case 512:
+    case 1:
+#define EMC_CASE(L) case L:
+    EMC_FOR_EACH_LENGTH(EMC_CASE)
+#undef EMC_CASE
       return true;
     default:
       return false;

@@ -140,8 +140,8 @@ __global__ void k_sf3d_accum(const float* __restrict__ imgs, const float2* __res
 
 // Binary Y-tilt-axis missing wedge of masking/BH_weightMask3d.m:103-120 on the half spectrum
 // (FFT order), without the Gaussian smoothing: theta = atan2d(kx, kz) is excluded inside the
-// +/-(90 - tilt) cones around kz; the |kx|,|kz| <= 2 slab through the origin is kept; zero
-// beyond the Nyquist sphere (BH_bandpass3d 'nyquist').  Optionally times the 3-D CTF of |k|
+// +/-(90 - tilt) cones around kz; the |kx|,|kz| <= 2 slab through the origin is kept; times the
+// 'nyquist' radial window of BH_bandpass3d (:124-131 of BH_weightMask3d.m).  Optionally times the 3-D CTF of |k|
 // (ctf.cu:45-62 with the radius taken in 3-D).
 __global__ void k_wedge_ctf(int n, float max_cone, float min_cone, int use_ctf, int squared, const CtfDev c,
                             float inv_box_pix, float* __restrict__ out) {
@@ -158,7 +158,13 @@ __global__ void k_wedge_ctf(int n, float max_cone, float min_cone, int use_ctf, 
     float w = excluded ? 0.f : 1.f;
     if (abs(kx) <= 2 && abs(kz) <= 2) w = 1.f;
     const float r2i = (float)(kx * kx + ky * ky + kz * kz);
-    if (r2i > 0.25f * (float)n * (float)n) w = 0.f;
+    // BH_bandpass3d(size, 0, 0, 0, METHOD, 'nyquist'): 1 below 0.485 cycles/pixel, Gaussian
+    // roll-off of width 1.5/n beyond (masking/BH_bandpass3d.m:60-77, :88-92)
+    const float rn = sqrtf(r2i) / (float)n;
+    if (rn >= 0.485f) {
+      const float roll = 1.5f / (float)n;
+      w *= expf(-(rn - 0.485f) * (rn - 0.485f) / (2.f * roll * roll));
+    }
     if (use_ctf && w != 0.f) {
       const float r2 = r2i * inv_box_pix * inv_box_pix;
       const float v = sinf(c.cs_term * (r2 * r2) - c.df_term * r2 * c.df1 - c.amp_phase);

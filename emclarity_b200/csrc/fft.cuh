@@ -124,7 +124,80 @@ template <int SIGN> struct Dft<16, SIGN> {
   }
 };
 
+// cos / sin(2 pi j / R) for the odd prime radices 5, 7 and 13 (exact values rounded to float).
+__host__ __device__ constexpr float prime_cos(int R, int j) {
+  return R == 5 ? (j == 0 ? 1.f : j == 1 ? 3.09016994374947451e-01f : j == 2 ? -8.09016994374947340e-01f
+                 : j == 3 ? -8.09016994374947562e-01f : 3.09016994374947229e-01f)
+       : R == 7 ? (j == 0 ? 1.f : j == 1 ? 6.23489801858733594e-01f : j == 2 ? -2.22520933956314337e-01f
+                 : j == 3 ? -9.00968867902419035e-01f : j == 4 ? -9.00968867902419146e-01f
+                 : j == 5 ? -2.22520933956314587e-01f : 6.23489801858733372e-01f)
+                : (j == 0 ? 1.f : j == 1 ? 8.85456025653209911e-01f : j == 2 ? 5.68064746731155923e-01f
+                 : j == 3 ? 1.20536680255323006e-01f : j == 4 ? -3.54604887042535455e-01f
+                 : j == 5 ? -7.48510748171101192e-01f : j == 6 ? -9.70941817426052012e-01f
+                 : j == 7 ? -9.70941817426052123e-01f : j == 8 ? -7.48510748171101303e-01f
+                 : j == 9 ? -3.54604887042535899e-01f : j == 10 ? 1.20536680255323200e-01f
+                 : j == 11 ? 5.68064746731154813e-01f : 8.85456025653210022e-01f);
+}
+__host__ __device__ constexpr float prime_sin(int R, int j) {
+  return R == 5 ? (j == 0 ? 0.f : j == 1 ? 9.51056516295153531e-01f : j == 2 ? 5.87785252292473248e-01f
+                 : j == 3 ? -5.87785252292473026e-01f : -9.51056516295153642e-01f)
+       : R == 7 ? (j == 0 ? 0.f : j == 1 ? 7.81831482468029804e-01f : j == 2 ? 9.74927912181823619e-01f
+                 : j == 3 ? 4.33883739117558231e-01f : j == 4 ? -4.33883739117558009e-01f
+                 : j == 5 ? -9.74927912181823619e-01f : -7.81831482468029915e-01f)
+                : (j == 0 ? 0.f : j == 1 ? 4.64723172043768507e-01f : j == 2 ? 8.22983865893656352e-01f
+                 : j == 3 ? 9.92708874098053973e-01f : j == 4 ? 9.35016242685414833e-01f
+                 : j == 5 ? 6.63122658240795193e-01f : j == 6 ? 2.39315664287557683e-01f
+                 : j == 7 ? -2.39315664287557434e-01f : j == 8 ? -6.63122658240794971e-01f
+                 : j == 9 ? -9.35016242685414722e-01f : j == 10 ? -9.92708874098053973e-01f
+                 : j == 11 ? -8.22983865893657018e-01f : -4.64723172043768396e-01f);
+}
+
+// Odd prime radix: pairs (r, R-r) share the cosine term, X_q = x0 + sum_r [(x_r + x_{R-r}) cos
+// + i SIGN (x_r - x_{R-r}) sin] with the angle 2 pi (q r mod R) / R.
+template <int R, int SIGN>
+struct DftPrime {
+  static __host__ __device__ __forceinline__ void run(float2* v) {
+    constexpr int H = (R - 1) / 2;
+    float2 t1[H], t2[H];
+#pragma unroll
+    for (int r = 1; r <= H; ++r) {
+      t1[r - 1] = cadd(v[r], v[R - r]);
+      t2[r - 1] = csub(v[r], v[R - r]);
+    }
+    const float2 x0 = v[0];
+    float2 s0 = x0;
+#pragma unroll
+    for (int r = 0; r < H; ++r) s0 = cadd(s0, t1[r]);
+#pragma unroll
+    for (int q = 1; q < R; ++q) {
+      float2 acc = x0;
+#pragma unroll
+      for (int r = 1; r <= H; ++r) {
+        const float c = prime_cos(R, (q * r) % R), s = (float)SIGN * prime_sin(R, (q * r) % R);
+        acc.x = fmaf(t1[r - 1].x, c, fmaf(-t2[r - 1].y, s, acc.x));
+        acc.y = fmaf(t1[r - 1].y, c, fmaf(t2[r - 1].x, s, acc.y));
+      }
+      v[q] = acc;
+    }
+    v[0] = s0;
+  }
+};
+template <int SIGN> struct Dft<5, SIGN> : DftPrime<5, SIGN> {};
+template <int SIGN> struct Dft<7, SIGN> : DftPrime<7, SIGN> {};
+template <int SIGN> struct Dft<13, SIGN> : DftPrime<13, SIGN> {};
+
 // ---------------------------------------------------------------- plans
+// Generic plan for lengths without an explicit entry: radix-8 stages for the power of two (a 4
+// or a 2 closes it), then 3s, 5s, 7s and 13s.  1 past the last stage, 0 for another prime factor.
+__host__ __device__ constexpr int next_radix(int rem) {
+  return rem % 8 == 0 ? 8 : rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2 : rem % 3 == 0 ? 3 : rem % 5 == 0 ? 5
+       : rem % 7 == 0 ? 7 : rem % 13 == 0 ? 13 : 0;
+}
+__host__ __device__ constexpr int radix_seq_rem(int rem, int s) {
+  return rem == 1 ? 1 : next_radix(rem) == 0 ? 0 : s == 0 ? next_radix(rem) : radix_seq_rem(rem / next_radix(rem), s - 1);
+}
+__host__ __device__ constexpr int radix_seq(int L, int s) { return L < 2 ? 0 : radix_seq_rem(L, s); }
+
 // Radix sequence per supported length.  Stage s uses radix radix_of(L, s); 1 ends the plan.
 __host__ __device__ constexpr int radix_of(int L, int s) {
   return L == 2   ? (s == 0 ? 2 : 1)
@@ -144,15 +217,16 @@ __host__ __device__ constexpr int radix_of(int L, int s) {
        : L == 256 ? (s == 0 ? 16 : s == 1 ? 16 : 1)
        : L == 384 ? (s == 0 ? 16 : s == 1 ? 8 : s == 2 ? 3 : 1)
        : L == 512 ? (s == 0 ? 8 : s == 1 ? 8 : s == 2 ? 8 : 1)
-       : 0;
+       // the remaining "nextBest" FFT sizes of coordinates/BH_multi_iterator.m:3-5 (factors 5, 7, 13)
+       : radix_seq(L, s);
 }
 
 // Largest radix of a plan; used to pick a team size.
-__host__ __device__ constexpr int min_butterflies(int L) {
-  return (radix_of(L, 0) == 0) ? 0
-         : (L / (radix_of(L, 0) > radix_of(L, 1) ? (radix_of(L, 0) > radix_of(L, 2) ? radix_of(L, 0) : radix_of(L, 2))
-                                                 : (radix_of(L, 1) > radix_of(L, 2) ? radix_of(L, 1) : radix_of(L, 2))));
+__host__ __device__ constexpr int max_radix(int L, int s = 0) {
+  return radix_of(L, s) <= 1 ? 1
+         : (radix_of(L, s) > max_radix(L, s + 1) ? radix_of(L, s) : max_radix(L, s + 1));
 }
+__host__ __device__ constexpr int min_butterflies(int L) { return radix_of(L, 0) == 0 ? 0 : L / max_radix(L); }
 
 // Default team size: a power of two no larger than the smallest butterfly count, <= 32.
 __host__ __device__ constexpr int team_size(int L) {

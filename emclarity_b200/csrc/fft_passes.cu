@@ -6,8 +6,6 @@
 
 namespace emc {
 
-#define EMC_FOR_EACH_LENGTH(X) \
-  X(2) X(3) X(4) X(6) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
 
 static int grid_for(long work_items, int per_block) {
   long b = (work_items + per_block - 1) / per_block;

@@ -176,7 +176,7 @@ static emc_status c2r_mip_any(int L, const float2* in, long nrows, const double*
                               float* peak, float* angle, cudaStream_t st) {
   switch (L) {
 #define X(n) case n: return launch_c2r_mip<n>(in, nrows, stats, nvox, angle_id, peak, angle, st);
-    X(2) X(3) X(4) X(6) X(8) X(12) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
+    EMC_FOR_EACH_LENGTH(X)
 #undef X
   }
   set_error("template search: edge %d not supported", L);

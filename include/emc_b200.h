@@ -150,12 +150,49 @@ EMC_API emc_status emc_sf3d(int half, int squared, const unsigned size[3], const
 
 /* Per-particle Fourier weight on the half spectrum ((n/2+1)*n*n floats, FFT order): the
  * binary Y-tilt-axis missing wedge of BH_weightMask3d 'binaryWedge' (masking/BH_weightMask3d.m:
- * 103-120; cones of +/-(90-|tilt|) around kz removed, |kx|,|kz| <= 2 slab kept, zero beyond
- * Nyquist; the Gaussian smoothing of :124-131 is not applied) times, when ctf != NULL, the CTF
+ * 103-120; cones of +/-(90-|tilt|) around kz removed, |kx|,|kz| <= 2 slab kept, times the
+ * 'nyquist' window of BH_bandpass3d; the Gaussian smoothing of :124-131 is not applied) times,
+ * when ctf != NULL, the CTF
  * of the 3-D spatial frequency (mexFiles/utils/ctf.cu:45-62; defocus1 used, no astigmatism),
  * squared when squared != 0. */
 EMC_API emc_status emc_wedge_ctf_weight(int n, float tilt_min_deg, float tilt_max_deg, const emc_ctf_params* ctf,
                                         int squared, float* d_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Volume and spectrum operators around the search                          */
+/* ------------------------------------------------------------------------ */
+
+/* BH_padZeros3d(IMAGE, padLow, padTop, 'GPU', 'single'|'singleTaper', fill)
+ * (masking/BH_padZeros3d.m:79-229): negative pads trim, positive pads add `fill`; taper != 0
+ * blends the 7 outermost voxels of every face towards `fill` with 0.5+0.5cos((0:6)pi/7).
+ * d_out: (nx+pl+pt) x ... floats. */
+EMC_API emc_status emc_pad3d(const float* d_in, int nx, int ny, int nz, const int pad_low[3], const int pad_top[3],
+                             float fill, int taper, float* d_out, void* stream);
+/* BH_bandpass3d(SIZE, HIGH_THRESH, HIGH_CUT, LOW_CUT, 'GPU', PIXEL_SIZE) (masking/BH_bandpass3d.m:
+ * 54-170) on the half spectrum (FFT order).  pixel_size > 0: cut-offs in Angstrom; pixel_size == 0:
+ * 'nyquist'; pixel_size < 0: 'nyquistHigh'. */
+EMC_API emc_status emc_bandpass3d(int nx, int ny, int nz, float high_thresh, float high_cut, float low_cut,
+                                  float pixel_size, float* d_out, void* stream);
+/* BH_bandLimitCenterNormalize(IMG, BANDPASS, [], PAD, 'single'|'singleTaper')
+ * (masking/BH_bandLimitCenterNormalize.m:40-61): pad with the image mean, fftn, F(0) = 0, times the
+ * bandpass (half spectrum or NULL), F / (sqrt(sum |F|^2) / numel).  Output: half spectrum. */
+EMC_API emc_status emc_band_limit_center_normalize(const float* d_img, int nx, int ny, int nz,
+                                                   const int pad_low[3], const int pad_top[3], int taper,
+                                                   const float* d_bandpass, float* d_spectrum_out,
+                                                   void* stream);
+/* BH_multi_xcf_Rotational(rotPART_FT, REF_FT, wdgMask, refWdg) (statistics/BH_multi_xcf_Rotational.m:
+ * 71-78), unweighted form: sum Re(refWdg P R wdgMask) / sqrt(sum |R wdgMask|^2 sum |P refWdg|^2) over
+ * the full spectrum; R is the already-conjugated reference spectrum; weights may be NULL (= 1). */
+EMC_API emc_status emc_xcf_rotational(const float* d_part_ft, const float* d_ref_ft_conj, const float* d_wdg_mask,
+                                      const float* d_ref_wdg, int nx, int ny, int nz, double* h_cc,
+                                      void* stream);
+/* BH_multi_xcf_Translational(A, B, peakMask, peakCOM) (statistics/BH_multi_xcf_Translational.m:31-104):
+ * map = fftshift(real(ifftn(A .* B))), peakMask < 0.95 set to the map minimum, argmax (first index),
+ * two centre-of-mass passes on the (2 peakCOM + 1)^3 box of map - min, peak minus the origin.
+ * peak_mask (fftshifted, n^3) may be NULL; d_map_out (optional) receives the fftshifted map. */
+EMC_API emc_status emc_xcf_translational(const float* d_a, const float* d_b, int nx, int ny, int nz,
+                                         const float* d_peak_mask, int peak_com, double peak_out[3],
+                                         double* max_val, float* d_map_out, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Fused orientation search (BH_alignRaw3d_v2.m:1119-1423 inner body,        */
@@ -231,6 +268,7 @@ EMC_API emc_status emc_search_set_profiling(emc_search_t s, int enable);
 EMC_API emc_status emc_search_timings(emc_search_t s, double ms[4], long launches[4], long* evals,
                                       long* launches_last_run, int reset);
 
+
 /* ------------------------------------------------------------------------ */
 /* Forward + adjoint of the masked CC w.r.t. 3 Euler angles and 3 shifts      */
 /* ------------------------------------------------------------------------ */
@@ -247,6 +285,11 @@ EMC_API emc_status emc_particle_template(int n, const float* d_spectrum, float* 
 EMC_API emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, double energy_p,
                           const double prior[9], const double* poses, int n_poses,
                           double* h_cc, double* h_grad, void* stream);
+/* Batched form for many particles in one launch: item i uses reference ref_ids[i], template d_h[i]
+ * (device pointer), energy energy_p[i], prior priors[9i..9i+8] and pose poses[6i..6i+5]. */
+EMC_API emc_status emc_cc_adjoint_batch(emc_search_t s, int n_items, const int* ref_ids,
+                                        const float* const* d_h, const double* energy_p, const double* priors,
+                                        const double* poses, double* h_cc, double* h_grad, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Template search (BH_templateSearch3d_2.m:633-887)                          */

@@ -274,3 +274,93 @@ def euler_search_np(symmetry, theta_max, theta_step, psi_max, psi_step):
             for ps in psi:
                 out.append((math.fmod(ph, 360.0), th, ps))
     return np.array(out)
+
+
+def pad3d_np(img, pad_low, pad_top, fill=0.0, taper=False):
+    """BH_padZeros3d (masking/BH_padZeros3d.m:79-229), numeric fill, 'single' / 'singleTaper'.
+    Arrays are (z, y, x); pads are given (x, y, z)."""
+    img = np.asarray(img, dtype=np.float64)
+    pl = list(pad_low)[::-1]
+    pt = list(pad_top)[::-1]
+    sl = tuple(slice(max(-l, 0), img.shape[a] - max(-t, 0)) for a, (l, t) in enumerate(zip(pl, pt)))
+    im = img[sl].copy()
+    if taper:
+        tap = 0.5 + 0.5 * np.cos(np.arange(7) * np.pi / 7)     # 1 ... 0.0495
+        for a in range(3):
+            n = im.shape[a]
+            t = np.ones(n)
+            k = min(7, n)
+            t[:k] *= tap[::-1][:k]           # low side: first slice gets the smallest weight
+            t[n - k:] *= tap[:k]                 # high side: last slice gets the smallest weight
+            shape = [1, 1, 1]
+            shape[a] = n
+            t = t.reshape(shape)
+            im = im * t + fill * (1 - t)
+    out = np.full(tuple(s + max(l, 0) + max(t, 0) for s, l, t in zip(im.shape, pl, pt)), fill, dtype=np.float64)
+    out[max(pl[0], 0):max(pl[0], 0) + im.shape[0], max(pl[1], 0):max(pl[1], 0) + im.shape[1],
+        max(pl[2], 0):max(pl[2], 0) + im.shape[2]] = im
+    return out
+
+
+def bandpass3d_np(shape_xyz, high_thresh, high_cut, low_cut, pixel_size):
+    """BH_bandpass3d (masking/BH_bandpass3d.m:54-170) on the half spectrum, returned (z, y, x//2+1).
+    pixel_size > 0 numeric, 0 -> 'nyquist', < 0 -> 'nyquistHigh'."""
+    nx, ny, nz = shape_xyz
+    mn = min(nx, ny, nz) if nz > 1 else min(nx, ny)
+    hc = hr = 0.0
+    if pixel_size > 0:
+        if high_cut != 0:
+            hc = pixel_size / high_cut
+        lc = pixel_size / low_cut
+        if lc > 0:
+            lr = 2.0 / mn
+        else:
+            lc = abs(lc)
+            lr = math.sqrt(-(0.5 - lc) ** 2 / (2 * math.log(1e-3)))
+        if high_cut != 0:
+            hr = math.sqrt(-hc ** 2 / (2 * math.log(high_thresh)))
+    else:
+        if pixel_size < 0:
+            hc = 7.0 / mn
+            hr = math.sqrt(-hc ** 2 / (2 * math.log(1e-6)))
+        lr = 1.5 / mn
+        lc = 0.485 + low_cut
+    fz = np.fft.fftfreq(nz)[:, None, None] if nz > 1 else np.zeros((1, 1, 1))
+    fy = np.fft.fftfreq(ny)[None, :, None]
+    fx = (np.arange(nx // 2 + 1) / nx)[None, None, :]
+    r = np.sqrt(fx ** 2 + fy ** 2 + fz ** 2)
+    w = np.where(r < lc, 1.0, np.exp(-(r - lc) ** 2 / (2 * lr * lr)))
+    if hc != 0:
+        w = np.where(r <= hc, np.exp(-(r - hc) ** 2 / (2 * hr * hr)), w)
+    return w
+
+
+def band_limit_center_normalize_np(img, pad_low, pad_top, taper=False, bandpass=None):
+    """BH_bandLimitCenterNormalize (masking/BH_bandLimitCenterNormalize.m:40-61), half spectrum."""
+    p = pad3d_np(img, pad_low, pad_top, float(np.mean(np.asarray(img, dtype=np.float64))), taper)
+    F = np.fft.rfftn(p)
+    F.flat[0] = 0
+    if bandpass is not None:
+        F = F * bandpass
+    nx = p.shape[2]
+    hw = np.full(F.shape[2], 2.0)
+    hw[0] = 1.0
+    if nx % 2 == 0:
+        hw[-1] = 1.0
+    e = float(np.sum(hw[None, None, :] * np.abs(F) ** 2))
+    return F / (math.sqrt(e) / p.size)
+
+
+def xcf_rotational_np(P, R, wdg_mask=None, ref_wdg=None, nx=None):
+    """BH_multi_xcf_Rotational (statistics/BH_multi_xcf_Rotational.m:71-78) on half spectra."""
+    wm = 1.0 if wdg_mask is None else wdg_mask
+    rw = 1.0 if ref_wdg is None else ref_wdg
+    nx = nx if nx is not None else 2 * (P.shape[2] - 1)
+    hw = np.full(P.shape[2], 2.0)
+    hw[0] = 1.0
+    if nx % 2 == 0:
+        hw[-1] = 1.0
+    hw = hw[None, None, :]
+    num = np.sum(hw * np.real(rw * P * R * wm))
+    den = np.sum(hw * np.abs(R * wm) ** 2) * np.sum(hw * np.abs(P * rw) ** 2)
+    return num / math.sqrt(den)

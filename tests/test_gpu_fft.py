@@ -9,7 +9,9 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("shape", [(64, 64, 64), (96, 96, 96), (128, 128, 128), (16, 24, 32), (48, 12, 8),
-                                   (256, 64, 48), (8, 8, 512), (3, 6, 384), (64, 64, 2), (1, 1, 512), (1, 96, 192)])
+                                   (256, 64, 48), (8, 8, 512), (3, 6, 384), (64, 64, 2), (1, 1, 512), (1, 96, 192),
+                                   (80, 84, 90), (108, 112, 120), (126, 144, 160), (162, 168, 180),
+                                   (16, 416, 486), (8, 504, 400), (12, 378, 270)])
 def test_r2c_c2r_against_oracle(built_lib, cuda, shape):
     from emclarity_b200 import api
     rng = np.random.default_rng(sum(shape))
