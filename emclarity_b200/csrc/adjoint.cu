@@ -14,7 +14,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "interp.cuh"
+#include "search_kernels.cuh"
 
 namespace emc {
 
@@ -28,15 +28,50 @@ struct AdjPose {
 
 struct AdjItem {
   const void* ref;      // n^3 reference (float or bf16)
+  const void* cells;    // (n+1)^3 trilinear corner cells of the reference (same type) or null
   const float* mask;    // n^3 or null
   const float* h;       // n^3 real-space particle template
   int n;
   int dtype;
+  int interp;           // EMC_INTERP_CUBIC or EMC_INTERP_LINEAR (through the cells)
   AdjPose pose;
 };
 
+// Tricubic (Catmull-Rom) value and gradient from the plain volume.
 template <typename T>
-__device__ __forceinline__ void adj_accumulate(const T* __restrict__ ref, const float* __restrict__ mask,
+struct CubicSampler {
+  const T* ref;
+  int n;
+  __device__ __forceinline__ float operator()(float sx, float sy, float sz, float g[3]) const {
+    return sample_cubic_grad(ref, n, n, n, sx, sy, sz, g);
+  }
+};
+
+// Trilinear value and gradient (interpn semantics, zero outside [0, n-1]) from the corner cells.
+template <typename T>
+struct CellSampler {
+  const CellT<T>* cells;
+  int n;
+  __device__ __forceinline__ float operator()(float sx, float sy, float sz, float g[3]) const {
+    float f[3];
+    bool ok;
+    const long ci = cell_index<EMC_INTERP_LINEAR>(n, sx, sy, sz, f, &ok);
+    float v[8];
+    cell_values(load_cell(cells + ci), v);
+    const float c00 = fmaf(f[0], v[1] - v[0], v[0]), c10 = fmaf(f[0], v[3] - v[2], v[2]);
+    const float c01 = fmaf(f[0], v[5] - v[4], v[4]), c11 = fmaf(f[0], v[7] - v[6], v[6]);
+    const float c0 = fmaf(f[1], c10 - c00, c00), c1 = fmaf(f[1], c11 - c01, c01);
+    const float d0 = fmaf(f[1], (v[3] - v[2]) - (v[1] - v[0]), v[1] - v[0]);
+    const float d1 = fmaf(f[1], (v[7] - v[6]) - (v[5] - v[4]), v[5] - v[4]);
+    g[0] = ok ? fmaf(f[2], d1 - d0, d0) : 0.f;
+    g[1] = ok ? fmaf(f[2], (c11 - c01) - (c10 - c00), c10 - c00) : 0.f;
+    g[2] = ok ? c1 - c0 : 0.f;
+    return ok ? fmaf(f[2], c1 - c0, c0) : 0.f;
+  }
+};
+
+template <typename S>
+__device__ __forceinline__ void adj_accumulate(const S sampler, const float* __restrict__ mask,
                                                const float* __restrict__ h, int n, const AdjPose& sp,
                                                float acc[kAdjSums]) {
   const int c = n / 2;
@@ -48,9 +83,10 @@ __device__ __forceinline__ void adj_accumulate(const T* __restrict__ ref, const 
     const float sx = fmaf(m[0], u0, fmaf(m[1], u1, m[2] * u2)) + (float)c;
     const float sy = fmaf(m[3], u0, fmaf(m[4], u1, m[5] * u2)) + (float)c;
     const float sz = fmaf(m[6], u0, fmaf(m[7], u1, m[8] * u2)) + (float)c;
-    float g[3];
-    const float v = sample_cubic_grad(ref, n, n, n, sx, sy, sz, g);
     const float mk = mask ? __ldg(mask + i) : 1.f;
+    if (mk == 0.f) continue;  // a zero mask voxel adds nothing to any of the sums
+    float g[3];
+    const float v = sampler(sx, sy, sz, g);
     const float r = mk * v;
     const float hv = __ldg(h + i);
     g[0] *= mk; g[1] *= mk; g[2] *= mk;
@@ -89,10 +125,22 @@ __global__ void __launch_bounds__(256) k_cc_adjoint(const AdjItem* __restrict__ 
   float acc[kAdjSums];
 #pragma unroll
   for (int k = 0; k < kAdjSums; ++k) acc[k] = 0.f;
-  if (it.dtype == EMC_DTYPE_F32)
-    adj_accumulate(reinterpret_cast<const float*>(it.ref), it.mask, it.h, it.n, it.pose, acc);
-  else
-    adj_accumulate(reinterpret_cast<const __nv_bfloat16*>(it.ref), it.mask, it.h, it.n, it.pose, acc);
+  const bool lin = it.interp == EMC_INTERP_LINEAR && it.cells;
+  if (it.dtype == EMC_DTYPE_F32) {
+    if (lin)
+      adj_accumulate(CellSampler<float>{reinterpret_cast<const CellT<float>*>(it.cells), it.n}, it.mask, it.h,
+                     it.n, it.pose, acc);
+    else
+      adj_accumulate(CubicSampler<float>{reinterpret_cast<const float*>(it.ref), it.n}, it.mask, it.h, it.n,
+                     it.pose, acc);
+  } else {
+    if (lin)
+      adj_accumulate(CellSampler<__nv_bfloat16>{reinterpret_cast<const CellT<__nv_bfloat16>*>(it.cells), it.n},
+                     it.mask, it.h, it.n, it.pose, acc);
+    else
+      adj_accumulate(CubicSampler<__nv_bfloat16>{reinterpret_cast<const __nv_bfloat16*>(it.ref), it.n}, it.mask,
+                     it.h, it.n, it.pose, acc);
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
   for (int k = 0; k < kAdjSums; ++k) {
@@ -164,14 +212,15 @@ static void pose_matrices(const double prior[9], const double* pose, AdjPose* ou
 }  // namespace emc
 
 // Defined in search.cu: access to a registered reference.
-emc_status emc_search_reference_info(emc_search_t s, int ref_id, const void** data, const float** mask, int* n,
-                                     int* dtype);
+emc_status emc_search_reference_info(emc_search_t s, int ref_id, const void** data, const void** cells,
+                                     const float** mask, int* n, int* dtype);
 
 extern "C" {
 
 emc_status emc_cc_adjoint_batch(emc_search_t s, int n_items, const int* ref_ids, const float* const* d_h,
-                                const double* energy_p, const double* priors, const double* poses, double* h_cc,
-                                double* h_grad, void* stream) {
+                                const double* energy_p, const double* priors, const double* poses, int interp,
+                                double* h_cc, double* h_grad, void* stream) {
+  EMC_CHECK_ARG(interp == EMC_INTERP_LINEAR || interp == EMC_INTERP_CUBIC, "emc_cc_adjoint_batch: interp %d", interp);
   EMC_CHECK_ARG(s && ref_ids && d_h && energy_p && priors && poses && h_cc && h_grad,
                 "emc_cc_adjoint_batch: null argument");
   EMC_CHECK_ARG(n_items > 0 && n_items <= 65535, "emc_cc_adjoint_batch: n_items %d", n_items);
@@ -181,10 +230,13 @@ emc_status emc_cc_adjoint_batch(emc_search_t s, int n_items, const int* ref_ids,
     EMC_CHECK_ARG(d_h[i], "emc_cc_adjoint_batch: item %d has no template", i);
     EMC_CHECK_ARG(energy_p[i] > 0.0, "emc_cc_adjoint_batch: item %d energy must be > 0", i);
     const void* data = nullptr;
+    const void* cells = nullptr;
     const float* mask = nullptr;
     int n = 0, dtype = 0;
-    EMC_TRY(emc_search_reference_info(s, ref_ids[i], &data, &mask, &n, &dtype));
+    EMC_TRY(emc_search_reference_info(s, ref_ids[i], &data, &cells, &mask, &n, &dtype));
     items[i].ref = data;
+    items[i].cells = cells;
+    items[i].interp = interp;
     items[i].mask = mask;
     items[i].h = d_h[i];
     items[i].n = n;
@@ -251,7 +303,8 @@ emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, double e
   std::vector<double> en(n_poses, energy_p), pr(9 * (size_t)n_poses);
   for (int i = 0; i < n_poses; ++i)
     for (int k = 0; k < 9; ++k) pr[9 * (size_t)i + k] = prior[k];
-  return emc_cc_adjoint_batch(s, n_poses, ids.data(), hs.data(), en.data(), pr.data(), poses, h_cc, h_grad, stream);
+  return emc_cc_adjoint_batch(s, n_poses, ids.data(), hs.data(), en.data(), pr.data(), poses, EMC_INTERP_CUBIC, h_cc,
+                              h_grad, stream);
 }
 
 }  // extern "C"

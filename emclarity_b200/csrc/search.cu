@@ -204,6 +204,7 @@ struct emc_search_s {
     void* data = nullptr;
     float* mask = nullptr;
     float* wref = nullptr;
+    void* cells = nullptr;
     int n = 0;
     int dtype = 0;
   };
@@ -294,6 +295,19 @@ emc_status emc_search_add_reference(emc_search_t s, const float* d_ref, int n, c
   if (d_wref) {
     EMC_CUDA(cudaMalloc(&r.wref, nhalf * sizeof(float)));
     EMC_CUDA(cudaMemcpyAsync(r.wref, d_wref, nhalf * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  }
+  {
+    // trilinear corner cells for the linear interpolation modes
+    const long nc = (long)(n + 1) * (n + 1) * (n + 1);
+    const int blocks = (int)std::min<long>((nc + 255) / 256, 4L * emc::device_sm_count());
+    if (store_dtype == EMC_DTYPE_F32) {
+      EMC_CUDA(cudaMalloc(&r.cells, nc * sizeof(emc::CellT<float>)));
+      emc::k_build_cells<float><<<blocks, 256, 0, st>>>(d_ref, n, (emc::CellT<float>*)r.cells);
+    } else {
+      EMC_CUDA(cudaMalloc(&r.cells, nc * sizeof(emc::CellT<__nv_bfloat16>)));
+      emc::k_build_cells<__nv_bfloat16><<<blocks, 256, 0, st>>>(d_ref, n, (emc::CellT<__nv_bfloat16>*)r.cells);
+    }
+    EMC_LAUNCH_CHECK();
   }
   EMC_TRY(emc::set_attrs_any(n, store_dtype));
   if (!emc::device_twiddles(n)) return EMC_E_CUDA;
@@ -489,7 +503,7 @@ emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, in
   if (s->refs_dirty) {
     std::vector<emc::DevRef> dr(s->refs.size());
     for (size_t i = 0; i < s->refs.size(); ++i)
-      dr[i] = {s->refs[i].data, s->refs[i].mask, s->refs[i].wref, s->refs[i].n, s->refs[i].dtype};
+      dr[i] = {s->refs[i].data, s->refs[i].mask, s->refs[i].wref, s->refs[i].n, s->refs[i].dtype, s->refs[i].cells};
     EMC_TRY(s->d_refs.reserve(dr.size()));
     EMC_CUDA(cudaMemcpy(s->d_refs.p, dr.data(), sizeof(emc::DevRef) * dr.size(), cudaMemcpyHostToDevice));
     s->refs_dirty = false;
@@ -607,6 +621,7 @@ emc_status emc_search_destroy(emc_search_t s) {
     cudaFree(r.data);
     cudaFree(r.mask);
     cudaFree(r.wref);
+    cudaFree(r.cells);
   }
   s->d_refs.release();
   s->d_dmat.release();
@@ -653,12 +668,13 @@ emc_status emc_particle_template(int n, const float* d_spectrum, float* d_h, voi
 }  // extern "C"
 
 // Read access to a registered reference (used by the adjoint entry point).
-emc_status emc_search_reference_info(emc_search_t s, int ref_id, const void** data, const float** mask, int* n,
-                                     int* dtype) {
-  EMC_CHECK_ARG(s && data && mask && n && dtype, "emc_search_reference_info: null argument");
+emc_status emc_search_reference_info(emc_search_t s, int ref_id, const void** data, const void** cells,
+                                     const float** mask, int* n, int* dtype) {
+  EMC_CHECK_ARG(s && data && cells && mask && n && dtype, "emc_search_reference_info: null argument");
   EMC_CHECK_ARG(ref_id >= 0 && ref_id < (int)s->refs.size(), "reference id %d not registered", ref_id);
   const auto& r = s->refs[ref_id];
   *data = r.data;
+  *cells = r.cells;
   *mask = r.mask;
   *n = r.n;
   *dtype = r.dtype;

@@ -35,7 +35,100 @@ struct DevRef {
   const float* wref;   // nh*n*n or null
   int n;
   int dtype;
+  const void* cells;   // (n+1)^3 trilinear corner cells (see build_cells) or null
 };
+
+// Trilinear corner cells: cell (i, j, k), i, j, k in [-1, n-1], holds the 8 voxels
+// v(i+a, j+b, k+c), a, b, c in {0, 1}, in the order (000, 100, 010, 110, 001, 101, 011, 111),
+// zero outside the volume.  One 32-byte (FP32) or 16-byte (BF16) vector load fetches every
+// corner a trilinear sample needs, instead of eight scattered 4-byte loads.
+template <typename T>
+struct CellT;
+template <>
+struct CellT<float> {
+  float4 lo, hi;
+};
+template <>
+struct CellT<__nv_bfloat16> {
+  uint4 v;
+};
+
+__device__ __forceinline__ void cell_values(const CellT<float>& c, float v[8]) {
+  v[0] = c.lo.x; v[1] = c.lo.y; v[2] = c.lo.z; v[3] = c.lo.w;
+  v[4] = c.hi.x; v[5] = c.hi.y; v[6] = c.hi.z; v[7] = c.hi.w;
+}
+__device__ __forceinline__ void cell_values(const CellT<__nv_bfloat16>& c, float v[8]) {
+  const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&c.v);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float2 f = __bfloat1622float2(p[i]);
+    v[2 * i] = f.x;
+    v[2 * i + 1] = f.y;
+  }
+}
+__device__ __forceinline__ CellT<float> load_cell(const CellT<float>* p) {
+  CellT<float> c;
+  c.lo = __ldg(&p->lo);
+  c.hi = __ldg(&p->hi);
+  return c;
+}
+__device__ __forceinline__ CellT<__nv_bfloat16> load_cell(const CellT<__nv_bfloat16>* p) {
+  CellT<__nv_bfloat16> c;
+  c.v = __ldg(&p->v);
+  return c;
+}
+
+// Cell index and fractions of sample point s; `valid` follows interpn (MODE 0: 0 <= s <= n-1)
+// or the zero-border texture addressing (MODE 2: -1 < s < n).
+template <int MODE>
+__device__ __forceinline__ long cell_index(int n, float sx, float sy, float sz, float f[3], bool* valid) {
+  const bool ok = MODE == EMC_INTERP_LINEAR_BORDER
+                      ? (sx > -1.f && sy > -1.f && sz > -1.f && sx < (float)n && sy < (float)n && sz < (float)n)
+                      : (sx >= 0.f && sy >= 0.f && sz >= 0.f && sx <= (float)(n - 1) && sy <= (float)(n - 1) &&
+                         sz <= (float)(n - 1));
+  const float fx0 = floorf(sx), fy0 = floorf(sy), fz0 = floorf(sz);
+  const int x0 = max(-1, min((int)fx0, n - 1)), y0 = max(-1, min((int)fy0, n - 1)), z0 = max(-1, min((int)fz0, n - 1));
+  f[0] = sx - (float)x0;
+  f[1] = sy - (float)y0;
+  f[2] = sz - (float)z0;
+  *valid = ok;
+  const long nc = n + 1;
+  return ((long)(z0 + 1) * nc + (y0 + 1)) * nc + (x0 + 1);
+}
+
+// Same interpolation order as sample_linear, so both paths give identical results.
+__device__ __forceinline__ float cell_trilinear(const float v[8], const float f[3]) {
+  const float c00 = fmaf(f[0], v[1] - v[0], v[0]), c10 = fmaf(f[0], v[3] - v[2], v[2]);
+  const float c01 = fmaf(f[0], v[5] - v[4], v[4]), c11 = fmaf(f[0], v[7] - v[6], v[6]);
+  const float c0 = fmaf(f[1], c10 - c00, c00), c1 = fmaf(f[1], c11 - c01, c01);
+  return fmaf(f[2], c1 - c0, c0);
+}
+
+// Builds the corner cells of an n^3 FP32 volume, stored as T.
+template <typename T>
+__global__ void k_build_cells(const float* __restrict__ vol, int n, CellT<T>* __restrict__ cells) {
+  const long nc = n + 1;
+  const long total = nc * nc * nc;
+  for (long ci = blockIdx.x * (long)blockDim.x + threadIdx.x; ci < total; ci += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(ci % nc) - 1, j = (int)((ci / nc) % nc) - 1, k = (int)(ci / (nc * nc)) - 1;
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int x = i + (q & 1), y = j + ((q >> 1) & 1), z = k + ((q >> 2) & 1);
+      v[q] = (x >= 0 && y >= 0 && z >= 0 && x < n && y < n && z < n) ? vol[((long)z * n + y) * n + x] : 0.f;
+    }
+    CellT<T> c;
+    if constexpr (sizeof(T) == 4) {
+      reinterpret_cast<CellT<float>&>(c).lo = make_float4(v[0], v[1], v[2], v[3]);
+      reinterpret_cast<CellT<float>&>(c).hi = make_float4(v[4], v[5], v[6], v[7]);
+    } else {
+      __nv_bfloat162* p = reinterpret_cast<__nv_bfloat162*>(&reinterpret_cast<CellT<__nv_bfloat16>&>(c).v);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) p[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+    }
+    cells[ci] = c;
+  }
+}
 
 struct EvalItem {
   int particle;
@@ -102,6 +195,50 @@ __device__ __forceinline__ Tv block_sum(Tv v, Tv* red) {
   return t;  // valid in thread 0
 }
 
+// Gather of the G planes of pass A through corner cells: U voxels per thread per step, all cell
+// loads of a step issued before any is used (memory-level parallelism for L2-resident cells).
+template <int N, typename T, int MODE>
+__device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells, const float* __restrict__ mask,
+                                             const float m[9], float tx, float ty, float tz, int z0,
+                                             float* __restrict__ fplanes, double& s1, double& s2) {
+  using C = SearchCfg<N>;
+  constexpr int G = C::G, NT = C::NT_A, NH = C::NH, U = 4;
+  constexpr int TOTAL = G * N * N;
+  static_assert(TOTAL % (NT * U) == 0, "gather tiling");
+  constexpr int c = N / 2;
+  for (int base = threadIdx.x; base < TOTAL; base += NT * U) {
+    CellT<T> cv[U];
+    float fr[U][3];
+    bool ok[U];
+    float mk[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base + u * NT;
+      const int x = idx % N, y = (idx / N) % N, zl = idx / (N * N);
+      const int z = z0 + zl;
+      const float pu = (float)(x - c) - tx, pv = (float)(y - c) - ty, pw = (float)(z - c) - tz;
+      const float sx = fmaf(m[0], pu, fmaf(m[1], pv, m[2] * pw)) + (float)c;
+      const float sy = fmaf(m[3], pu, fmaf(m[4], pv, m[5] * pw)) + (float)c;
+      const float sz = fmaf(m[6], pu, fmaf(m[7], pv, m[8] * pw)) + (float)c;
+      const long ci = cell_index<MODE>(N, sx, sy, sz, fr[u], &ok[u]);
+      cv[u] = load_cell(cells + ci);
+      mk[u] = mask ? __ldg(mask + ((long)z * N + y) * N + x) : 1.f;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base + u * NT;
+      const int x = idx % N, y = (idx / N) % N, zl = idx / (N * N);
+      float v[8];
+      cell_values(cv[u], v);
+      float val = ok[u] ? cell_trilinear(v, fr[u]) : 0.f;
+      val *= mk[u];
+      fplanes[((size_t)zl * N + y) * (2 * NH) + x] = val;
+      s1 += (double)val;
+      s2 += (double)val * (double)val;
+    }
+  }
+}
+
 // ------------------------------------------------------------------ pass A
 template <int N, typename T>
 __global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const SearchChunkArgs a,
@@ -136,18 +273,26 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const Sear
   // 1. gather (x fastest: a warp walks 32 consecutive voxels of one row)
   double s1 = 0.0, s2 = 0.0;
   float* fplanes = reinterpret_cast<float*>(planes);
-  for (int idx = threadIdx.x; idx < G * N * N; idx += C::NT_A) {
-    const int x = idx % N, y = (idx / N) % N, zl = idx / (N * N);
-    const int z = z0 + zl;
-    const float u = (float)(x - c) - tx, v = (float)(y - c) - ty, w = (float)(z - c) - tz;
-    const float sx = fmaf(m[0], u, fmaf(m[1], v, m[2] * w)) + (float)c;
-    const float sy = fmaf(m[3], u, fmaf(m[4], v, m[5] * w)) + (float)c;
-    const float sz = fmaf(m[6], u, fmaf(m[7], v, m[8] * w)) + (float)c;
-    float val = sample(a.interp, src, N, N, N, sx, sy, sz);
-    if (mask) val *= __ldg(mask + ((long)z * N + y) * N + x);
-    fplanes[((size_t)zl * N + y) * (2 * NH) + x] = val;
-    s1 += (double)val;
-    s2 += (double)val * (double)val;
+  if (rf.cells && a.interp == EMC_INTERP_LINEAR) {
+    gather_cells<N, T, EMC_INTERP_LINEAR>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, m, tx, ty, tz, z0,
+                                          fplanes, s1, s2);
+  } else if (rf.cells && a.interp == EMC_INTERP_LINEAR_BORDER) {
+    gather_cells<N, T, EMC_INTERP_LINEAR_BORDER>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, m, tx, ty, tz,
+                                                 z0, fplanes, s1, s2);
+  } else {
+    for (int idx = threadIdx.x; idx < G * N * N; idx += C::NT_A) {
+      const int x = idx % N, y = (idx / N) % N, zl = idx / (N * N);
+      const int z = z0 + zl;
+      const float u = (float)(x - c) - tx, v = (float)(y - c) - ty, w = (float)(z - c) - tz;
+      const float sx = fmaf(m[0], u, fmaf(m[1], v, m[2] * w)) + (float)c;
+      const float sy = fmaf(m[3], u, fmaf(m[4], v, m[5] * w)) + (float)c;
+      const float sz = fmaf(m[6], u, fmaf(m[7], v, m[8] * w)) + (float)c;
+      float val = sample(a.interp, src, N, N, N, sx, sy, sz);
+      if (mask) val *= __ldg(mask + ((long)z * N + y) * N + x);
+      fplanes[((size_t)zl * N + y) * (2 * NH) + x] = val;
+      s1 += (double)val;
+      s2 += (double)val * (double)val;
+    }
   }
   {
     double t1 = block_sum(s1, red[0]);

@@ -286,10 +286,13 @@ EMC_API emc_status emc_cc_adjoint(emc_search_t s, int ref_id, const float* d_h, 
                           const double prior[9], const double* poses, int n_poses,
                           double* h_cc, double* h_grad, void* stream);
 /* Batched form for many particles in one launch: item i uses reference ref_ids[i], template d_h[i]
- * (device pointer), energy energy_p[i], prior priors[9i..9i+8] and pose poses[6i..6i+5]. */
+ * (device pointer), energy energy_p[i], prior priors[9i..9i+8] and pose poses[6i..6i+5].
+ * interp: EMC_INTERP_CUBIC (smooth, as emc_cc_adjoint) or EMC_INTERP_LINEAR (trilinear through the
+ * reference's corner cells, one vector load per voxel; piecewise-linear objective). */
 EMC_API emc_status emc_cc_adjoint_batch(emc_search_t s, int n_items, const int* ref_ids,
                                         const float* const* d_h, const double* energy_p, const double* priors,
-                                        const double* poses, double* h_cc, double* h_grad, void* stream);
+                                        const double* poses, int interp, double* h_cc, double* h_grad,
+                                        void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Template search (BH_templateSearch3d_2.m:633-887)                          */
