@@ -269,6 +269,22 @@ EMC_API emc_status emc_search_timings(emc_search_t s, double ms[4], long launche
                                       long* launches_last_run, int reset);
 
 
+/* Single-particle search that allocates no device memory.  No counterpart in the reference.
+ * For callers that may not call cudaMalloc after start-up: hosts whose own pool owns the GPU
+ * memory (MATLAB's gpuArray allocator, a framework caching allocator), where a raw allocation
+ * can fail or fragment the pool, and loops that must keep a bounded latency.  All scratch lives
+ * in one static 24 MiB device array per GPU (held from library load until exit).  The first call
+ * on a device resolves that array's address and uploads FFT twiddles (make it before any stream
+ * capture).  Every call reuses the same array, so calls that overlap on the GPU race; the call
+ * synchronises the stream before returning.  Limits (EMC_E_ARG beyond them): box 64, 96 or 128,
+ * FP32 reference, 1..4096 orientations (host (phi, theta, psi) triples), peak radius 1..15.
+ * Same arguments and outputs as emc_search_run for one particle (device outputs may be NULL). */
+EMC_API emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int n,
+                                            const float* d_spectrum, double energy, const double prior[9],
+                                            const float shift[3], const double* phi_theta_psi, int n_orient,
+                                            int peak_radius, int interp, float* d_cc, int* d_peak,
+                                            emc_search_hit* d_best, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Forward + adjoint of the masked CC w.r.t. 3 Euler angles and 3 shifts      */
 /* ------------------------------------------------------------------------ */
