@@ -394,6 +394,213 @@ def run_reference(args, world, rank):
     }
 
 
+# --------------------------------------------------------------------------------------------- other workloads
+def _timed(fn, reps=1):
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.time()
+    for _ in range(reps):
+        out = fn()
+    torch.cuda.synchronize()
+    return (time.time() - t0) / reps, out
+
+
+def run_mixed(args, store="f32"):
+    """Batched uneven alignment: 60% 64^3, 30% 96^3, 10% 128^3, 256 local orientations each, seeded
+    defocus in [1.5, 4] um and tilt range in [+-50, +-65] deg, one emc_search_run per step."""
+    import torch
+
+    from emclarity_b200 import api, synthetic
+    n_part = args.particles if args.particles != 1200 else 2000
+    sizes = synthetic.batched_sizes(n_part, seed=3)
+    rng = np.random.default_rng(2024)
+    grid = synthetic.local_grid(N_ORIENT, 8.0, 2.0)
+    s = api.Search(peak_radius=PEAK_RADIUS)
+    refs, fts = {}, {}
+    for n in (64, 96, 128):
+        ref = synthetic.blob_reference(rng, n)
+        mask = synthetic.soft_sphere_mask(n, 28 * n / 64)
+        rg = torch.from_numpy(ref).cuda()
+        refs[n] = (rg, s.add_reference(rg, torch.from_numpy(mask).cuda(), store=store))
+        fts[n] = api.FourierTransformer((n, n, n))
+    s.set_orientations(grid)
+    descs, keep = [], []
+    for n in sizes:
+        prior = api.define_matrix(synthetic.random_euler(rng), "inv")
+        truth = prior @ api.define_matrix([rng.uniform(-6, 6), rng.uniform(0, 6), rng.uniform(-6, 6)], "inv")
+        w = api.wedge_ctf_weight(int(n), -rng.uniform(50, 65), rng.uniform(50, 65),
+                                 synthetic.ctf_dict(rng.uniform(15000, 40000)))
+        p = synthetic.make_particle(refs[n][0], rng, truth, rng.integers(-4, 5, 3), w, 0.1, ft=fts[n])
+        q, e = api.particle_spectrum(p, w)
+        keep.append(q)
+        descs.append(s.particle(q, e.item(), refs[n][1], prior=prior, orient_count=N_ORIENT))
+        del p, w
+    evals = len(descs) * N_ORIENT
+    best = torch.empty((len(descs), 5), dtype=torch.int32, device="cuda")
+    for _ in range(args.warmup):
+        s.run(descs, best=best)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        s.run(descs, best=best)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    counts = {int(n): int(np.sum(sizes == n)) for n in (64, 96, 128)}
+    byts = sum(bytes_per_eval(n) * c * N_ORIENT for n, c in counts.items())
+    peak, which = measured_peaks()
+    return {"metric": "CC evals/s, batched uneven boxes" + (" (BF16 reference storage)" if store == "bf16" else ""),
+            "value": evals / (ms / 1e3), "unit": "CC evals/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": store,
+            "data": "synthetic", "config": {"workload": "%d particles (%s) x %d local orientations, one call" %
+                                            (len(descs), counts, N_ORIENT), "store": store},
+            "roofline": {"bound": "hbm", "achieved": byts / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": byts / (ms / 1e3) / 1e9 / peak, "peak_source": which}}
+
+
+def run_tsearch(args):
+    """Template search: 512x512x256 noise tomogram with 150 planted 48^3 copies, wedge + CTF (3 um),
+    every orientation of eulerSearch(C1, 180, 12, 48, 12) (2,592) over the full volume."""
+    import torch
+
+    from emclarity_b200 import api, synthetic
+    rng = np.random.default_rng(77)
+    nz, ny, nx = 256, 512, 512
+    t = 48
+    tmpl = synthetic.blob_reference(rng, t)
+    grid = api.euler_search("C1", 180, 12, 48, 12)
+    if args.particles != 1200:
+        grid = grid[:args.particles]
+    tomo = torch.randn((nz, ny, nx), device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))
+    tg = torch.from_numpy(tmpl).cuda()
+    ip = api.Interpolator(tg)
+    placed = []
+    tries = 0
+    while len(placed) < 150 and tries < 100000:
+        tries += 1
+        c = rng.integers([t, t, t], [nz - t, ny - t, nx - t])
+        if all(np.sum((c - q) ** 2) >= t * t for q in placed):
+            placed.append(c)
+    for c in placed:
+        o = grid[rng.integers(len(grid))]
+        rot = ip.interp3d(api.define_matrix([o[0], o[1], o[2] - o[0]], "forward"), (0, 0, 0), "forward")
+        z, y, x = (int(v) - t // 2 for v in c)
+        tomo[z:z + t, y:y + t, x:x + t] -= 2.0 * rot
+    ts = api.TemplateSearch(tomo.contiguous())
+    peak = torch.empty_like(tomo)
+    ang = torch.empty_like(tomo)
+    ts.run(tg, grid[:4], peak, ang)
+    dt, _ = _timed(lambda: ts.run(tg, grid, peak, ang))
+    per_orient = dt / len(grid)
+    byts = 8 * (nx // 2 + 1) * ny * nz + 16 * nx * ny * nz + 4 * t ** 3
+    pk, which = measured_peaks()
+    return {"metric": "template search orientations/s over 512x512x256", "value": len(grid) / dt,
+            "unit": "orientations/s", "n_gpus": 1, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "512x512x256 tomogram, 150 planted 48^3 templates, %d orientations" % len(grid)},
+            "roofline": {"bound": "hbm", "achieved": byts / per_orient / 1e9, "peak": pk, "unit": "GB/s",
+                         "frac": byts / per_orient / 1e9 / pk, "peak_source": which}}
+
+
+def _rodrigues(axis, deg):
+    a = np.asarray(axis, dtype=np.float64)
+    a = a / np.linalg.norm(a)
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    th = np.radians(deg)
+    return np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
+
+
+def run_refine(args):
+    """Gradient pose refinement: 96^3 particles at SNR 0.05, coarse 15-degree local search (95
+    orientations around a seeded prior within 12 degrees of the truth), then either 20 L-BFGS steps on
+    the forward + adjoint CC or a dense 1-degree local grid (3,859 orientations) around the coarse best;
+    wall-clock time and median pose error of both."""
+    import torch
+
+    from emclarity_b200 import api, refine, synthetic
+    n = 96
+    n_part = args.particles if args.particles != 1200 else 1000
+    rng = np.random.default_rng(96)
+    ref = synthetic.blob_reference(rng, n)
+    mask = synthetic.soft_sphere_mask(n, 28 * n / 64)
+    rg, mg = torch.from_numpy(ref).cuda(), torch.from_numpy(mask).cuda()
+    ft = api.FourierTransformer((n, n, n))
+    coarse = api.euler_search("C1", 30, 15, 30, 15)
+    dense = api.euler_search("C1", 8, 1, 8, 1)
+    s = api.Search(peak_radius=6)
+    rid = s.add_reference(rg, mg)
+    priors, truths, specs, hs, ens = [], [], [], [], []
+    for _ in range(n_part):
+        prior = api.define_matrix(synthetic.random_euler(rng), "inv")
+        jitter = _rodrigues(rng.standard_normal(3), rng.uniform(0, 12))
+        truth = prior @ jitter
+        w = api.wedge_ctf_weight(n, -60, 60, synthetic.ctf_dict(rng.uniform(15000, 40000)))
+        p = synthetic.make_particle(rg, rng, truth, rng.integers(-3, 4, 3), w, 0.05, ft=ft)
+        q, e = api.particle_spectrum(p, w)
+        priors.append(prior)
+        truths.append(truth)
+        specs.append(q)
+        ens.append(e.item())
+        hs.append(api.particle_template(q))
+    truths = np.array(truths)
+
+    def coarse_search():
+        s.set_orientations(coarse)
+        d = [s.particle(specs[i], ens[i], rid, prior=priors[i], orient_count=len(coarse)) for i in range(n_part)]
+        _, _, best = s.run_host(d)
+        return best
+
+    t_coarse, best = _timed(coarse_search)
+    Dc = [api.define_matrix([coarse[b[1]][0], coarse[b[1]][1], coarse[b[1]][2] - coarse[b[1]][0]], "inv")
+          for b in best]
+    R_coarse = np.array([priors[i] @ Dc[i] for i in range(n_part)])
+    err_coarse = refine.geodesic_deg(R_coarse, truths)
+
+    # (a) L-BFGS on the forward + adjoint, parameterised around the coarse best at theta = 90 deg
+    rx90 = api.define_matrix([0.0, -90.0, 0.0], "inv")
+    pri2 = [R_coarse[i] @ rx90 for i in range(n_part)]
+    x0 = np.array([[0.0, 90.0, 0.0] + [float(v) for v in best[i][2]] for i in range(n_part)])
+
+    def grad_refine(interp):
+        obj = refine.BatchObjective(s, [rid] * n_part, hs, ens, pri2, interp=interp)
+        x, f, hist = refine.lbfgs(obj, x0, n_iter=20)
+        return x, obj.evals
+
+    results = {}
+    for interp in ("linear", "cubic"):
+        t_ref, (x, nev) = _timed(lambda: grad_refine(interp))
+        R = np.array([pri2[i] @ api.define_matrix([x[i, 0], x[i, 1], x[i, 2] - x[i, 0]], "inv")
+                      for i in range(n_part)])
+        err = refine.geodesic_deg(R, truths)
+        results[interp] = {"seconds": t_ref, "median_err_deg": float(np.median(err)),
+                           "p90_err_deg": float(np.percentile(err, 90)), "objective_evals": int(nev)}
+
+    # (b) plain GPU grid search: dense 1-degree local grid around the coarse best
+    def dense_search():
+        s.set_orientations(dense)
+        d = [s.particle(specs[i], ens[i], rid, prior=R_coarse[i], orient_count=len(dense)) for i in range(n_part)]
+        _, _, bd = s.run_host(d)
+        return bd
+
+    t_dense, bd = _timed(dense_search)
+    R_dense = np.array([R_coarse[i] @ api.define_matrix(
+        [dense[b[1]][0], dense[b[1]][1], dense[b[1]][2] - dense[b[1]][0]], "inv") for i, b in enumerate(bd)])
+    err_dense = refine.geodesic_deg(R_dense, truths)
+    lin = results["linear"]
+    return {"metric": "pose-refine time at <= 0.5 deg median error", "value": lin["seconds"], "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "%d x 96^3 particles, SNR 0.05, coarse local 15-degree grid (%d orientations), "
+                                   "20 L-BFGS steps vs dense 1-degree grid (%d orientations)" %
+                                   (n_part, len(coarse), len(dense))},
+            "coarse": {"seconds": t_coarse, "median_err_deg": float(np.median(err_coarse))},
+            "lbfgs": results,
+            "dense_grid": {"seconds": t_dense, "median_err_deg": float(np.median(err_dense)),
+                           "p90_err_deg": float(np.percentile(err_dense, 90)), "evals": n_part * len(dense)},
+            "speedup_refine_phase": t_dense / lin["seconds"],
+            "speedup_total": (t_coarse + t_dense) / (t_coarse + lin["seconds"])}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -402,7 +609,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=1200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine"])
     args = ap.parse_args()
+    if args.impl == "ours" and args.workload != "batched64":
+        import torch
+        torch.cuda.set_device(0)
+        fn = {"mixed": run_mixed, "bf16": lambda a: run_mixed(a, "bf16"), "tsearch": run_tsearch,
+              "refine": run_refine}[args.workload]
+        print(json.dumps(fn(args)))
+        return
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))

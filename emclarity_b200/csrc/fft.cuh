@@ -246,7 +246,16 @@ __device__ __forceinline__ float2 twiddle(const float2* tw, int m) {
 // One Stockham stage of radix R on a line of length L; NS = product of earlier radices.
 // buf: line base, elements at buf[i * stride].  Every lane of the warp must call this
 // (inactive lanes pass active = false) because of the __syncwarp() calls.
-template <int L, int R, int NS, int SIGN, int P>
+// Physical slot of line element i.  With PAD, one spare slot follows every 8 elements: the
+// radix-8 first stage writes elements 8j + r, which without the gap would put the 8 lanes of a
+// team on 2 shared-memory banks.  padded_len(L) slots hold a padded line.
+template <int PAD>
+__host__ __device__ __forceinline__ constexpr int lpos(int i) {
+  return PAD ? i + (i >> 3) : i;
+}
+__host__ __device__ constexpr int padded_len(int L) { return L + L / 8; }
+
+template <int L, int R, int NS, int SIGN, int P, int PAD>
 __device__ __forceinline__ void stockham_stage(float2* buf, int stride, int lane, const float2* tw,
                                                bool active) {
   constexpr int NB = L / R;
@@ -257,7 +266,7 @@ __device__ __forceinline__ void stockham_stage(float2* buf, int stride, int lane
     const int j = lane + b * P;
     if (active && (PER * P == NB || j < NB)) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = buf[(j + r * NB) * stride];
+      for (int r = 0; r < R; ++r) v[b][r] = buf[lpos<PAD>(j + r * NB) * stride];
     }
   }
   __syncwarp();
@@ -273,32 +282,33 @@ __device__ __forceinline__ void stockham_stage(float2* buf, int stride, int lane
       Dft<R, SIGN>::run(v[b]);
       const int idx = (j / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) buf[(idx + r * NS) * stride] = v[b][r];
+      for (int r = 0; r < R; ++r) buf[lpos<PAD>(idx + r * NS) * stride] = v[b][r];
     }
   }
   __syncwarp();
 }
 
-template <int L, int SIGN, int P, int S, int NS>
+template <int L, int SIGN, int P, int PAD, int S, int NS>
 struct StageChain {
   static __device__ __forceinline__ void run(float2* buf, int stride, int lane, const float2* tw, bool active) {
     constexpr int R = radix_of(L, S);
-    stockham_stage<L, R, NS, SIGN, P>(buf, stride, lane, tw, active);
-    StageChain<L, SIGN, P, S + 1, NS * R>::run(buf, stride, lane, tw, active);
+    stockham_stage<L, R, NS, SIGN, P, PAD>(buf, stride, lane, tw, active);
+    StageChain<L, SIGN, P, PAD, S + 1, NS * R>::run(buf, stride, lane, tw, active);
   }
 };
 // terminate when the sub-transform length reaches L
-template <int L, int SIGN, int P, int S>
-struct StageChain<L, SIGN, P, S, L> {
+template <int L, int SIGN, int P, int PAD, int S>
+struct StageChain<L, SIGN, P, PAD, S, L> {
   static __device__ __forceinline__ void run(float2*, int, int, const float2*, bool) {}
 };
 
-// In-place complex FFT of one line held by a team of P lanes.
-template <int L, int SIGN, int P = team_size(L)>
+// In-place complex FFT of one line held by a team of P lanes.  Element i lives at
+// buf[lpos<PAD>(i) * stride].
+template <int L, int SIGN, int P = team_size(L), int PAD = 0>
 __device__ __forceinline__ void fft_line(float2* buf, int stride, int lane, const float2* tw, bool active) {
   static_assert(radix_of(L, 0) != 0, "unsupported FFT length");
   static_assert(P >= 1 && P <= 32 && (32 % P) == 0, "team must divide a warp");
-  StageChain<L, SIGN, P, 0, 1>::run(buf, stride, lane, tw, active);
+  StageChain<L, SIGN, P, PAD, 0, 1>::run(buf, stride, lane, tw, active);
 }
 
 // Loads the length-L twiddle table into shared memory (cooperatively, whole block).

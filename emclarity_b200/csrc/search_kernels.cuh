@@ -176,10 +176,26 @@ struct SearchCfg {
   static constexpr int TEAMS_A = NT_A / P;
   static constexpr int NT_BC = ((NH * P + 31) / 32) * 32;
   static constexpr int TEAMS_BC = NT_BC / P;
-  static constexpr size_t SMEM_A = sizeof(float2) * ((size_t)G * N * NH + (size_t)TEAMS_A * (N + 1) + N) + 64;
-  static constexpr size_t SMEM_B = sizeof(float2) * ((size_t)N * NH + N);
-  static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)N * NH + N + (size_t)TEAMS_BC * (N + 1));
+  // FFT lines use padded positions (lpos<1>): a strided line of N elements spans PY rows, a
+  // contiguous line buffer LP slots; LP = 8 (mod 16) puts neighbouring teams 16 banks apart.
+  static constexpr int PY = padded_len(N);
+  static constexpr int LP = PY + ((8 - PY % 16) + 16) % 16;
+  // teams with a line buffer for the row-pair transforms (pass A R2C, pass C C2R); the others
+  // idle during those loops, which keeps two pass-A CTAs per SM for every box size
+  static constexpr int TEAMS_LA = N <= 64 ? TEAMS_A : 16;
+  static constexpr int TEAMS_LC = 16;  // (2 r + 1 + 1) / 2 <= 16 row pairs for r <= 15
+  static constexpr size_t SMEM_A = sizeof(float2) * ((size_t)G * PY * NH + (size_t)TEAMS_LA * LP + N) + 64;
+  static constexpr size_t SMEM_B = sizeof(float2) * ((size_t)PY * NH + N);
+  static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
 };
+
+// Line li of a strided-FFT round handled by team `team`: consecutive teams get kx values 8
+// apart (NH is odd, so kx -> 8 kx mod NH is a permutation), which puts the teams of a warp on
+// different shared-memory banks.
+template <int NH>
+__device__ __forceinline__ int spread_kx(int li) {
+  return (li * 8) % NH;
+}
 
 template <typename Tv>
 __device__ __forceinline__ Tv block_sum(Tv v, Tv* red) {
@@ -232,7 +248,7 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
       cell_values(cv[u], v);
       float val = ok[u] ? cell_trilinear(v, fr[u]) : 0.f;
       val *= mk[u];
-      fplanes[((size_t)zl * N + y) * (2 * NH) + x] = val;
+      fplanes[((size_t)zl * C::PY + lpos<1>(y)) * (2 * NH) + x] = val;
       s1 += (double)val;
       s2 += (double)val * (double)val;
     }
@@ -246,9 +262,10 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const Sear
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, G = C::G, P = C::P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* planes = reinterpret_cast<float2*>(smem_raw);          // [G][N][NH]
-  float2* lines = planes + (size_t)G * N * NH;                    // [TEAMS][N+1]
-  float2* s_tw = lines + (size_t)C::TEAMS_A * (N + 1);             // [N]
+  constexpr int PY = C::PY, LP = C::LP;
+  float2* planes = reinterpret_cast<float2*>(smem_raw);          // [G][PY][NH], row y at lpos<1>(y)
+  float2* lines = planes + (size_t)G * PY * NH;                   // [TEAMS][LP]
+  float2* s_tw = lines + (size_t)C::TEAMS_LA * LP;                 // [N]
   float* s_m = reinterpret_cast<float*>(s_tw + N);                // 9 floats
   __shared__ double red[2][32];
 
@@ -289,7 +306,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const Sear
       const float sz = fmaf(m[6], u, fmaf(m[7], v, m[8] * w)) + (float)c;
       float val = sample(a.interp, src, N, N, N, sx, sy, sz);
       if (mask) val *= __ldg(mask + ((long)z * N + y) * N + x);
-      fplanes[((size_t)zl * N + y) * (2 * NH) + x] = val;
+      fplanes[((size_t)zl * PY + lpos<1>(y)) * (2 * NH) + x] = val;
       s1 += (double)val;
       s2 += (double)val * (double)val;
     }
@@ -308,21 +325,25 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const Sear
   // 2. R2C along x: rows 2q and 2q+1 of the slab share one complex FFT
   {
     constexpr int NPAIRS = G * N / 2;
-    float2* buf = lines + (size_t)team * (N + 1);
-    for (int base = 0; base < NPAIRS; base += C::TEAMS_A) {
+    const bool has_line = team < C::TEAMS_LA;
+    float2* buf = lines + (size_t)(has_line ? team : 0) * LP;
+    for (int base = 0; base < NPAIRS; base += C::TEAMS_LA) {
       const int q = base + team;
-      const bool active = q < NPAIRS;
-      const float* ra = fplanes + (size_t)(2 * q) * (2 * NH);
+      const bool active = has_line && q < NPAIRS;
+      // rows 2q, 2q+1 of the slab (same plane, adjacent padded rows since 2q+1 is odd)
+      const int zl = (2 * q) / N, ya = (2 * q) % N;
+      const size_t row_a = (size_t)zl * PY + lpos<1>(ya);
+      const float* ra = fplanes + row_a * (2 * NH);
       const float* rb = ra + 2 * NH;
       if (active)
-        for (int n = lane; n < N; n += P) buf[n] = make_float2(ra[n], rb[n]);
+        for (int n = lane; n < N; n += P) buf[lpos<1>(n)] = make_float2(ra[n], rb[n]);
       __syncwarp();
-      fft_line<N, -1, P>(buf, 1, lane, s_tw, active);
+      fft_line<N, -1, P, 1>(buf, 1, lane, s_tw, active);
       if (active) {
-        float2* oa = planes + (size_t)(2 * q) * NH;
+        float2* oa = planes + row_a * NH;
         float2* ob = oa + NH;
         for (int k = lane; k < NH; k += P) {
-          const float2 zk = buf[k], zm = buf[(N - k) % N];
+          const float2 zk = buf[lpos<1>(k)], zm = buf[lpos<1>((N - k) % N)];
           oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
           ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
         }
@@ -337,17 +358,20 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const Sear
     for (int base = 0; base < NLINES; base += C::TEAMS_A) {
       const int li = base + team;
       const bool active = li < NLINES;
-      const int zl = active ? li / NH : 0, kx = active ? li % NH : 0;
-      fft_line<N, -1, P>(planes + (size_t)zl * N * NH + kx, NH, lane, s_tw, active);
+      const int zl = active ? li / NH : 0, kx = active ? spread_kx<NH>(li % NH) : 0;
+      fft_line<N, -1, P, 1>(planes + (size_t)zl * PY * NH + kx, NH, lane, s_tw, active);
     }
   }
   __syncthreads();
-  // 4. store the slab (contiguous in S1)
+  // 4. store the slab: S1[e][z0 + zl][y][kx], rows gathered from their padded positions
   {
-    float4* dst = reinterpret_cast<float4*>(a.s1 + ((size_t)e * N + z0) * N * NH);
-    const float4* srcv = reinterpret_cast<const float4*>(planes);
-    constexpr int NV = G * N * NH / 2;  // float2 pairs; G*N*NH is even because N is even
-    for (int i = threadIdx.x; i < NV; i += C::NT_A) dst[i] = srcv[i];
+    float2* dst = a.s1 + ((size_t)e * N + z0) * N * NH;
+    constexpr int NV = G * N * NH;
+    for (int i = threadIdx.x; i < NV; i += C::NT_A) {
+      const int row = i / NH, kx = i % NH;  // row = zl * N + y
+      const int zl = row / N, y = row % N;
+      dst[i] = planes[((size_t)zl * PY + lpos<1>(y)) * NH + kx];
+    }
   }
 }
 
@@ -358,8 +382,8 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, P = C::P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tile = reinterpret_cast<float2*>(smem_raw);  // [N (z)][NH]
-  float2* s_tw = tile + (size_t)N * NH;
+  float2* tile = reinterpret_cast<float2*>(smem_raw);  // [PY][NH], row z at lpos<1>(z)
+  float2* s_tw = tile + (size_t)C::PY * NH;
   __shared__ double red[32];
 
   const int e = blockIdx.y;
@@ -375,20 +399,22 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
   const float2* src = a.s1 + (size_t)e * N * N * NH + (size_t)ky * NH;
   for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) {
     const int z = i / NH, kx = i % NH;
-    tile[i] = src[(size_t)z * N * NH + kx];
+    tile[lpos<1>(z) * NH + kx] = src[(size_t)z * N * NH + kx];
   }
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
   for (int base = 0; base < NH; base += C::TEAMS_BC) {
-    const int kx = base + team;
-    fft_line<N, -1, P>(tile + (kx < NH ? kx : 0), NH, lane, s_tw, kx < NH);
+    const int li = base + team;
+    const int kx = li < NH ? spread_kx<NH>(li) : 0;
+    fft_line<N, -1, P, 1>(tile + kx, NH, lane, s_tw, li < NH);
   }
   __syncthreads();
   double en = 0.0;
   for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) {
     const int z = i / NH, kx = i % NH;
     const size_t gi = ((size_t)z * N + ky) * NH + kx;
-    float2 r = tile[i];
+    float2& slot = tile[lpos<1>(z) * NH + kx];
+    float2 r = slot;
     if (wref) {
       const float wv = __ldg(wref + gi);
       r.x *= wv;
@@ -397,7 +423,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
     }
     float2 x = cmulc(__ldg(q + gi), r);
     if (gi == 0) x = make_float2(0.f, 0.f);
-    tile[i] = x;
+    slot = x;
   }
   if (wref) {
     double t = block_sum(en, red);
@@ -405,15 +431,16 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
   }
   __syncthreads();
   for (int base = 0; base < NH; base += C::TEAMS_BC) {
-    const int kx = base + team;
-    fft_line<N, 1, P>(tile + (kx < NH ? kx : 0), NH, lane, s_tw, kx < NH);
+    const int li = base + team;
+    const int kx = li < NH ? spread_kx<NH>(li) : 0;
+    fft_line<N, 1, P, 1>(tile + kx, NH, lane, s_tw, li < NH);
   }
   __syncthreads();
   float2* dst = a.s2 + (size_t)e * w * N * NH + (size_t)ky * NH;
   for (int i = threadIdx.x; i < w * NH; i += C::NT_BC) {
     const int j = i / NH, kx = i % NH;
     const int z = (j - a.radius + N) % N;
-    dst[(size_t)j * N * NH + kx] = tile[(size_t)z * NH + kx];
+    dst[(size_t)j * N * NH + kx] = tile[lpos<1>(z) * NH + kx];
   }
 }
 
@@ -424,9 +451,9 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, P = C::P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tile = reinterpret_cast<float2*>(smem_raw);   // [N (y)][NH]
-  float2* s_tw = tile + (size_t)N * NH;
-  float2* lines = s_tw + N;                              // [TEAMS][N+1]
+  float2* tile = reinterpret_cast<float2*>(smem_raw);   // [PY][NH], row y at lpos<1>(y)
+  float2* s_tw = tile + (size_t)C::PY * NH;
+  float2* lines = s_tw + N;                              // [TEAMS][LP]
   __shared__ unsigned long long s_best;
 
   const int e = blockIdx.y;
@@ -441,12 +468,13 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
   load_twiddles<N>(s_tw, g_tw);
   if (threadIdx.x == 0) s_best = 0ull;
   const float2* src = a.s2 + ((size_t)e * w + j) * N * NH;
-  for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) tile[i] = src[i];
+  for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) tile[lpos<1>(i / NH) * NH + i % NH] = src[i];
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
   for (int base = 0; base < NH; base += C::TEAMS_BC) {
-    const int kx = base + team;
-    fft_line<N, 1, P>(tile + (kx < NH ? kx : 0), NH, lane, s_tw, kx < NH);
+    const int li = base + team;
+    const int kx = li < NH ? spread_kx<NH>(li) : 0;
+    fft_line<N, 1, P, 1>(tile + kx, NH, lane, s_tw, li < NH);
   }
   __syncthreads();
 
@@ -458,16 +486,17 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
 
   unsigned long long best = 0ull;
   const int npairs = (w + 1) / 2;
-  float2* buf = lines + (size_t)team * (N + 1);
-  for (int base = 0; base < npairs; base += C::TEAMS_BC) {
+  const bool has_line = team < C::TEAMS_LC;
+  float2* buf = lines + (size_t)(has_line ? team : 0) * C::LP;
+  for (int base = 0; base < npairs; base += C::TEAMS_LC) {
     const int pr = base + team;
-    const bool active = pr < npairs;
+    const bool active = has_line && pr < npairs;
     const int ja = 2 * pr, jb = 2 * pr + 1;
     const bool has_b = jb < w;
     const int ya = (ja - r + N) % N, yb = has_b ? (jb - r + N) % N : ya;
     if (active) {
-      const float2* ra = tile + (size_t)ya * NH;
-      const float2* rb = tile + (size_t)yb * NH;
+      const float2* ra = tile + (size_t)lpos<1>(ya) * NH;
+      const float2* rb = tile + (size_t)lpos<1>(yb) * NH;
       for (int n = lane; n < N; n += P) {
         const bool lower = n <= N / 2;
         const int k = lower ? n : N - n;
@@ -475,11 +504,11 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
         float2 B = has_b ? rb[k] : make_float2(0.f, 0.f);
         if (k == 0 || 2 * k == N) { A.y = 0.f; B.y = 0.f; }
         if (!lower) { A.y = -A.y; B.y = -B.y; }
-        buf[n] = make_float2(A.x - B.y, A.y + B.x);
+        buf[lpos<1>(n)] = make_float2(A.x - B.y, A.y + B.x);
       }
     }
     __syncwarp();
-    fft_line<N, 1, P>(buf, 1, lane, s_tw, active);
+    fft_line<N, 1, P, 1>(buf, 1, lane, s_tw, active);
     if (active) {
       for (int t = lane; t < 2 * w; t += P) {
         const int which = t / w;  // 0: row a, 1: row b
@@ -487,7 +516,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
         const int sx = (t % w) - r;
         const int sy = (which ? jb : ja) - r;
         if (sx * sx + sy * sy + sz * sz > r * r) continue;
-        const float2 zv = buf[(sx + N) % N];
+        const float2 zv = buf[lpos<1>((sx + N) % N)];
         const float v = (which ? zv.y : zv.x) * inv_norm;
         if (v != v) continue;  // NaN never wins (MATLAB max ignores NaN)
         const unsigned int lin = (unsigned int)(((sz + c) * N + (sy + c)) * N + (sx + c));

@@ -158,6 +158,30 @@ static double interp_cubic_grad(const REAL* v, int nx, int ny, int nz, double sx
   return acc;
 }
 
+/* value and gradient of the trilinear interpolant (interpn semantics, 0 outside [0,n-1]) */
+static double interp_linear_grad(const REAL* v, int nx, int ny, int nz, double sx, double sy, double sz,
+                                 double g[3]) {
+  g[0] = g[1] = g[2] = 0;
+  if (sx < 0 || sy < 0 || sz < 0 || sx > nx - 1 || sy > ny - 1 || sz > nz - 1) return 0;
+  const int x0 = (int)floor(sx), y0 = (int)floor(sy), z0 = (int)floor(sz);
+  const double fx = sx - x0, fy = sy - y0, fz = sz - z0;
+  double c[2][2][2];
+  for (int dz = 0; dz < 2; ++dz)
+    for (int dy = 0; dy < 2; ++dy)
+      for (int dx = 0; dx < 2; ++dx) c[dz][dy][dx] = (double)vox(v, nx, ny, nz, x0 + dx, y0 + dy, z0 + dz);
+  double val = 0;
+  for (int dz = 0; dz < 2; ++dz)
+    for (int dy = 0; dy < 2; ++dy)
+      for (int dx = 0; dx < 2; ++dx) {
+        const double wx = dx ? fx : 1 - fx, wy = dy ? fy : 1 - fy, wz = dz ? fz : 1 - fz;
+        val += wx * wy * wz * c[dz][dy][dx];
+        g[0] += (dx ? 1.0 : -1.0) * wy * wz * c[dz][dy][dx];
+        g[1] += wx * (dy ? 1.0 : -1.0) * wz * c[dz][dy][dx];
+        g[2] += wx * wy * (dz ? 1.0 : -1.0) * c[dz][dy][dx];
+      }
+  return val;
+}
+
 /* Sample position of output voxel p (mexXform3d.cu:45-65 with the texture-coordinate
  * shift of :293-296 and :67-74 folded back to index space, i.e. s = M u + floor(n/2)):
  *   fwd : u = p - c - shift ; s = M u + c
@@ -701,8 +725,17 @@ EXPORT void FN(orc_tsearch)(const REAL* tomo, int nx, int ny, int nz, const REAL
  * against the real-space particle template h = C2R(Q) and its exact gradient w.r.t. the
  * 9 matrix entries and the 3 shift components.  E_R is the DC-free energy
  * n^3 sum r^2 - (sum r)^2 (Parseval).  Returns CC; dM (9, column-major) and dt (3). */
+EXPORT double FN(orc_cc_pose_interp)(const REAL* ref, const REAL* mask, int n, const REAL* h, double EP,
+                                     const double M[9], const double t[3], int interp, double dM[9], double dt[3]);
+
 EXPORT double FN(orc_cc_pose)(const REAL* ref, const REAL* mask, int n, const REAL* h, double EP, const double M[9],
                               const double t[3], double dM[9], double dt[3]) {
+  return FN(orc_cc_pose_interp)(ref, mask, n, h, EP, M, t, 1, dM, dt);
+}
+
+/* As orc_cc_pose with interp 0 = trilinear (interpn) or 1 = tricubic. */
+EXPORT double FN(orc_cc_pose_interp)(const REAL* ref, const REAL* mask, int n, const REAL* h, double EP,
+                                     const double M[9], const double t[3], int interp, double dM[9], double dt[3]) {
   const int c = n / 2;
   const long nvox = (long)n * n * n;
   double* r = (double*)malloc(sizeof(double) * nvox);
@@ -714,7 +747,8 @@ EXPORT double FN(orc_cc_pose)(const REAL* ref, const REAL* mask, int n, const RE
         double s[3], g[3];
         sample_pos(M, t, 1, x, y, z, c, c, c, s);
         long i = ((long)z * n + y) * n + x;
-        double v = interp_cubic_grad(ref, n, n, n, s[0], s[1], s[2], g);
+        double v = interp == 1 ? interp_cubic_grad(ref, n, n, n, s[0], s[1], s[2], g)
+                               : interp_linear_grad(ref, n, n, n, s[0], s[1], s[2], g);
         double m = mask ? (double)mask[i] : 1.0;
         r[i] = m * v;
         gs[3 * i] = m * g[0]; gs[3 * i + 1] = m * g[1]; gs[3 * i + 2] = m * g[2];

@@ -51,6 +51,7 @@ def lib(precision="f64"):
         "orc_xcf_translational": (C.c_double, [pR, pR, pR, C.c_int, pR, C.c_double, pd, pd, pR, C.c_int, pR, pd]),
         "orc_tsearch": (None, [pR, C.c_int, C.c_int, C.c_int, pR, C.c_int, pd, C.c_int, pR, pR]),
         "orc_cc_pose": (C.c_double, [pR, pR, C.c_int, pR, C.c_double, pd, pd, pd, pd]),
+        "orc_cc_pose_interp": (C.c_double, [pR, pR, C.c_int, pR, C.c_double, pd, pd, C.c_int, pd, pd]),
     }
     funcs = {}
     for name, (res, args) in sig.items():
@@ -208,9 +209,10 @@ def tsearch(tomo, tmpl, matrices, precision="f64"):
     return peak, ang
 
 
-def cc_pose(ref, h, energy, matrix, t, mask=None):
-    """Zero-lag normalised CC of the tricubic-rotated reference (sampled through matrix,
-    'forward', shift t) against the real-space template h; returns (cc, dM (3x3), dt (3))."""
+def cc_pose(ref, h, energy, matrix, t, mask=None, interp=1):
+    """Zero-lag normalised CC of the rotated reference (tricubic interp=1 or trilinear interp=0,
+    sampled through matrix, 'forward', shift t) against the real-space template h; returns
+    (cc, dM (3x3), dt (3))."""
     L = lib("f64")
     r = _arr(ref, L.dtype)
     hh = _arr(h, L.dtype)
@@ -219,8 +221,8 @@ def cc_pose(ref, h, energy, matrix, t, mask=None):
     tt = np.ascontiguousarray(t, dtype=np.float64)
     dM = np.zeros(9)
     dt = np.zeros(3)
-    cc = L.orc_cc_pose(L.ptr(r), L.ptr(m) if m is not None else None, r.shape[0], L.ptr(hh), float(energy), _p(M),
-                       _p(tt), _p(dM), _p(dt))
+    cc = L.orc_cc_pose_interp(L.ptr(r), L.ptr(m) if m is not None else None, r.shape[0], L.ptr(hh), float(energy),
+                              _p(M), _p(tt), int(interp), _p(dM), _p(dt))
     return cc, dM.reshape(3, 3, order="F"), dt
 
 
