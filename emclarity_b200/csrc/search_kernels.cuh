@@ -397,9 +397,20 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
 
   load_twiddles<N>(s_tw, g_tw);
   const float2* src = a.s1 + (size_t)e * N * N * NH + (size_t)ky * NH;
-  for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) {
-    const int z = i / NH, kx = i % NH;
-    tile[lpos<1>(z) * NH + kx] = src[(size_t)z * N * NH + kx];
+  {
+    // all of a thread's loads in flight before the first shared-memory store
+    constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
+    float2 v[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int i = threadIdx.x + k * C::NT_BC;
+      if (i < N * NH) v[k] = src[(size_t)(i / NH) * N * NH + i % NH];
+    }
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int i = threadIdx.x + k * C::NT_BC;
+      if (i < N * NH) tile[lpos<1>(i / NH) * NH + i % NH] = v[k];
+    }
   }
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
@@ -410,20 +421,32 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
   }
   __syncthreads();
   double en = 0.0;
-  for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) {
-    const int z = i / NH, kx = i % NH;
-    const size_t gi = ((size_t)z * N + ky) * NH + kx;
-    float2& slot = tile[lpos<1>(z) * NH + kx];
-    float2 r = slot;
-    if (wref) {
-      const float wv = __ldg(wref + gi);
-      r.x *= wv;
-      r.y *= wv;
-      if (gi != 0) en += (kx == 0 || 2 * kx == N ? 1.0 : 2.0) * ((double)r.x * r.x + (double)r.y * r.y);
+  {
+    constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
+    float2 qv[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int i = threadIdx.x + k * C::NT_BC;
+      if (i < N * NH) qv[k] = __ldg(q + ((size_t)(i / NH) * N + ky) * NH + i % NH);
     }
-    float2 x = cmulc(__ldg(q + gi), r);
-    if (gi == 0) x = make_float2(0.f, 0.f);
-    slot = x;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int i = threadIdx.x + k * C::NT_BC;
+      if (i >= N * NH) continue;
+      const int z = i / NH, kx = i % NH;
+      const size_t gi = ((size_t)z * N + ky) * NH + kx;
+      float2& slot = tile[lpos<1>(z) * NH + kx];
+      float2 r = slot;
+      if (wref) {
+        const float wv = __ldg(wref + gi);
+        r.x *= wv;
+        r.y *= wv;
+        if (gi != 0) en += (kx == 0 || 2 * kx == N ? 1.0 : 2.0) * ((double)r.x * r.x + (double)r.y * r.y);
+      }
+      float2 x = cmulc(qv[k], r);
+      if (gi == 0) x = make_float2(0.f, 0.f);
+      slot = x;
+    }
   }
   if (wref) {
     double t = block_sum(en, red);
@@ -468,7 +491,20 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
   load_twiddles<N>(s_tw, g_tw);
   if (threadIdx.x == 0) s_best = 0ull;
   const float2* src = a.s2 + ((size_t)e * w + j) * N * NH;
-  for (int i = threadIdx.x; i < N * NH; i += C::NT_BC) tile[lpos<1>(i / NH) * NH + i % NH] = src[i];
+  {
+    constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
+    float2 v[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int i = threadIdx.x + k * C::NT_BC;
+      if (i < N * NH) v[k] = src[i];
+    }
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int i = threadIdx.x + k * C::NT_BC;
+      if (i < N * NH) tile[lpos<1>(i / NH) * NH + i % NH] = v[k];
+    }
+  }
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
   for (int base = 0; base < NH; base += C::TEAMS_BC) {
