@@ -170,6 +170,8 @@ def run_ours(args, world, rank, local):
     n = args.particles
     b = build_batch(1000 + rank, n)
     s = api.Search(peak_radius=PEAK_RADIUS)
+    if args.planes:
+        s.set_planes(BOX, args.planes)
     rid = s.add_reference(b["ref"], b["mask"])
     s.set_orientations(b["grid"])
     d_parts = b["parts"].cuda()
@@ -273,6 +275,8 @@ def run_ours(args, world, rank, local):
         "plain": plain,
     }
     res["roofline"], res["passes"] = roofline(prof)
+    g, g_ms = s.planes(BOX)
+    res["passes"]["fwd_xy"]["planes_per_cta"] = {"chosen": g, "tuning_ms_per_launch": g_ms}
     res["clocks"] = clk.summary()
     return res
 
@@ -609,6 +613,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=1200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--planes", type=int, default=0, help="pass-A z-planes per CTA (0: timed choice)")
     ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine"])
     args = ap.parse_args()
     if args.impl == "ours" and args.workload != "batched64":

@@ -88,6 +88,8 @@ SIGNATURES = {
     "emc_search_destroy": (_i, [_vp]),
     "emc_search_set_profiling": (_i, [_vp, _i]),
     "emc_search_timings": (_i, [_vp, _pd, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_long), _i]),
+    "emc_search_set_planes": (_i, [_vp, _i, _i]),
+    "emc_search_get_planes": (_i, [_vp, _i, _i, _pi, _pf]),
     "emc_search_plain_noalloc": (_i, [_vp, _vp, _i, _vp, _d, _pd, _pf, _pd, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "emc_cc_adjoint_batch": (_i, [_vp, _i, _pi, C.POINTER(_vp), _pd, _pd, _pd, _i, _pd, _pd, _vp]),
     "emc_cc_adjoint": (_i, [_vp, _i, _vp, _d, _pd, _pd, _i, _pd, _pd, _vp]),

@@ -317,6 +317,18 @@ class Search:
         return {"ms": dict(zip(names, list(ms))), "launches": dict(zip(names, list(ln))), "evals": ev.value,
                 "launches_last_run": last.value}
 
+    def set_planes(self, box, planes):
+        """Fixes pass A's z-planes per CTA for `box` (1, 2, 4 or 8); 0 returns it to timing-based tuning."""
+        L.call("emc_search_set_planes", self._h, int(box), int(planes))
+
+    def planes(self, box, dtype="f32"):
+        """(planes in use, {planes option: pass-A ms per launch at tuning}) for (box, dtype); 0 = not tuned yet."""
+        g = C.c_int(0)
+        ms = (C.c_float * 4)()
+        L.call("emc_search_get_planes", self._h, int(box), {"f32": L.DTYPE_F32, "bf16": L.DTYPE_BF16}[dtype],
+               C.byref(g), ms)
+        return g.value, {1 << k: float(ms[k]) for k in range(4) if ms[k] >= 0}
+
     def cc_adjoint(self, ref_id, h, energy_p, prior, poses):
         """CC and gradient (dphi, dtheta, dpsi per degree; dtx, dty, dtz per voxel) per pose."""
         poses = np.ascontiguousarray(np.asarray(poses, dtype=np.float64).reshape(-1, 6))

@@ -80,26 +80,75 @@ __global__ void k_search_scatter(const EvalResult* __restrict__ results, long n,
 }
 
 // ------------------------------------------------------------------ per-size dispatch
+// Pass A holds G z-planes per CTA: larger G amortises the per-CTA setup (sampling matrix,
+// twiddles, reductions) over more planes, smaller G raises the number of resident CTAs. The
+// best G depends on the box, the chunk size (wave quantisation over the SMs) and the
+// reference storage type, so it is chosen by timing (tune_planes) rather than fixed.
+constexpr size_t kMaxSmemPerCta = 227 * 1024;
+constexpr int kPlaneOptions[] = {1, 2, 4, 8};
+
+template <int N, int G>
+constexpr bool planes_fit() {
+  return N % G == 0 && SearchCfg<N, G>::SMEM_A <= kMaxSmemPerCta;
+}
+
+template <int N, typename T, int G>
+static emc_status set_attr_fwd() {
+  if constexpr (planes_fit<N, G>())
+    EMC_CUDA(cudaFuncSetAttribute(k_search_fwd_xy<N, T, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)SearchCfg<N, G>::SMEM_A));
+  return EMC_OK;
+}
+
 template <int N, typename T>
 static emc_status set_attrs() {
   using C = SearchCfg<N>;
-  EMC_CUDA(cudaFuncSetAttribute(k_search_fwd_xy<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_A));
+  EMC_TRY((set_attr_fwd<N, T, 1>()));
+  EMC_TRY((set_attr_fwd<N, T, 2>()));
+  EMC_TRY((set_attr_fwd<N, T, 4>()));
+  EMC_TRY((set_attr_fwd<N, T, 8>()));
   EMC_CUDA(cudaFuncSetAttribute(k_search_z_mul<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_B));
   EMC_CUDA(cudaFuncSetAttribute(k_search_inv_peak<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM_C));
   return EMC_OK;
 }
 
-// Launches the three passes of one chunk; ev (optional) receives an event record before
-// each pass and after the last one (4 events).
+template <int N, typename T, int G>
+static bool launch_fwd_g(const SearchChunkArgs& a, const float2* tw, cudaStream_t st) {
+  if constexpr (planes_fit<N, G>()) {
+    using C = SearchCfg<N, G>;
+    k_search_fwd_xy<N, T, G><<<dim3(N / G, a.n_items), C::NT_A, C::SMEM_A, st>>>(a, tw);
+    return true;
+  }
+  return false;
+}
+
 template <int N, typename T>
-static emc_status launch_chunk(const SearchChunkArgs& a, cudaStream_t st, cudaEvent_t* ev) {
+static emc_status launch_fwd(int g, const SearchChunkArgs& a, const float2* tw, cudaStream_t st) {
+  bool ok = false;
+  switch (g) {
+    case 1: ok = launch_fwd_g<N, T, 1>(a, tw, st); break;
+    case 2: ok = launch_fwd_g<N, T, 2>(a, tw, st); break;
+    case 4: ok = launch_fwd_g<N, T, 4>(a, tw, st); break;
+    case 8: ok = launch_fwd_g<N, T, 8>(a, tw, st); break;
+  }
+  if (!ok) {
+    set_error("search: %d planes per CTA not available for box %d", g, N);
+    return EMC_E_ARG;
+  }
+  EMC_LAUNCH_CHECK();
+  return EMC_OK;
+}
+
+// Launches the three passes of one chunk with g planes per pass-A CTA; ev (optional) receives
+// an event record before each pass and after the last one (4 events).
+template <int N, typename T>
+static emc_status launch_chunk(int g, const SearchChunkArgs& a, cudaStream_t st, cudaEvent_t* ev) {
   using C = SearchCfg<N>;
   const float2* tw = device_twiddles(N);
   if (!tw) return EMC_E_CUDA;
   const int w = 2 * a.radius + 1;
   if (ev) EMC_CUDA(cudaEventRecord(ev[0], st));
-  k_search_fwd_xy<N, T><<<dim3(N / C::G, a.n_items), C::NT_A, C::SMEM_A, st>>>(a, tw);
-  EMC_LAUNCH_CHECK();
+  EMC_TRY((launch_fwd<N, T>(g, a, tw, st)));
   if (ev) EMC_CUDA(cudaEventRecord(ev[1], st));
   k_search_z_mul<N><<<dim3(N, a.n_items), C::NT_BC, C::SMEM_B, st>>>(a, tw);
   EMC_LAUNCH_CHECK();
@@ -112,18 +161,60 @@ static emc_status launch_chunk(const SearchChunkArgs& a, cudaStream_t st, cudaEv
 
 static bool box_supported(int n) { return n == 64 || n == 96 || n == 128; }
 
-static emc_status launch_chunk_any(int n, int dtype, const SearchChunkArgs& a, cudaStream_t st, cudaEvent_t* ev) {
+static int box_index(int n) { return n == 64 ? 0 : (n == 96 ? 1 : 2); }
+
+template <int N>
+static bool planes_fit_rt(int g) {
+  switch (g) {
+    case 1: return planes_fit<N, 1>();
+    case 2: return planes_fit<N, 2>();
+    case 4: return planes_fit<N, 4>();
+    case 8: return planes_fit<N, 8>();
+  }
+  return false;
+}
+
+// Whether pass A can run box n with g planes per CTA (g divides n, the slab fits shared memory).
+static bool planes_available(int n, int g) {
+  switch (n) {
+    case 64: return planes_fit_rt<64>(g);
+    case 96: return planes_fit_rt<96>(g);
+    case 128: return planes_fit_rt<128>(g);
+  }
+  return false;
+}
+
+template <typename T>
+static emc_status launch_fwd_any_t(int n, int g, const SearchChunkArgs& a, cudaStream_t st) {
+  const float2* tw = device_twiddles(n);
+  if (!tw) return EMC_E_CUDA;
+  switch (n) {
+    case 64: return launch_fwd<64, T>(g, a, tw, st);
+    case 96: return launch_fwd<96, T>(g, a, tw, st);
+    case 128: return launch_fwd<128, T>(g, a, tw, st);
+  }
+  set_error("search: box %d not supported (64, 96, 128)", n);
+  return EMC_E_UNSUPPORTED;
+}
+
+static emc_status launch_fwd_any(int n, int dtype, int g, const SearchChunkArgs& a, cudaStream_t st) {
+  return dtype == EMC_DTYPE_F32 ? launch_fwd_any_t<float>(n, g, a, st)
+                                : launch_fwd_any_t<__nv_bfloat16>(n, g, a, st);
+}
+
+static emc_status launch_chunk_any(int n, int dtype, int g, const SearchChunkArgs& a, cudaStream_t st,
+                                   cudaEvent_t* ev) {
   if (dtype == EMC_DTYPE_F32) {
     switch (n) {
-      case 64: return launch_chunk<64, float>(a, st, ev);
-      case 96: return launch_chunk<96, float>(a, st, ev);
-      case 128: return launch_chunk<128, float>(a, st, ev);
+      case 64: return launch_chunk<64, float>(g, a, st, ev);
+      case 96: return launch_chunk<96, float>(g, a, st, ev);
+      case 128: return launch_chunk<128, float>(g, a, st, ev);
     }
   } else {
     switch (n) {
-      case 64: return launch_chunk<64, __nv_bfloat16>(a, st, ev);
-      case 96: return launch_chunk<96, __nv_bfloat16>(a, st, ev);
-      case 128: return launch_chunk<128, __nv_bfloat16>(a, st, ev);
+      case 64: return launch_chunk<64, __nv_bfloat16>(g, a, st, ev);
+      case 96: return launch_chunk<96, __nv_bfloat16>(g, a, st, ev);
+      case 128: return launch_chunk<128, __nv_bfloat16>(g, a, st, ev);
     }
   }
   set_error("search: box %d not supported (64, 96, 128)", n);
@@ -239,6 +330,12 @@ struct emc_search_s {
   double prof_ms[4] = {0, 0, 0, 0};
   long prof_launches[4] = {0, 0, 0, 0};
   long prof_evals = 0;
+
+  // pass-A planes per CTA per [box 64/96/128][dtype]: 0 = tune on the next run
+  int planes[3][2] = {};
+  float tune_ms[3][2][4] = {{{-1, -1, -1, -1}, {-1, -1, -1, -1}},
+                            {{-1, -1, -1, -1}, {-1, -1, -1, -1}},
+                            {{-1, -1, -1, -1}, {-1, -1, -1, -1}}};
 };
 
 namespace {
@@ -356,23 +453,75 @@ static emc_status harvest_slot(emc_search_t s, int slot) {
   return EMC_OK;
 }
 
+static emc::SearchChunkArgs chunk_args(emc_search_t s, const Chunk& c) {
+  emc::SearchChunkArgs a;
+  a.items = s->d_items.p + c.item_offset;
+  a.parts = s->d_parts.p;
+  a.refs = s->d_refs.p;
+  a.dmat = s->d_dmat.p;
+  a.s1 = s->s1.p;
+  a.s2 = s->s2.p;
+  a.stats = s->stats.p;
+  a.keys = s->keys.p;
+  a.n_items = c.count;
+  a.radius = effective_radius(s, c.n);
+  a.interp = s->interp;
+  return a;
+}
+
+static int& planes_slot(emc_search_t s, int n, int dtype) {
+  return s->planes[emc::box_index(n)][dtype == EMC_DTYPE_BF16 ? 1 : 0];
+}
+
+// Times pass A on chunk c with every planes option that fits (one warm-up launch, then three
+// timed ones each) and stores the fastest. Pass A's outputs (S1 slabs, energy sums) are scratch
+// that the real run rewrites, so the trial launches leave no trace in the results.
+static emc_status tune_planes(emc_search_t s, const Chunk& c, cudaStream_t st) {
+  const emc::SearchChunkArgs a = chunk_args(s, c);
+  float* ms_out = s->tune_ms[emc::box_index(c.n)][c.dtype == EMC_DTYPE_BF16 ? 1 : 0];
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  EMC_CUDA(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    emc::set_error("search: event creation failed");
+    return EMC_E_CUDA;
+  }
+  emc_status rs = EMC_OK;
+  int best = 0;
+  float best_ms = 0.f;
+  constexpr int kReps = 3;
+  for (int k = 0; k < 4 && rs == EMC_OK; ++k) {
+    const int g = emc::kPlaneOptions[k];
+    ms_out[k] = -1.f;
+    if (!emc::planes_available(c.n, g)) continue;
+    rs = emc::launch_fwd_any(c.n, c.dtype, g, a, st);
+    if (rs == EMC_OK && cudaEventRecord(e0, st) != cudaSuccess) rs = EMC_E_CUDA;
+    for (int r = 0; r < kReps && rs == EMC_OK; ++r) rs = emc::launch_fwd_any(c.n, c.dtype, g, a, st);
+    float ms = 0.f;
+    if (rs == EMC_OK && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                         cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+      rs = EMC_E_CUDA;
+    if (rs != EMC_OK) break;
+    ms_out[k] = ms / kReps;
+    if (!best || ms < best_ms) {
+      best = g;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rs == EMC_E_CUDA) emc::set_error("search: pass-A tuning failed: %s", cudaGetErrorString(cudaGetLastError()));
+  if (rs != EMC_OK) return rs;
+  planes_slot(s, c.n, c.dtype) = best;
+  return EMC_OK;
+}
+
 static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks, int np, long total_evals,
                                 float* d_cc, int* d_peak, emc_search_hit* d_best, cudaStream_t st) {
   EMC_CUDA(cudaMemsetAsync(s->d_best_keys.p, 0, sizeof(unsigned long long) * np, st));
   long launches = 0;
   for (const Chunk& c : chunks) {
-    emc::SearchChunkArgs a;
-    a.items = s->d_items.p + c.item_offset;
-    a.parts = s->d_parts.p;
-    a.refs = s->d_refs.p;
-    a.dmat = s->d_dmat.p;
-    a.s1 = s->s1.p;
-    a.s2 = s->s2.p;
-    a.stats = s->stats.p;
-    a.keys = s->keys.p;
-    a.n_items = c.count;
-    a.radius = effective_radius(s, c.n);
-    a.interp = s->interp;
+    const emc::SearchChunkArgs a = chunk_args(s, c);
     EMC_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(emc::EvalStats) * c.count, st));
     EMC_CUDA(cudaMemsetAsync(s->keys.p, 0, sizeof(unsigned long long) * c.count, st));
     cudaEvent_t* ev = nullptr;
@@ -383,7 +532,7 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
       ev = s->ev[slot];
       s->ev_pending[slot] = true;
     }
-    EMC_TRY(emc::launch_chunk_any(c.n, c.dtype, a, st, ev));
+    EMC_TRY(emc::launch_chunk_any(c.n, c.dtype, planes_slot(s, c.n, c.dtype), a, st, ev));
     emc::k_search_decode<<<(c.count + 255) / 256, 256, 0, st>>>(a, c.n, s->d_results.p, s->d_best_keys.p);
     EMC_LAUNCH_CHECK();
     if (ev) EMC_CUDA(cudaEventRecord(ev[4], st));
@@ -513,6 +662,8 @@ emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, in
                            st));
   // host vectors must outlive the async copies
   EMC_CUDA(cudaStreamSynchronize(st));
+  for (const Chunk& c : chunks)
+    if (!planes_slot(s, c.n, c.dtype)) EMC_TRY(tune_planes(s, c, st));
   if (s->profiling) {
     s->gkey.clear();
     return search_record(s, chunks, np, total, d_cc, d_peak, d_best, st);
@@ -608,6 +759,31 @@ emc_status emc_search_timings(emc_search_t s, double ms[4], long launches[4], lo
     }
     s->prof_evals = 0;
   }
+  return EMC_OK;
+}
+
+emc_status emc_search_set_planes(emc_search_t s, int box, int planes) {
+  EMC_CHECK_ARG(s, "emc_search_set_planes: null handle");
+  EMC_CHECK_ARG(emc::box_supported(box), "emc_search_set_planes: box %d not supported (64, 96, 128)", box);
+  EMC_CHECK_ARG(planes == 0 || emc::planes_available(box, planes),
+                "emc_search_set_planes: %d planes per CTA not available for box %d", planes, box);
+  const int b = emc::box_index(box);
+  for (int d = 0; d < 2; ++d) {
+    s->planes[b][d] = planes;
+    for (int k = 0; k < 4; ++k) s->tune_ms[b][d][k] = -1.f;
+  }
+  s->gkey.clear();
+  return EMC_OK;
+}
+
+emc_status emc_search_get_planes(emc_search_t s, int box, int dtype, int* planes, float ms_per_option[4]) {
+  EMC_CHECK_ARG(s && planes, "emc_search_get_planes: null argument");
+  EMC_CHECK_ARG(emc::box_supported(box), "emc_search_get_planes: box %d not supported (64, 96, 128)", box);
+  EMC_CHECK_ARG(dtype == EMC_DTYPE_F32 || dtype == EMC_DTYPE_BF16, "emc_search_get_planes: dtype %d", dtype);
+  const int b = emc::box_index(box), d = dtype == EMC_DTYPE_BF16 ? 1 : 0;
+  *planes = s->planes[b][d];
+  if (ms_per_option)
+    for (int k = 0; k < 4; ++k) ms_per_option[k] = s->tune_ms[b][d][k];
   return EMC_OK;
 }
 

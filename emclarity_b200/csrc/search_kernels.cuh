@@ -66,10 +66,14 @@ __device__ __forceinline__ void cell_values(const CellT<__nv_bfloat16>& c, float
     v[2 * i + 1] = f.y;
   }
 }
+// One 256-bit read-only load (sm_100): the whole 32-byte cell in a single request, so the cell's
+// sector is looked up once instead of once per 16-byte half.  Cells are 32-byte aligned.
 __device__ __forceinline__ CellT<float> load_cell(const CellT<float>* p) {
   CellT<float> c;
-  c.lo = __ldg(&p->lo);
-  c.hi = __ldg(&p->hi);
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(c.lo.x), "=f"(c.lo.y), "=f"(c.lo.z), "=f"(c.lo.w), "=f"(c.hi.x), "=f"(c.hi.y), "=f"(c.hi.z),
+        "=f"(c.hi.w)
+      : "l"(p));
   return c;
 }
 __device__ __forceinline__ CellT<__nv_bfloat16> load_cell(const CellT<__nv_bfloat16>* p) {
@@ -167,11 +171,14 @@ __device__ __forceinline__ void compose_sampling_matrix(const double* prior, con
     }
 }
 
-template <int N>
+// Default planes per pass-A CTA; the autotuner of search.cu may pick another supported value.
+__host__ __device__ constexpr int default_planes(int N) { return N <= 64 ? 4 : (N <= 96 ? 2 : 1); }
+
+template <int N, int GG = 0>
 struct SearchCfg {
   static constexpr int NH = N / 2 + 1;
   static constexpr int P = team_size(N);
-  static constexpr int G = N <= 64 ? 4 : (N <= 96 ? 2 : 1);  // planes per pass-A CTA
+  static constexpr int G = GG ? GG : default_planes(N);  // planes per pass-A CTA
   static constexpr int NT_A = 256;
   static constexpr int TEAMS_A = NT_A / P;
   static constexpr int NT_BC = ((NH * P + 31) / 32) * 32;
@@ -213,11 +220,11 @@ __device__ __forceinline__ Tv block_sum(Tv v, Tv* red) {
 
 // Gather of the G planes of pass A through corner cells: U voxels per thread per step, all cell
 // loads of a step issued before any is used (memory-level parallelism for L2-resident cells).
-template <int N, typename T, int MODE>
+template <int N, typename T, int MODE, int GG>
 __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells, const float* __restrict__ mask,
                                              const float m[9], float tx, float ty, float tz, int z0,
                                              float* __restrict__ fplanes, double& s1, double& s2) {
-  using C = SearchCfg<N>;
+  using C = SearchCfg<N, GG>;
   constexpr int G = C::G, NT = C::NT_A, NH = C::NH, U = 4;
   constexpr int TOTAL = G * N * N;
   static_assert(TOTAL % (NT * U) == 0, "gather tiling");
@@ -256,10 +263,10 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
 }
 
 // ------------------------------------------------------------------ pass A
-template <int N, typename T>
-__global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const SearchChunkArgs a,
-                                                                       const float2* __restrict__ g_tw) {
-  using C = SearchCfg<N>;
+template <int N, typename T, int GG = 0>
+__global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A) k_search_fwd_xy(const SearchChunkArgs a,
+                                                                           const float2* __restrict__ g_tw) {
+  using C = SearchCfg<N, GG>;
   constexpr int NH = C::NH, G = C::G, P = C::P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int PY = C::PY, LP = C::LP;
@@ -291,10 +298,10 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_A) k_search_fwd_xy(const Sear
   double s1 = 0.0, s2 = 0.0;
   float* fplanes = reinterpret_cast<float*>(planes);
   if (rf.cells && a.interp == EMC_INTERP_LINEAR) {
-    gather_cells<N, T, EMC_INTERP_LINEAR>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, m, tx, ty, tz, z0,
+    gather_cells<N, T, EMC_INTERP_LINEAR, GG>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, m, tx, ty, tz, z0,
                                           fplanes, s1, s2);
   } else if (rf.cells && a.interp == EMC_INTERP_LINEAR_BORDER) {
-    gather_cells<N, T, EMC_INTERP_LINEAR_BORDER>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, m, tx, ty, tz,
+    gather_cells<N, T, EMC_INTERP_LINEAR_BORDER, GG>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, m, tx, ty, tz,
                                                  z0, fplanes, s1, s2);
   } else {
     for (int idx = threadIdx.x; idx < G * N * N; idx += C::NT_A) {

@@ -268,6 +268,17 @@ EMC_API emc_status emc_search_set_profiling(emc_search_t s, int enable);
 EMC_API emc_status emc_search_timings(emc_search_t s, double ms[4], long launches[4], long* evals,
                                       long* launches_last_run, int reset);
 
+/* Tuning hook (no counterpart in the reference).  Pass A (rotate + xy R2C) runs planes = 1, 2, 4
+ * or 8 z-planes per CTA.  Unless fixed here, the first emc_search_run that meets a (box, dtype)
+ * times pass A on its first chunk with every planes value whose slab fits shared memory and
+ * keeps the fastest for that handle.  emc_search_set_planes fixes the value for one box (both
+ * dtypes; EMC_E_ARG if it does not divide the box or does not fit), 0 returns it to tuning.
+ * emc_search_get_planes reports the value in use for (box, dtype), 0 if not tuned yet, and the
+ * pass-A time of each option at tuning (ms_per_option[k] for planes = 1 << k, -1 where not
+ * timed; may be NULL). */
+EMC_API emc_status emc_search_set_planes(emc_search_t s, int box, int planes);
+EMC_API emc_status emc_search_get_planes(emc_search_t s, int box, int dtype, int* planes, float ms_per_option[4]);
+
 
 /* Single-particle search that allocates no device memory.  No counterpart in the reference.
  * For callers that may not call cudaMalloc after start-up: hosts whose own pool owns the GPU

@@ -210,3 +210,48 @@ def test_nan_particle_does_not_win(plain_case):
     cc, pk, best = s.run_host([s.particle(qn, e.item(), rid, orient_count=10)])
     assert np.all(np.isnan(cc))
     assert best[0][1] == -1
+
+
+@pytest.mark.parametrize("store", ["f32", "bf16"])
+def test_planes_per_cta_options_agree(built_lib, cuda, store):
+    """Pass A with 1, 2, 4 or 8 z-planes per CTA computes the same CCs and peaks; the tuner
+    picks one of the options it timed."""
+    from emclarity_b200 import EmcError, api, synthetic
+    rng = np.random.default_rng(41)
+    grid = synthetic.local_grid(30, 8.0, 2.0)
+    s = api.Search(peak_radius=4)
+    descs, keep = [], []
+    for n in (64, 96, 128):
+        ref = synthetic.blob_reference(rng, n)
+        mask = synthetic.soft_sphere_mask(n, 28 * n / 64)
+        rid = s.add_reference(torch.from_numpy(ref).cuda(), torch.from_numpy(mask).cuda(), store=store)
+        wt = api.wedge_ctf_weight(n, -55, 62, synthetic.ctf_dict(25000.0))
+        truth = api.define_matrix([2.0, 4.0, -3.0], "inv")
+        part = synthetic.make_particle(torch.from_numpy(ref).cuda(), rng, truth, (1, 0, -1), wt, 0.5)
+        q, e = api.particle_spectrum(part, wt)
+        keep.append(q)
+        descs.append(s.particle(q, e.item(), rid, orient_count=len(grid)))
+    s.set_orientations(grid)
+    cc0, pk0, best0 = s.run_host(descs)
+    for n in (64, 96, 128):
+        g, ms = s.planes(n, store)
+        assert g in ms and ms[g] == min(ms.values())
+        assert set(ms) <= {1, 2, 4, 8} and 1 in ms
+    options = {64: (1, 2, 4, 8), 96: (1, 2, 4), 128: (1, 2)}
+    for k in range(4):
+        for n in (64, 96, 128):
+            opts = options[n]
+            s.set_planes(n, opts[min(k, len(opts) - 1)])
+        cc, pk, best = s.run_host(descs)
+        assert np.allclose(cc, cc0, rtol=1e-6, atol=1e-7)
+        assert np.array_equal(pk, pk0)
+        assert [b[1] for b in best] == [b[1] for b in best0]
+    with pytest.raises(EmcError):
+        s.set_planes(128, 4)
+    with pytest.raises(EmcError):
+        s.set_planes(96, 8)
+    with pytest.raises(EmcError):
+        s.set_planes(64, 3)
+    s.set_planes(64, 0)
+    assert s.planes(64, store)[0] == 0
+    s.close()
