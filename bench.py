@@ -291,6 +291,19 @@ def L_call_spectrum(api, part, w, q, e):
            C.c_void_p(q.data_ptr()), C.c_void_p(e.data_ptr()), api._stream())
 
 
+def profiled_traffic():
+    """DRAM bytes per pipeline launch from the committed ncu summary (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "search_batched64_passes.md")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_pipeline_launch:"):
+                    return int(line.split(":")[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def roofline(prof):
     peak, which = measured_peaks()
     nl = max(1, prof["launches"]["fwd_xy"])
@@ -303,9 +316,13 @@ def roofline(prof):
     total = sum(prof["ms"].values())
     for k in passes:
         passes[k]["share"] = prof["ms"][k] / total if total else None
+    traffic = profiled_traffic()
     return ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
              "peak_source": which + " (MEASURED_PEAKS.json hbm_gbs)" if which == "measured" else which,
-             "traffic": None, "kernel": "fused search pipeline (fwd_xy + z_mul + inv_peak per chunk)",
+             "traffic": traffic, "traffic_algorithmic": b,
+             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, --cache-control none, bytes per "
+                               "pipeline launch (profiles/search_batched64_passes.md)" if traffic else None,
+             "kernel": "fused search pipeline (fwd_xy + z_mul + inv_peak per chunk)",
              "algorithmic_bytes_per_eval": bytes_per_eval(BOX), "evals_per_launch": evals_per_launch,
              "us_per_launch": per_launch_ms * 1e3}, passes)
 
