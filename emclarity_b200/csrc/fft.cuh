@@ -255,9 +255,55 @@ __host__ __device__ __forceinline__ constexpr int lpos(int i) {
 }
 __host__ __device__ constexpr int padded_len(int L) { return L + L / 8; }
 
-template <int L, int R, int NS, int SIGN, int P, int PAD>
+// Per-lane twiddles of stage S (NS = product of the earlier radices), kept in registers.  Lane
+// `lane` of a team always handles butterflies j = lane + b P, whose twiddle exponents depend on
+// k = j mod NS only -- not on which line the team transforms -- so a team can load them once
+// and reuse them for every line.  Stages whose cache would exceed kTwCacheMax complex values
+// (or that need no twiddles) read the shared-memory table instead.  The cache holds forward
+// twiddles; inverse stages use their conjugates.
+constexpr int kTwCacheMax = 8;
+
+template <int L, int P, int S, int NS>
+struct StageTw {
+  static constexpr int R = radix_of(L, S);
+  static constexpr int NB = L / R;
+  static constexpr int PER = (NB + P - 1) / P;
+  static constexpr bool kOn = NS > 1 && PER * (R - 1) <= kTwCacheMax;
+  float2 w[kOn ? PER : 1][kOn ? R - 1 : 1];
+  __device__ __forceinline__ void init(const float2* tw, int lane) {
+    if constexpr (kOn) {
+#pragma unroll
+      for (int b = 0; b < PER; ++b) {
+        const int k = (lane + b * P) % NS;
+#pragma unroll
+        for (int r = 1; r < R; ++r) w[b][r - 1] = tw[(r * k * (L / (NS * R))) % L];
+      }
+    }
+  }
+};
+
+template <int L, int P, int S, int NS>
+struct TwChain {
+  StageTw<L, P, S, NS> st;
+  TwChain<L, P, S + 1, NS * radix_of(L, S)> next;
+  __device__ __forceinline__ void init(const float2* tw, int lane) {
+    st.init(tw, lane);
+    next.init(tw, lane);
+  }
+};
+template <int L, int P, int S>
+struct TwChain<L, P, S, L> {
+  __device__ __forceinline__ void init(const float2*, int) {}
+};
+
+// Register twiddles of every stage of a length-L line transformed by teams of P lanes.
+template <int L, int P = team_size(L)>
+using LineTw = TwChain<L, P, 0, 1>;
+
+// One Stockham stage of radix R on a line of length L (cache: optional register twiddles).
+template <int L, int R, int NS, int SIGN, int P, int PAD, int S>
 __device__ __forceinline__ void stockham_stage(float2* buf, int stride, int lane, const float2* tw,
-                                               bool active) {
+                                               bool active, const StageTw<L, P, S, NS>* cache) {
   constexpr int NB = L / R;
   constexpr int PER = (NB + P - 1) / P;
   float2 v[PER][R];
@@ -275,9 +321,20 @@ __device__ __forceinline__ void stockham_stage(float2* buf, int stride, int lane
     const int j = lane + b * P;
     if (active && (PER * P == NB || j < NB)) {
       const int k = j % NS;
-      if (NS > 1) {
+      if constexpr (NS > 1) {
+        if constexpr (StageTw<L, P, S, NS>::kOn) {
+          if (cache) {
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], twiddle<SIGN>(tw, (r * k * (L / (NS * R))) % L));
+            for (int r = 1; r < R; ++r)
+              v[b][r] = SIGN < 0 ? cmul(v[b][r], cache->w[b][r - 1]) : cmulc(v[b][r], cache->w[b][r - 1]);
+          } else {
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], twiddle<SIGN>(tw, (r * k * (L / (NS * R))) % L));
+          }
+        } else {
+#pragma unroll
+          for (int r = 1; r < R; ++r) v[b][r] = cmul(v[b][r], twiddle<SIGN>(tw, (r * k * (L / (NS * R))) % L));
+        }
       }
       Dft<R, SIGN>::run(v[b]);
       const int idx = (j / NS) * NS * R + k;
@@ -290,25 +347,27 @@ __device__ __forceinline__ void stockham_stage(float2* buf, int stride, int lane
 
 template <int L, int SIGN, int P, int PAD, int S, int NS>
 struct StageChain {
-  static __device__ __forceinline__ void run(float2* buf, int stride, int lane, const float2* tw, bool active) {
+  static __device__ __forceinline__ void run(float2* buf, int stride, int lane, const float2* tw, bool active,
+                                             const TwChain<L, P, S, NS>* tc) {
     constexpr int R = radix_of(L, S);
-    stockham_stage<L, R, NS, SIGN, P, PAD>(buf, stride, lane, tw, active);
-    StageChain<L, SIGN, P, PAD, S + 1, NS * R>::run(buf, stride, lane, tw, active);
+    stockham_stage<L, R, NS, SIGN, P, PAD, S>(buf, stride, lane, tw, active, tc ? &tc->st : nullptr);
+    StageChain<L, SIGN, P, PAD, S + 1, NS * R>::run(buf, stride, lane, tw, active, tc ? &tc->next : nullptr);
   }
 };
 // terminate when the sub-transform length reaches L
 template <int L, int SIGN, int P, int PAD, int S>
 struct StageChain<L, SIGN, P, PAD, S, L> {
-  static __device__ __forceinline__ void run(float2*, int, int, const float2*, bool) {}
+  static __device__ __forceinline__ void run(float2*, int, int, const float2*, bool, const TwChain<L, P, S, L>*) {}
 };
 
 // In-place complex FFT of one line held by a team of P lanes.  Element i lives at
-// buf[lpos<PAD>(i) * stride].
+// buf[lpos<PAD>(i) * stride].  tc (optional) holds the team lane's register twiddles.
 template <int L, int SIGN, int P = team_size(L), int PAD = 0>
-__device__ __forceinline__ void fft_line(float2* buf, int stride, int lane, const float2* tw, bool active) {
+__device__ __forceinline__ void fft_line(float2* buf, int stride, int lane, const float2* tw, bool active,
+                                         const LineTw<L, P>* tc = nullptr) {
   static_assert(radix_of(L, 0) != 0, "unsupported FFT length");
   static_assert(P >= 1 && P <= 32 && (32 % P) == 0, "team must divide a warp");
-  StageChain<L, SIGN, P, PAD, 0, 1>::run(buf, stride, lane, tw, active);
+  StageChain<L, SIGN, P, PAD, 0, 1>::run(buf, stride, lane, tw, active, tc);
 }
 
 // Loads the length-L twiddle table into shared memory (cooperatively, whole block).

@@ -192,6 +192,11 @@ struct SearchCfg {
   static constexpr int TEAMS_LA = N <= 64 ? TEAMS_A : 16;
   static constexpr int TEAMS_LC = 16;  // (2 r + 1 + 1) / 2 <= 16 row pairs for r <= 15
   static constexpr size_t SMEM_A = sizeof(float2) * ((size_t)G * PY * NH + (size_t)TEAMS_LA * LP + N) + 64;
+  // resident pass-A CTAs per SM that shared memory allows (228 KB per SM, 1 KB reserved per CTA),
+  // and the target the register budget is capped for: 3 at 64^3 (80 registers), 2 for the larger
+  // boxes, whose FFT codelets need more registers
+  static constexpr int SMEM_CTAS_A = (int)((228 * 1024) / (SMEM_A + 1024));
+  static constexpr int MINB_A = N <= 64 ? 0 : (SMEM_CTAS_A < 2 ? SMEM_CTAS_A : 2);
   static constexpr size_t SMEM_B = sizeof(float2) * ((size_t)PY * NH + N);
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
 };
@@ -218,53 +223,82 @@ __device__ __forceinline__ Tv block_sum(Tv v, Tv* red) {
   return t;  // valid in thread 0
 }
 
-// Gather of the G planes of pass A through corner cells: U voxels per thread per step, all cell
-// loads of a step issued before any is used (memory-level parallelism for L2-resident cells).
+// Gather of the G planes of pass A through corner cells.  Each warp takes RU whole rows per step;
+// lane l samples x = l + 32 k (k < N / 32) of each, so one load instruction of a warp covers 32
+// consecutive voxels of a row (neighbouring cells, few L1 lines per request).  A thread computes
+// its sample point once per row and steps 32 voxels along x by adding 32 x (first column of the
+// sampling matrix); its RU * N / 32 cell loads are all issued before any is used.  Sums of r and
+// r^2 are formed per step in FP32 and accumulated in FP64.
 template <int N, typename T, int MODE, int GG>
 __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells, const float* __restrict__ mask,
                                              const float m[9], float tx, float ty, float tz, int z0,
                                              float* __restrict__ fplanes, double& s1, double& s2) {
   using C = SearchCfg<N, GG>;
-  constexpr int G = C::G, NT = C::NT_A, NH = C::NH, U = 4;
-  constexpr int TOTAL = G * N * N;
-  static_assert(TOTAL % (NT * U) == 0, "gather tiling");
+  constexpr int G = C::G, NT = C::NT_A, NH = C::NH;
+  constexpr int SEG = N / 32;                     // row segments per lane
+  constexpr int RU = SEG >= 3 ? 1 : 4 / SEG;      // rows per warp per step: U = RU * SEG loads in flight
+  constexpr int U = RU * SEG;
+  constexpr int WARPS = NT / 32;
+  constexpr int ROWS = G * N;
+  static_assert(N % 32 == 0 && ROWS % (WARPS * RU) == 0, "gather tiling");
   constexpr int c = N / 2;
-  for (int base = threadIdx.x; base < TOTAL; base += NT * U) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const float step_x = 32.f * m[0], step_y = 32.f * m[3], step_z = 32.f * m[6];
+#pragma unroll 1
+  for (int r0 = warp * RU; r0 < ROWS; r0 += WARPS * RU) {
     CellT<T> cv[U];
     float fr[U][3];
     bool ok[U];
     float mk[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int idx = base + u * NT;
-      const int x = idx % N, y = (idx / N) % N, zl = idx / (N * N);
-      const int z = z0 + zl;
-      const float pu = (float)(x - c) - tx, pv = (float)(y - c) - ty, pw = (float)(z - c) - tz;
-      const float sx = fmaf(m[0], pu, fmaf(m[1], pv, m[2] * pw)) + (float)c;
-      const float sy = fmaf(m[3], pu, fmaf(m[4], pv, m[5] * pw)) + (float)c;
-      const float sz = fmaf(m[6], pu, fmaf(m[7], pv, m[8] * pw)) + (float)c;
-      const long ci = cell_index<MODE>(N, sx, sy, sz, fr[u], &ok[u]);
-      cv[u] = load_cell(cells + ci);
-      mk[u] = mask ? __ldg(mask + ((long)z * N + y) * N + x) : 1.f;
-    }
+    for (int ru = 0; ru < RU; ++ru) {
+      const int row = r0 + ru, y = row % N, zl = row / N, z = z0 + zl;
+      const float pu = (float)(lane - c) - tx, pv = (float)(y - c) - ty, pw = (float)(z - c) - tz;
+      float sx = fmaf(m[0], pu, fmaf(m[1], pv, m[2] * pw)) + (float)c;
+      float sy = fmaf(m[3], pu, fmaf(m[4], pv, m[5] * pw)) + (float)c;
+      float sz = fmaf(m[6], pu, fmaf(m[7], pv, m[8] * pw)) + (float)c;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int idx = base + u * NT;
-      const int x = idx % N, y = (idx / N) % N, zl = idx / (N * N);
-      float v[8];
-      cell_values(cv[u], v);
-      float val = ok[u] ? cell_trilinear(v, fr[u]) : 0.f;
-      val *= mk[u];
-      fplanes[((size_t)zl * C::PY + lpos<1>(y)) * (2 * NH) + x] = val;
-      s1 += (double)val;
-      s2 += (double)val * (double)val;
+      for (int k = 0; k < SEG; ++k) {
+        const int u = ru * SEG + k;
+        const long ci = cell_index<MODE>(N, sx, sy, sz, fr[u], &ok[u]);
+        cv[u] = load_cell(cells + ci);
+        mk[u] = mask ? __ldg(mask + ((long)z * N + y) * N + lane + 32 * k) : 1.f;
+        sx += step_x;
+        sy += step_y;
+        sz += step_z;
+      }
     }
+    float p1 = 0.f, p2 = 0.f;
+#pragma unroll
+    for (int ru = 0; ru < RU; ++ru) {
+      const int row = r0 + ru, y = row % N, zl = row / N;
+      float* dst = fplanes + ((size_t)zl * C::PY + lpos<1>(y)) * (2 * NH) + lane;
+#pragma unroll
+      for (int k = 0; k < SEG; ++k) {
+        const int u = ru * SEG + k;
+        float cvv[8];
+        cell_values(cv[u], cvv);
+        const float val = (ok[u] ? cell_trilinear(cvv, fr[u]) : 0.f) * mk[u];
+        dst[32 * k] = val;
+        p1 += val;
+        p2 = fmaf(val, val, p2);
+      }
+    }
+    s1 += (double)p1;
+    s2 += (double)p2;
   }
+}
+
+// Column of the y transforms handled as line li of a plane: the N/2 lines are spread so that the
+// teams of a half-warp touch different shared-memory banks (H = N/2, a multiple of 4).
+template <int H>
+__device__ __forceinline__ int spread_half(int li) {
+  return (li % 4) * (H / 4) + li / 4;
 }
 
 // ------------------------------------------------------------------ pass A
 template <int N, typename T, int GG = 0>
-__global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A) k_search_fwd_xy(const SearchChunkArgs a,
+__global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB_A) k_search_fwd_xy(const SearchChunkArgs a,
                                                                            const float2* __restrict__ g_tw) {
   using C = SearchCfg<N, GG>;
   constexpr int NH = C::NH, G = C::G, P = C::P;
@@ -329,6 +363,8 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A) k_search_fwd_xy(const 
   __syncthreads();
 
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  LineTw<N, P> tc;
+  tc.init(s_tw, lane);
   // 2. R2C along x: rows 2q and 2q+1 of the slab share one complex FFT
   {
     constexpr int NPAIRS = G * N / 2;
@@ -345,39 +381,57 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A) k_search_fwd_xy(const 
       if (active)
         for (int n = lane; n < N; n += P) buf[lpos<1>(n)] = make_float2(ra[n], rb[n]);
       __syncwarp();
-      fft_line<N, -1, P, 1>(buf, 1, lane, s_tw, active);
+      fft_line<N, -1, P, 1>(buf, 1, lane, s_tw, active, &tc);
       if (active) {
+        // columns 0 and N/2 of a row transform are real: row a's pair goes to slot 0 of row a,
+        // row b's to slot 0 of row b, as (X(0), X(N/2)), so the y pass needs N/2 complex lines
         float2* oa = planes + row_a * NH;
         float2* ob = oa + NH;
-        for (int k = lane; k < NH; k += P) {
-          const float2 zk = buf[lpos<1>(k)], zm = buf[lpos<1>((N - k) % N)];
-          oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-          ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        for (int k = lane; k < NH - 1; k += P) {
+          const float2 zk = buf[lpos<1>(k)], zm = buf[lpos<1>(k ? N - k : N / 2)];
+          if (k == 0) {
+            oa[0] = make_float2(zk.x, zm.x);
+            ob[0] = make_float2(zk.y, zm.y);
+          } else {
+            oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+            ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+          }
         }
       }
       __syncwarp();
     }
   }
   __syncthreads();
-  // 3. FFT along y for every (plane, kx) column
+  // 3. FFT along y for columns 0 .. N/2-1 of every plane (column 0 carries X(0) + i X(N/2))
   {
-    constexpr int NLINES = G * NH;
+    constexpr int NLINES = G * (N / 2);
     for (int base = 0; base < NLINES; base += C::TEAMS_A) {
       const int li = base + team;
       const bool active = li < NLINES;
-      const int zl = active ? li / NH : 0, kx = active ? spread_kx<NH>(li % NH) : 0;
-      fft_line<N, -1, P, 1>(planes + (size_t)zl * PY * NH + kx, NH, lane, s_tw, active);
+      const int zl = active ? li / (N / 2) : 0, kx = active ? spread_half<N / 2>(li % (N / 2)) : 0;
+      fft_line<N, -1, P, 1>(planes + (size_t)zl * PY * NH + kx, NH, lane, s_tw, active, &tc);
     }
   }
   __syncthreads();
-  // 4. store the slab: S1[e][z0 + zl][y][kx], rows gathered from their padded positions
+  // 4. store the slab: S1[e][z0 + zl][y][kx], rows gathered from their padded positions; columns
+  //    0 and N/2 are separated from the packed column 0: with Z = F(X(0) + i X(N/2)),
+  //    F X(0)(y) = (Z(y) + conj Z(-y)) / 2 and F X(N/2)(y) = (Z(y) - conj Z(-y)) / 2i
   {
     float2* dst = a.s1 + ((size_t)e * N + z0) * N * NH;
     constexpr int NV = G * N * NH;
     for (int i = threadIdx.x; i < NV; i += C::NT_A) {
       const int row = i / NH, kx = i % NH;  // row = zl * N + y
       const int zl = row / N, y = row % N;
-      dst[i] = planes[((size_t)zl * PY + lpos<1>(y)) * NH + kx];
+      const float2* pl = planes + (size_t)zl * PY * NH;
+      float2 v;
+      if (kx == 0 || kx == NH - 1) {
+        const float2 zp = pl[lpos<1>(y) * NH], zm = pl[lpos<1>((N - y) % N) * NH];
+        v = kx == 0 ? make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y))
+                    : make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
+      } else {
+        v = pl[lpos<1>(y) * NH + kx];
+      }
+      dst[i] = v;
     }
   }
 }
@@ -514,10 +568,12 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
   }
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  LineTw<N, P> tc;
+  tc.init(s_tw, lane);
   for (int base = 0; base < NH; base += C::TEAMS_BC) {
     const int li = base + team;
     const int kx = li < NH ? spread_kx<NH>(li) : 0;
-    fft_line<N, 1, P, 1>(tile + kx, NH, lane, s_tw, li < NH);
+    fft_line<N, 1, P, 1>(tile + kx, NH, lane, s_tw, li < NH, &tc);
   }
   __syncthreads();
 
@@ -551,7 +607,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
       }
     }
     __syncwarp();
-    fft_line<N, 1, P, 1>(buf, 1, lane, s_tw, active);
+    fft_line<N, 1, P, 1>(buf, 1, lane, s_tw, active, &tc);
     if (active) {
       for (int t = lane; t < 2 * w; t += P) {
         const int which = t / w;  // 0: row a, 1: row b
