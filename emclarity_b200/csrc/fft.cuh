@@ -360,6 +360,28 @@ struct StageChain<L, SIGN, P, PAD, S, L> {
   static __device__ __forceinline__ void run(float2*, int, int, const float2*, bool, const TwChain<L, P, S, L>*) {}
 };
 
+// First stage (NS = 1, no twiddles) with its inputs produced by ld(i) -- element i of the line
+// -- instead of loaded from the buffer, so a caller that builds the line (packing two real rows,
+// Hermitian extension) skips one shared-memory round trip.
+template <int L, int R, int SIGN, int P, int PAD, class Ld>
+__device__ __forceinline__ void stockham_first_stage_in(const Ld& ld, float2* buf, int stride, int lane, bool active) {
+  constexpr int NB = L / R;
+  constexpr int PER = (NB + P - 1) / P;
+  float2 v[PER][R];
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int j = lane + b * P;
+    if (active && (PER * P == NB || j < NB)) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = ld(j + r * NB);
+      Dft<R, SIGN>::run(v[b]);
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[lpos<PAD>(j * R + r) * stride] = v[b][r];
+    }
+  }
+  __syncwarp();
+}
+
 // In-place complex FFT of one line held by a team of P lanes.  Element i lives at
 // buf[lpos<PAD>(i) * stride].  tc (optional) holds the team lane's register twiddles.
 template <int L, int SIGN, int P = team_size(L), int PAD = 0>
@@ -368,6 +390,17 @@ __device__ __forceinline__ void fft_line(float2* buf, int stride, int lane, cons
   static_assert(radix_of(L, 0) != 0, "unsupported FFT length");
   static_assert(P >= 1 && P <= 32 && (32 % P) == 0, "team must divide a warp");
   StageChain<L, SIGN, P, PAD, 0, 1>::run(buf, stride, lane, tw, active, tc);
+}
+
+// FFT of a line whose elements come from ld(i) (see stockham_first_stage_in); the result is left
+// in buf like fft_line's.
+template <int L, int SIGN, int P = team_size(L), int PAD = 0, class Ld>
+__device__ __forceinline__ void fft_line_in(const Ld& ld, float2* buf, int stride, int lane, const float2* tw,
+                                            bool active, const LineTw<L, P>* tc = nullptr) {
+  static_assert(radix_of(L, 0) != 0, "unsupported FFT length");
+  constexpr int R0 = radix_of(L, 0);
+  stockham_first_stage_in<L, R0, SIGN, P, PAD>(ld, buf, stride, lane, active);
+  StageChain<L, SIGN, P, PAD, 1, R0>::run(buf, stride, lane, tw, active, tc ? &tc->next : nullptr);
 }
 
 // Loads the length-L twiddle table into shared memory (cooperatively, whole block).

@@ -100,6 +100,24 @@ __device__ __forceinline__ long cell_index(int n, float sx, float sy, float sz, 
   return ((long)(z0 + 1) * nc + (y0 + 1)) * nc + (x0 + 1);
 }
 
+// cell_index for the search gather: floor by a round-down conversion, 32-bit index arithmetic,
+// and no clamping -- an invalid sample reads cell 0 and its value is discarded by the caller
+// (`valid` false), so only in-range indices ever reach memory.
+template <int MODE>
+__device__ __forceinline__ unsigned cell_index_gather(int n, float sx, float sy, float sz, float f[3], bool& valid) {
+  valid = MODE == EMC_INTERP_LINEAR_BORDER
+              ? (sx > -1.f && sy > -1.f && sz > -1.f && sx < (float)n && sy < (float)n && sz < (float)n)
+              : (sx >= 0.f && sy >= 0.f && sz >= 0.f && sx <= (float)(n - 1) && sy <= (float)(n - 1) &&
+                 sz <= (float)(n - 1));
+  const int x0 = __float2int_rd(sx), y0 = __float2int_rd(sy), z0 = __float2int_rd(sz);
+  f[0] = sx - (float)x0;
+  f[1] = sy - (float)y0;
+  f[2] = sz - (float)z0;
+  const unsigned nc = (unsigned)n + 1u;
+  const unsigned idx = ((unsigned)(z0 + 1) * nc + (unsigned)(y0 + 1)) * nc + (unsigned)(x0 + 1);
+  return valid ? idx : 0u;
+}
+
 // Same interpolation order as sample_linear, so both paths give identical results.
 __device__ __forceinline__ float cell_trilinear(const float v[8], const float f[3]) {
   const float c00 = fmaf(f[0], v[1] - v[0], v[0]), c10 = fmaf(f[0], v[3] - v[2], v[2]);
@@ -260,7 +278,7 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
 #pragma unroll
       for (int k = 0; k < SEG; ++k) {
         const int u = ru * SEG + k;
-        const long ci = cell_index<MODE>(N, sx, sy, sz, fr[u], &ok[u]);
+        const unsigned ci = cell_index_gather<MODE>(N, sx, sy, sz, fr[u], ok[u]);
         cv[u] = load_cell(cells + ci);
         mk[u] = mask ? __ldg(mask + ((long)z * N + y) * N + lane + 32 * k) : 1.f;
         sx += step_x;
@@ -378,10 +396,7 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
       const size_t row_a = (size_t)zl * PY + lpos<1>(ya);
       const float* ra = fplanes + row_a * (2 * NH);
       const float* rb = ra + 2 * NH;
-      if (active)
-        for (int n = lane; n < N; n += P) buf[lpos<1>(n)] = make_float2(ra[n], rb[n]);
-      __syncwarp();
-      fft_line<N, -1, P, 1>(buf, 1, lane, s_tw, active, &tc);
+      fft_line_in<N, -1, P, 1>([&](int n) { return make_float2(ra[n], rb[n]); }, buf, 1, lane, s_tw, active, &tc);
       if (active) {
         // columns 0 and N/2 of a row transform are real: row a's pair goes to slot 0 of row a,
         // row b's to slot 0 of row b, as (X(0), X(N/2)), so the y pass needs N/2 complex lines
@@ -593,21 +608,20 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
     const int ja = 2 * pr, jb = 2 * pr + 1;
     const bool has_b = jb < w;
     const int ya = (ja - r + N) % N, yb = has_b ? (jb - r + N) % N : ya;
-    if (active) {
-      const float2* ra = tile + (size_t)lpos<1>(ya) * NH;
-      const float2* rb = tile + (size_t)lpos<1>(yb) * NH;
-      for (int n = lane; n < N; n += P) {
-        const bool lower = n <= N / 2;
-        const int k = lower ? n : N - n;
-        float2 A = ra[k];
-        float2 B = has_b ? rb[k] : make_float2(0.f, 0.f);
-        if (k == 0 || 2 * k == N) { A.y = 0.f; B.y = 0.f; }
-        if (!lower) { A.y = -A.y; B.y = -B.y; }
-        buf[lpos<1>(n)] = make_float2(A.x - B.y, A.y + B.x);
-      }
-    }
-    __syncwarp();
-    fft_line<N, 1, P, 1>(buf, 1, lane, s_tw, active, &tc);
+    const float2* ra = tile + (size_t)lpos<1>(ya) * NH;
+    const float2* rb = tile + (size_t)lpos<1>(yb) * NH;
+    // Hermitian extension of rows a and b packed as a + i b
+    fft_line_in<N, 1, P, 1>(
+        [&](int n) {
+          const bool lower = n <= N / 2;
+          const int k = lower ? n : N - n;
+          float2 A = ra[k];
+          float2 B = has_b ? rb[k] : make_float2(0.f, 0.f);
+          if (k == 0 || 2 * k == N) { A.y = 0.f; B.y = 0.f; }
+          if (!lower) { A.y = -A.y; B.y = -B.y; }
+          return make_float2(A.x - B.y, A.y + B.x);
+        },
+        buf, 1, lane, s_tw, active, &tc);
     if (active) {
       for (int t = lane; t < 2 * w; t += P) {
         const int which = t / w;  // 0: row a, 1: row b
