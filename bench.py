@@ -524,6 +524,92 @@ def run_tsearch(args):
                          "frac": byts / per_orient / 1e9 / pk, "peak_source": which}}
 
 
+def run_average(args):
+    """Subtomogram averaging (the accumulation loop of BH_average3d): P extracted 64^3 windows holding
+    noisy rotated, shifted copies of a reference, seeded rotations / subvoxel shifts / peak weights,
+    alternating half sets, 8 tilt-group wedge weights (64^3), C1.  One step = reset + add all P + read
+    both half-set averages."""
+    import torch
+
+    from emclarity_b200 import api, synthetic
+    from oracle import oracle as O
+    n = nw = 64
+    P = args.particles if args.particles != 1200 else 1024
+    rng = np.random.default_rng(99)
+    ref = synthetic.blob_reference(rng, n)
+    ip = api.Interpolator(torch.from_numpy(ref).cuda(), interp="linear_border")
+    d_parts = torch.empty((P, n, n, n), dtype=torch.float32, device="cuda")
+    rots, shifts = [], []
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    for i in range(P):
+        R = api.define_matrix(synthetic.random_euler(rng), "inv")
+        t = rng.uniform(-2, 2, 3)
+        ip.interp3d(R.T, t, "forward", out=d_parts[i])
+        rots.append(R)
+        shifts.append(t)
+    d_parts += 0.5 * torch.randn(d_parts.shape, device="cuda", generator=gen)
+    rots = np.array(rots)
+    shifts = np.array(shifts, np.float32)
+    weights = rng.uniform(0.5, 1.0, P).astype(np.float32)
+    halves = 1 + (np.arange(P) % 2)
+    wedges = torch.rand((8, nw, nw, nw), device="cuda", generator=gen)
+    widx = np.arange(P) % 8
+    mask = torch.from_numpy(synthetic.soft_sphere_mask(n, 28)).cuda()
+    avg = api.Average(mask, wedge_box=nw)
+    h_parts = d_parts.cpu().pin_memory()
+    h_avg = torch.empty((2, n, n, n), dtype=torch.float32).pin_memory()
+
+    def step(src):
+        avg.reset()
+        avg.add(src, rots, halves, shifts=shifts, weights=weights, wedges=wedges, wedge_index=widx)
+        return avg.result(1)[0], avg.result(2)[0]
+
+    for _ in range(args.warmup):
+        step(d_parts)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(d_parts)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # end to end: pinned host windows -> device -> average -> both half averages back to the host
+    d_in = torch.empty_like(d_parts)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        d_in.copy_(h_parts, non_blocking=True)
+        a1, a2 = step(d_in)
+        h_avg[0].copy_(a1, non_blocking=True)
+        h_avg[1].copy_(a2, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    # CPU: the FP64 restatement on a bounded sample
+    k = 8
+    t0 = time.time()
+    O.average_np(list(h_parts[:k].numpy()), mask.cpu().numpy(), list(rots[:k]), halves[:k], shifts=shifts[:k],
+                 weights=weights[:k], wedges=list(wedges.cpu().numpy()), wedge_index=widx[:k])
+    cpu_rate = k / (time.time() - t0)
+    byts = 4 * n ** 3 + 4 * nw ** 3
+    pk, which = measured_peaks()
+    rate = P / (ms / 1e3)
+    return {"metric": "particles/s averaged (64^3, with 64^3 wedge weights)", "value": rate,
+            "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "%d extracted 64^3 windows, odd/even half sets, 8 wedge weights 64^3, C1, one "
+                                   "emc_average_add per step" % P},
+            "e2e": {"value": P / (e2e_ms / 1e3), "unit": "particles/s", "h2d_bytes_per_step": int(h_parts.numel() * 4),
+                    "d2h_bytes_per_step": int(h_avg.numel() * 4)},
+            "roofline": {"bound": "hbm", "achieved": byts * rate / 1e9, "peak": pk, "unit": "GB/s",
+                         "frac": byts * rate / 1e9 / pk, "peak_source": which,
+                         "algorithmic_bytes_per_particle": byts},
+            "cpu_baseline": {"value": cpu_rate, "unit": "particles/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "%d particles through the FP64 restatement (C rotation, numpy sums)" % k}}
+
+
 def _rodrigues(axis, deg):
     a = np.asarray(axis, dtype=np.float64)
     a = a / np.linalg.norm(a)
@@ -631,13 +717,13 @@ def main():
     ap.add_argument("--particles", type=int, default=1200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--planes", type=int, default=0, help="pass-A z-planes per CTA (0: timed choice)")
-    ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine"])
+    ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine", "average"])
     args = ap.parse_args()
     if args.impl == "ours" and args.workload != "batched64":
         import torch
         torch.cuda.set_device(0)
         fn = {"mixed": run_mixed, "bf16": lambda a: run_mixed(a, "bf16"), "tsearch": run_tsearch,
-              "refine": run_refine}[args.workload]
+              "refine": run_refine, "average": run_average}[args.workload]
         print(json.dumps(fn(args)))
         return
     if args.impl == "reference":

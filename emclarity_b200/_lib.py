@@ -96,6 +96,12 @@ SIGNATURES = {
     "emc_tsearch_create": (_i, [_vp, _i, _i, _i, C.POINTER(_vp), _vp]),
     "emc_tsearch_run": (_i, [_vp, _vp, _i, _pd, _i, _vp, _vp, _vp]),
     "emc_tsearch_destroy": (_i, [_vp]),
+    "emc_symmetry_matrices": (_i, [C.c_char_p, _pd, _pi]),
+    "emc_average_create": (_i, [_i, _vp, _f, _i, _pd, _i, _i, C.POINTER(_vp), _vp]),
+    "emc_average_add": (_i, [_vp, _vp, _i, _pd, _pf, _pf, _pi, _vp, _i, _pi, _pi, _vp]),
+    "emc_average_result": (_i, [_vp, _i, _vp, _vp, C.POINTER(C.c_long), _vp]),
+    "emc_average_reset": (_i, [_vp, _vp]),
+    "emc_average_destroy": (_i, [_vp]),
 }
 
 _lib = None

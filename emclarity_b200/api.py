@@ -10,6 +10,7 @@ argument meaning of the reference call it replaces:
                           with the normalised translational CC of
                           statistics/BH_multi_xcf_Translational_2.m
 * ``TemplateSearch``      alignment/BH_templateSearch3d_2.m:633-887
+* ``Average``             transformations/BH_average3d.m:1207-1707 (half-set sums)
 
 Tensors are torch CUDA tensors used as device buffers only; volumes have shape
 (nz, ny, nx) (x fastest, the reference's column-major order), half spectra are complex64
@@ -378,6 +379,79 @@ class TemplateSearch:
     def close(self):
         if getattr(self, "_h", None):
             L.load().emc_tsearch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------- averaging
+def symmetry_matrices(symmetry):
+    """The operators interpolator applies for 'C<n>', 'D<n>' or 'O' as (k, 3, 3) float64 arrays
+    (testScripts/interpolator.m:172-214)."""
+    cnt = C.c_int(0)
+    L.call("emc_symmetry_matrices", symmetry.encode(), None, C.byref(cnt))
+    out = np.zeros(9 * cnt.value)
+    L.call("emc_symmetry_matrices", symmetry.encode(), out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cnt))
+    return out.reshape(cnt.value, 3, 3).transpose(0, 2, 1).copy()  # column-major -> (row, col)
+
+
+class Average:
+    """Odd / even half-set subtomogram sums of BH_average3d (transformations/BH_average3d.m:1207-1707).
+
+    ``add(particles, rotations, shifts, weights, halves, wedges=None, wedge_index=None)`` rotates each
+    extracted window back with interpolator(..., 'inv', symmetry), normalises it inside
+    ``mask > bin_threshold``, multiplies by the soft mask and adds it (times its peak weight) to
+    its half set; ``result(half)`` returns (sum / count, summed rotated weights, count).
+    """
+
+    def __init__(self, mask, symmetry="C1", wedge_box=0, bin_threshold=0.01, batch=0):
+        n = mask.shape[-1]
+        self.n, self.nw = n, int(wedge_box)
+        sym = symmetry_matrices(symmetry) if isinstance(symmetry, str) else np.asarray(symmetry, np.float64)
+        packed, pp = _dptr(np.concatenate([m.flatten(order="F") for m in sym.reshape(-1, 3, 3)]))
+        h = C.c_void_p()
+        L.call("emc_average_create", n, _need_cuda(mask, "mask"), float(bin_threshold), self.nw, pp, len(sym),
+               int(batch), C.byref(h), _stream())
+        self._h = h
+        self._keep = packed
+
+    def add(self, particles, rotations, halves, shifts=None, weights=None, wedges=None, wedge_index=None):
+        k = particles.shape[0]
+        rot = np.ascontiguousarray(np.concatenate([np.asarray(r, np.float64).reshape(3, 3).flatten(order="F")
+                                                   for r in np.asarray(rotations).reshape(-1, 3, 3)]))
+        hv = np.ascontiguousarray(halves, dtype=np.int32).reshape(k)
+        sh = None if shifts is None else np.ascontiguousarray(shifts, dtype=np.float32).reshape(k, 3)
+        wt = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32).reshape(k)
+        kept = np.zeros(k, dtype=np.int32)
+        wp, nwdg, wi = None, 0, None
+        if wedges is not None:
+            wp, nwdg = _need_cuda(wedges, "wedges"), wedges.shape[0]
+            wi = np.ascontiguousarray(wedge_index, dtype=np.int32).reshape(k)
+        fp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+        ip = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_int))
+        L.call("emc_average_add", self._h, _need_cuda(particles, "particles"), k,
+               rot.ctypes.data_as(C.POINTER(C.c_double)), fp(sh), fp(wt), ip(hv), wp, nwdg, ip(wi), ip(kept),
+               _stream())
+        return kept.astype(bool)
+
+    def result(self, half):
+        avg = torch.empty((self.n,) * 3, dtype=torch.float32, device="cuda")
+        wsum = torch.empty((self.nw,) * 3, dtype=torch.float32, device="cuda") if self.nw else None
+        cnt = C.c_long(0)
+        L.call("emc_average_result", self._h, int(half), _need_cuda(avg, "avg"),
+               None if wsum is None else _need_cuda(wsum, "wedge_sum"), C.byref(cnt), _stream())
+        return avg, wsum, cnt.value
+
+    def reset(self):
+        L.call("emc_average_reset", self._h, _stream())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.load().emc_average_destroy(self._h)
             self._h = None
 
     def __del__(self):

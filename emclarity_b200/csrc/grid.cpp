@@ -3,6 +3,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "../../include/emc_b200.h"
@@ -124,6 +125,55 @@ emc_status emc_euler_search(const char* symmetry, double theta_max, double theta
       }
   }
   *count = total;
+  return EMC_OK;
+}
+
+// The symmetry operators the interpolator applies (testScripts/interpolator.m:172-214, used by
+// interp3d over iSym = 1:nSymMats):  C<n>: defineMatrix([0, 0, k 360/n], 'Bah', 'forward'),
+// k = 0..n-1.  D<n>: the same n in-plane rotations -- check_symmetry also stores their mirrored
+// copies (element-wise times [1 -1 1; 1 -1 1; 1 1 -1]) after them, but sets nSymMats = n before
+// adding them, so the interpolator never applies the copies.  O: the 24 rotations of the cube
+// (the signed permutation matrices of determinant +1, identity first).
+emc_status emc_symmetry_matrices(const char* symmetry, double* out, int* count) {
+  if (!symmetry || !count) {
+    emc::set_error("emc_symmetry_matrices: null argument");
+    return EMC_E_ARG;
+  }
+  std::vector<double> mats;
+  const char kind = symmetry[0];
+  if (kind == 'C' || kind == 'D') {
+    char* end = nullptr;
+    const long n = strtol(symmetry + 1, &end, 10);
+    if (end == symmetry + 1 || *end != '\0' || n < 1 || n > 30) {
+      emc::set_error("emc_symmetry_matrices: '%s' needs an order 1..30", symmetry);
+      return EMC_E_ARG;
+    }
+    const double inc = 360.0 / (double)n;
+    for (long k = 0; k < n; ++k) {
+      double R[9];
+      const double ang[3] = {0.0, 0.0, (double)k * inc};
+      const emc_status rs = emc_define_matrix(ang, 0, R);
+      if (rs != EMC_OK) return rs;
+      mats.insert(mats.end(), R, R + 9);
+    }
+  } else if (kind == 'O' && symmetry[1] == '\0') {
+    const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    const int perm_sign[6] = {1, -1, -1, 1, 1, -1};
+    for (int p = 0; p < 6; ++p)
+      for (int s = 0; s < 8; ++s) {
+        const int sg[3] = {(s & 1) ? -1 : 1, (s & 2) ? -1 : 1, (s & 4) ? -1 : 1};
+        if (perm_sign[p] * sg[0] * sg[1] * sg[2] != 1) continue;
+        double R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < 3; ++i) R[i + 3 * perms[p][i]] = sg[i];  // row i has its entry in column perm[i]
+        mats.insert(mats.end(), R, R + 9);
+      }
+  } else {
+    emc::set_error("emc_symmetry_matrices: symmetry '%s' not supported (C<n>, D<n>, O)", symmetry);
+    return EMC_E_UNSUPPORTED;
+  }
+  const int n = (int)(mats.size() / 9);
+  if (out) std::copy(mats.begin(), mats.end(), out);
+  *count = n;
   return EMC_OK;
 }
 

@@ -344,6 +344,49 @@ EMC_API emc_status emc_tsearch_run(emc_tsearch_t h, const float* d_template, int
                            float* d_peak, float* d_angle, void* stream);
 EMC_API emc_status emc_tsearch_destroy(emc_tsearch_t h);
 
+/* ------------------------------------------------------------------------ */
+/* Subtomogram averaging (transformations/BH_average3d.m:1207-1500)           */
+/* ------------------------------------------------------------------------ */
+
+/* Symmetry operators the interpolator applies for "C<n>", "D<n>" or "O"
+ * (testScripts/interpolator.m:172-214), column-major 3x3 each, identity first.  For D<n> that is
+ * the n in-plane rotations only: the reference stores the mirrored copies but never applies them
+ * (nSymMats = n).  out may be NULL to query *count; at most 60 matrices. */
+EMC_API emc_status emc_symmetry_matrices(const char* symmetry, double* out, int* count);
+
+typedef struct emc_average_s* emc_average_t;
+
+/* Running odd / even half-set sums of BH_average3d.  n: particle box; d_mask: the soft
+ * interpolation mask interpMask (n^3, device; copied), whose voxels > bin_threshold (0.01 in the
+ * reference, :1087-1092) form the statistics region; nw: box of the wedge / CTF weights (0: no
+ * weights); sym / nsym: symmetry matrices (column-major, as emc_symmetry_matrices; NULL and 1 for
+ * C1); batch: particles rotated per pass (0: sized for about 2 GB of scratch). */
+EMC_API emc_status emc_average_create(int n, const float* d_mask, float bin_threshold, int nw,
+                                      const double* sym, int nsym, int batch, emc_average_t* out,
+                                      void* stream);
+/* Adds particles, in order (:1417-1482).  d_particles: count extracted windows [count][n^3]
+ * (device); rot: [count][9] host, the geometry's rotation matrix (columns 17:25, column-major);
+ * shift: [count][3] host (NULL = 0), the subvoxel shift of the window; weight: [count] host
+ * (peakWgt; NULL = 1); half: [count] host, 1 (ODD) or 2 (EVE).  Each particle is rotated with
+ * interpolator(vol, rot, shift, 'inv', symmetry): s = (rot S_k)(p - c) + shift + c with a zero
+ * border, averaged over k; normalised r = (r - mean(r(B))) / rms(r(B) - mean) .* mask; dropped
+ * when mean(r(:)) is not finite; then r .* weight is added to its half set.  With wedges,
+ * d_wedges holds n_wedges weight volumes [n_wedges][nw^3] (device) and wedge_index[p] picks the
+ * particle's one, rotated the same way with a zero shift and added (times weight) when the
+ * particle is kept.  kept (host, may be NULL): 1 for particles added, 0 for dropped ones.
+ * Synchronises the stream. */
+EMC_API emc_status emc_average_add(emc_average_t a, const float* d_particles, int count,
+                                   const double* rot, const float* shift, const float* weight,
+                                   const int* half, const float* d_wedges, int n_wedges,
+                                   const int* wedge_index, int* kept, void* stream);
+/* Half set `half` (1 or 2): d_avg (n^3, may be NULL) = sum / count (:1703-1707; NaN when the half
+ * set is empty), d_wedge_sum (nw^3, may be NULL) = the summed rotated weights, *count (may be
+ * NULL) = particles added. */
+EMC_API emc_status emc_average_result(emc_average_t a, int half, float* d_avg, float* d_wedge_sum,
+                                      long* count, void* stream);
+EMC_API emc_status emc_average_reset(emc_average_t a, void* stream);
+EMC_API emc_status emc_average_destroy(emc_average_t a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -366,3 +366,69 @@ def xcf_rotational_np(P, R, wdg_mask=None, ref_wdg=None, nx=None):
     num = np.sum(hw * np.real(rw * P * R * wm))
     den = np.sum(hw * np.abs(R * wm) ** 2) * np.sum(hw * np.abs(P * rw) ** 2)
     return num / math.sqrt(den)
+
+
+def symmetry_matrices_np(symmetry):
+    """interpolator.check_symmetry operators as applied by interp3d (testScripts/interpolator.m:172-214):
+    C<n> / D<n>: defineMatrix([0, 0, k 360/n], 'Bah', 'forward') for k < n (for D<n> nSymMats = n, so the
+    stored mirrored copies are never applied); O: the 24 proper signed permutation matrices."""
+    kind = symmetry[0]
+    if kind in "CD":
+        n = int(symmetry[1:])
+        return np.array([define_matrix_np([0.0, 0.0, k * 360.0 / n], "forward") for k in range(n)])
+    if symmetry == "O":
+        import itertools
+        out = []
+        for perm in itertools.permutations(range(3)):
+            for signs in itertools.product((1, -1), repeat=3):
+                m = np.zeros((3, 3))
+                for i in range(3):
+                    m[i, perm[i]] = signs[i]
+                if round(np.linalg.det(m)) == 1:
+                    out.append(m)
+        return np.array(out)
+    raise ValueError("symmetry %s" % symmetry)
+
+
+def average_np(particles, mask, rotations, halves, shifts=None, weights=None, wedges=None, wedge_index=None,
+               symmetry=None, bin_threshold=0.01):
+    """FP64 restatement of the accumulation loop of transformations/BH_average3d.m:1417-1482 and the
+    final division (:1703-1707).  Per particle: r = interpolator(particle, R, shift, 'inv', symmetry)
+    (testScripts/interpolator.m:29-78: zero-border trilinear of mexXform3d, the sum over R S_k divided
+    by the number of operators); r = (r - mean(r(B))) / rms(r(B) - mean) .* mask with B = mask >
+    bin_threshold (:1087-1092, :1439-1441); skipped when mean(r(:)) is not finite (:1450-1456); r .*
+    weight added to the sum of its half set, and the rotated wedge (zero shift) times weight to the
+    half set's wedge sum.  Returns {half: (average, wedge_sum or None, count)} and the kept flags."""
+    k = len(particles)
+    syms = [np.eye(3)] if symmetry is None else list(symmetry)
+    n = particles[0].shape[-1]
+    B = mask > bin_threshold
+    sums = {1: np.zeros((n,) * 3), 2: np.zeros((n,) * 3)}
+    nw = wedges[0].shape[-1] if wedges is not None else 0
+    wsums = {1: np.zeros((nw,) * 3), 2: np.zeros((nw,) * 3)} if nw else None
+    counts = {1: 0, 2: 0}
+    kept = np.zeros(k, dtype=bool)
+    for p in range(k):
+        R = np.asarray(rotations[p], dtype=np.float64).reshape(3, 3)
+        sh = (0.0, 0.0, 0.0) if shifts is None else tuple(float(v) for v in shifts[p])
+        w = 1.0 if weights is None else float(weights[p])
+        r = rotate(np.asarray(particles[p], np.float64), R, sh, "inv", interp=2, symmetry=syms)
+        mu = r[B].mean()
+        r = r - mu
+        r = r / np.sqrt(np.mean(r[B] ** 2))
+        r = r * mask
+        if not np.isfinite(r.mean()):
+            continue
+        kept[p] = True
+        h = int(halves[p])
+        sums[h] += r * w
+        counts[h] += 1
+        if nw:
+            wv = rotate(np.asarray(wedges[int(wedge_index[p])], np.float64), R, (0.0, 0.0, 0.0), "inv", interp=2,
+                        symmetry=syms)
+            wsums[h] += wv * w
+    out = {}
+    for h in (1, 2):
+        avg = sums[h] / counts[h] if counts[h] else np.full((n,) * 3, np.nan)
+        out[h] = (avg, wsums[h] if nw else None, counts[h])
+    return out, kept
