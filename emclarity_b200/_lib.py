@@ -101,6 +101,7 @@ SIGNATURES = {
     "emc_average_add": (_i, [_vp, _vp, _i, _pd, _pf, _pf, _pi, _vp, _i, _pi, _pi, _vp]),
     "emc_average_result": (_i, [_vp, _i, _vp, _vp, C.POINTER(C.c_long), _vp]),
     "emc_average_reset": (_i, [_vp, _vp]),
+    "emc_average_boxes": (_i, [_vp, _pi, _pi]),
     "emc_average_destroy": (_i, [_vp]),
 }
 

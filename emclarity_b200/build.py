@@ -61,7 +61,7 @@ def build(verbose=False, extra=()):
 
 MEX_DIR = os.path.join(HERE, "mex")
 MEX_OUT = os.path.join(MEX_DIR, "_shim")
-GATEWAYS = ["mexXform3d_b200", "mexFFT_b200", "mexCTF_b200", "mexSF3D_b200", "mexEmcSearch"]
+GATEWAYS = ["mexXform3d_b200", "mexFFT_b200", "mexCTF_b200", "mexSF3D_b200", "mexEmcSearch", "mexEmcAverage"]
 
 
 def build_mex(verbose=False):

@@ -514,6 +514,13 @@ emc_status emc_average_result(emc_average_t a, int half, float* d_avg, float* d_
   return EMC_OK;
 }
 
+emc_status emc_average_boxes(emc_average_t a, int* n, int* nw) {
+  EMC_CHECK_ARG(a && n && nw, "emc_average_boxes: null argument");
+  *n = a->n;
+  *nw = a->nw;
+  return EMC_OK;
+}
+
 emc_status emc_average_destroy(emc_average_t a) {
   if (!a) return EMC_OK;
   avg_free(a);

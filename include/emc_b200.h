@@ -385,6 +385,8 @@ EMC_API emc_status emc_average_add(emc_average_t a, const float* d_particles, in
 EMC_API emc_status emc_average_result(emc_average_t a, int half, float* d_avg, float* d_wedge_sum,
                                       long* count, void* stream);
 EMC_API emc_status emc_average_reset(emc_average_t a, void* stream);
+/* Particle box and wedge box (0: none) of a handle. */
+EMC_API emc_status emc_average_boxes(emc_average_t a, int* n, int* nw);
 EMC_API emc_status emc_average_destroy(emc_average_t a);
 
 #ifdef __cplusplus

@@ -142,3 +142,35 @@ def test_fft_matches_reference_mexFFT(built_lib, cuda):
     ref(0, torch.zeros(1, device="cuda"), np.int32(2), pf, pi)
     yo = api.FourierTransformer((48, 64, 96)).inv_fft(ours)
     assert (yo - y).abs().max().item() < 1e-5 * y.abs().max().item()
+
+
+def test_mexEmcAverage_gateway(gateways):
+    """create / add / result / free through the gateway give the same half-set averages as the
+    C-ABI (MATLAB layout: particles n x n x n x p, rotations 9 x p, 1-based wedge indices)."""
+    from emclarity_b200 import api, synthetic
+    rng = np.random.default_rng(8)
+    n, p, nw = 32, 6, 24
+    mask = torch.from_numpy(synthetic.soft_sphere_mask(n, 11)).cuda()
+    parts = torch.randn((p, n, n, n), device="cuda")
+    wedges = torch.rand((2, nw, nw, nw), device="cuda")
+    rots = np.array([api.define_matrix(synthetic.random_euler(rng), "inv") for _ in range(p)])
+    shifts = rng.uniform(-1, 1, (p, 3)).astype(np.float32)
+    wts = rng.uniform(0.5, 1, p).astype(np.float32)
+    halves = np.array([1, 2, 1, 2, 2, 1], np.int32)
+    widx = np.array([0, 1, 1, 0, 0, 1], np.int32)
+    sym = api.symmetry_matrices("C2")
+    g = gateways["mexEmcAverage"]
+    symcm = np.stack([m for m in sym], axis=-1)  # 3 x 3 x k, each a MATLAB matrix
+    (h,) = g(1, mask, symcm, np.int32(nw), np.float32(0.01))
+    rots_cm = np.stack([r.flatten(order="F") for r in rots], axis=1)  # 9 x p
+    (kept,) = g(1, h, parts, rots_cm, shifts.T.copy(), wts, halves, wedges, widx + 1)
+    assert kept.reshape(-1).tolist() == [1] * p
+    outs = [g(3, h, np.int32(hf)) for hf in (1, 2)]
+    g(0, h)
+    avg = api.Average(mask, symmetry="C2", wedge_box=nw)
+    avg.add(parts, rots, halves, shifts=shifts, weights=wts, wedges=wedges, wedge_index=widx)
+    for hf, (a, w, c) in zip((1, 2), outs):
+        ra, rw, rc = avg.result(hf)
+        assert int(c.reshape(-1)[0]) == rc == 3
+        assert torch.equal(a, ra) and torch.equal(w, rw)
+    avg.close()
