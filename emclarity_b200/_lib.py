@@ -50,6 +50,14 @@ class CtfParams(C.Structure):
                 ("astig_deg", C.c_float)]
 
 
+class MrcHeader(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("mode", C.c_int),
+                ("mx", C.c_int), ("my", C.c_int), ("mz", C.c_int), ("cell", C.c_float * 3),
+                ("pixel_size", C.c_float * 3), ("dmin", C.c_float), ("dmax", C.c_float), ("dmean", C.c_float),
+                ("rms", C.c_float), ("origin", C.c_float * 3), ("ext_bytes", C.c_int), ("imod_stamp", C.c_int),
+                ("imod_flags", C.c_int), ("data_offset", C.c_long), ("byte_swapped", C.c_int)]
+
+
 _vp, _i, _d, _f = C.c_void_p, C.c_int, C.c_double, C.c_float
 _pd, _pi, _pf = C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_float)
 
@@ -103,6 +111,14 @@ SIGNATURES = {
     "emc_average_reset": (_i, [_vp, _vp]),
     "emc_average_boxes": (_i, [_vp, _pi, _pi]),
     "emc_average_destroy": (_i, [_vp]),
+    "emc_sf3d_particles": (_i, [C.POINTER(C.c_uint), _d, _pd, _i, _i, _pd, _pd, _i, _vp, _vp]),
+    "emc_mrc_read_header": (_i, [C.c_char_p, C.POINTER(MrcHeader)]),
+    "emc_mrc_read": (_i, [C.c_char_p, _pi, _pf]),
+    "emc_mrc_read_device": (_i, [C.c_char_p, _pi, _vp, _vp]),
+    "emc_mrc_write": (_i, [C.c_char_p, _pf, _i, _i, _i, _pf, _pf]),
+    "emc_tlt_read": (_i, [C.c_char_p, _pd, _i, _pi, _pi]),
+    "emc_window_bounds": (_i, [_pi, _pi, _d, _pd, _pi, _pi, _pi, _pd, _pi]),
+    "emc_extract_windows": (_i, [_vp, _i, _i, _i, _pi, _pd, _i, _d, _vp, _pd, _pi, _vp]),
 }
 
 _lib = None

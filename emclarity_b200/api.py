@@ -461,6 +461,112 @@ class Average:
             pass
 
 
+# --------------------------------------------------------------------------- data formats
+def _box(box):
+    if box is None:
+        return None
+    b = np.ascontiguousarray(np.asarray(box, dtype=np.int32).reshape(6))
+    return b
+
+
+def mrc_header(path):
+    """MRCImage header fields (@MRCImage/private/readHeader.m) as a dict."""
+    h = L.MrcHeader()
+    L.call("emc_mrc_read_header", str(path).encode(), C.byref(h))
+    out = {f: getattr(h, f) for f, _ in L.MrcHeader._fields_}
+    for k in ("cell", "pixel_size", "origin"):
+        out[k] = tuple(out[k])
+    return out
+
+
+def mrc_read(path, box=None):
+    """getVolume(MRCImage(path), [x1 x2], [y1 y2], [z1 z2]) as a float32 (nz, ny, nx) numpy array;
+    box = (x1, x2, y1, y2, z1, z2), 1-based inclusive, 0 = whole axis."""
+    h = mrc_header(path)
+    b = _box(box)
+    lo = [(b[2 * d] if b is not None and b[2 * d] else 1) for d in range(3)]
+    hi = [(b[2 * d + 1] if b is not None and b[2 * d + 1] else (h["nx"], h["ny"], h["nz"])[d]) for d in range(3)]
+    out = np.empty((hi[2] - lo[2] + 1, hi[1] - lo[1] + 1, hi[0] - lo[0] + 1), dtype=np.float32)
+    L.call("emc_mrc_read", str(path).encode(), None if b is None else b.ctypes.data_as(C.POINTER(C.c_int)),
+           out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def mrc_read_device(path, box=None, out=None):
+    """The same box read straight into a CUDA tensor (pinned double-buffered staging)."""
+    h = mrc_header(path)
+    b = _box(box)
+    lo = [(b[2 * d] if b is not None and b[2 * d] else 1) for d in range(3)]
+    hi = [(b[2 * d + 1] if b is not None and b[2 * d + 1] else (h["nx"], h["ny"], h["nz"])[d]) for d in range(3)]
+    shape = (hi[2] - lo[2] + 1, hi[1] - lo[1] + 1, hi[0] - lo[0] + 1)
+    if out is None:
+        out = torch.empty(shape, dtype=torch.float32, device="cuda")
+    L.call("emc_mrc_read_device", str(path).encode(), None if b is None else b.ctypes.data_as(C.POINTER(C.c_int)),
+           _need_cuda(out, "out"), _stream())
+    return out
+
+
+def mrc_write(path, vol, pixel_size=1.0, origin=None):
+    """SAVE_IMG for a float32 (nz, ny, nx) volume (mode 2)."""
+    v = np.ascontiguousarray(vol, dtype=np.float32)
+    nz, ny, nx = v.shape
+    px = (C.c_float * 3)(*([float(pixel_size)] * 3 if np.isscalar(pixel_size) else [float(p) for p in pixel_size]))
+    org = None if origin is None else (C.c_float * 3)(*[float(o) for o in origin])
+    L.call("emc_mrc_write", str(path).encode(), v.ctypes.data_as(C.POINTER(C.c_float)), nx, ny, nz, px, org)
+
+
+def tlt_read(path):
+    """A whitespace-separated tilt table (e.g. <tilt>_ctf.tlt) as a (rows, cols) float64 array."""
+    r, c = C.c_int(0), C.c_int(0)
+    L.call("emc_tlt_read", str(path).encode(), None, 0, C.byref(r), C.byref(c))
+    out = np.zeros((r.value, c.value))
+    L.call("emc_tlt_read", str(path).encode(), out.ctypes.data_as(C.POINTER(C.c_double)), r.value, C.byref(r),
+           C.byref(c))
+    return out
+
+
+def window_bounds(volume_size, window_size, mask_radius, center):
+    """BH_isWindowValid: (start0 (x, y, z), pad_low, pad_top, shift, valid)."""
+    vs = (C.c_int * 3)(*[int(v) for v in volume_size])
+    ws = (C.c_int * 3)(*[int(v) for v in window_size])
+    cen = (C.c_double * 3)(*[float(v) for v in center])
+    st, pl, pt = (C.c_int * 3)(), (C.c_int * 3)(), (C.c_int * 3)()
+    sh = (C.c_double * 3)()
+    ok = C.c_int(0)
+    L.call("emc_window_bounds", vs, ws, float(mask_radius), cen, st, pl, pt, sh, C.byref(ok))
+    return tuple(st), tuple(pl), tuple(pt), tuple(sh), bool(ok.value)
+
+
+def extract_windows(volume, window_size, centers, mask_radius):
+    """Windows of a (nz, ny, nx) CUDA volume around 1-based (x, y, z) centres, zero padded:
+    returns (windows [count, wz, wy, wx], fractional shifts [count, 3], valid [count])."""
+    nz, ny, nx = volume.shape
+    ws = (C.c_int * 3)(*[int(v) for v in window_size])
+    cen = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
+    k = cen.shape[0]
+    out = torch.empty((k, int(window_size[2]), int(window_size[1]), int(window_size[0])), dtype=torch.float32,
+                      device="cuda")
+    sh = np.zeros((k, 3))
+    ok = np.zeros(k, dtype=np.int32)
+    L.call("emc_extract_windows", _need_cuda(volume, "volume"), nx, ny, nz, ws,
+           cen.ctypes.data_as(C.POINTER(C.c_double)), k, float(mask_radius), _need_cuda(out, "out"),
+           sh.ctypes.data_as(C.POINTER(C.c_double)), ok.ctypes.data_as(C.POINTER(C.c_int)), _stream())
+    return out, sh, ok.astype(bool)
+
+
+def sf3d_particles(size, sampling, tlt, xyz, recon_geometry):
+    """BH_weightMaskMex for each particle position: (count, nz, ny, nx) CUDA tensor."""
+    t = np.ascontiguousarray(tlt, dtype=np.float64)
+    p = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    rg = np.ascontiguousarray(recon_geometry, dtype=np.float64).reshape(2, 3)
+    sz = (C.c_uint * 3)(*[int(v) for v in size])
+    out = torch.empty((p.shape[0], int(size[2]), int(size[1]), int(size[0])), dtype=torch.float32, device="cuda")
+    L.call("emc_sf3d_particles", sz, float(sampling), t.ctypes.data_as(C.POINTER(C.c_double)), t.shape[0],
+           t.shape[1], p.ctypes.data_as(C.POINTER(C.c_double)), rg.ctypes.data_as(C.POINTER(C.c_double)),
+           p.shape[0], _need_cuda(out, "out"), _stream())
+    return out
+
+
 # --------------------------------------------------------------------------- volume / spectrum operators
 def pad3d(img, pad_low, pad_top, fill=0.0, taper=False):
     """BH_padZeros3d(img, padLow, padTop, 'GPU', 'single'|'singleTaper', fill); pads given (x, y, z)."""

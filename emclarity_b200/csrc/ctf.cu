@@ -188,6 +188,40 @@ static CtfGrid make_grid(int nx, int ny, int half, int squared, int centred, flo
   return g;
 }
 
+// Per-volume minimum (for SF3D - (min(SF3D(:)) - 1e-4), masking/BH_weightMaskMex.m:55).
+__global__ void k_vol_min(const float* __restrict__ v, long n, unsigned* __restrict__ out_key) {
+  __shared__ unsigned red[32];
+  const float* src = v + (long)blockIdx.y * n;
+  unsigned best = 0xffffffffu;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const float x = src[i];
+    // order-preserving key of a float; NaN sorts last
+    const unsigned u = __float_as_uint(x);
+    const unsigned k = (x != x) ? 0xffffffffu : ((u & 0x80000000u) ? ~u : (u | 0x80000000u));
+    best = min(best, k);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = best;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned b = red[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = min(b, red[w]);
+    atomicMin(out_key + blockIdx.y, b);
+  }
+}
+
+__global__ void k_vol_sub_min(float* __restrict__ v, long n, const unsigned* __restrict__ key, float eps) {
+  float* dst = v + (long)blockIdx.y * n;
+  const unsigned k = key[blockIdx.y];
+  const unsigned u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  const float mn = __uint_as_float(u);
+  const float off = mn - eps;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    dst[i] = dst[i] - off;
+}
+
 }  // namespace emc
 
 extern "C" {
@@ -299,6 +333,83 @@ emc_status emc_sf3d(int half, int squared, const unsigned size[3], const float* 
   // host staging vectors must outlive the async copies
   cudaStreamSynchronize(st);
   cudaFreeAsync(buf, st);
+  return rs;
+}
+
+// BH_weightMaskMex(SIZE, SAMPLING, TLT, xyzSubTomo, reconGeometry) for a batch of particles
+// (masking/BH_weightMaskMex.m:1-60), arithmetic in single precision like the reference (TLT is cast to
+// single first, :11).
+emc_status emc_sf3d_particles(const unsigned size[3], double sampling, const double* tlt, int rows, int cols,
+                              const double* xyz, const double recon_geometry[6], int count, float* d_out,
+                              void* stream) {
+  EMC_CHECK_ARG(size && tlt && xyz && recon_geometry && d_out, "emc_sf3d_particles: null argument");
+  EMC_CHECK_ARG(rows > 0 && cols >= 19, "emc_sf3d_particles: tilt table %d x %d (needs 19 columns)", rows, cols);
+  EMC_CHECK_ARG(count >= 0, "emc_sf3d_particles: count %d", count);
+  if (count == 0) return EMC_OK;
+  // sortrows(TLT, 1): stable ascending sort on column 1, then single precision
+  std::vector<int> order(rows);
+  for (int r = 0; r < rows; ++r) order[r] = r;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tlt[(size_t)a * cols] < tlt[(size_t)b * cols]; });
+  auto T = [&](int r, int c) { return (float)tlt[(size_t)order[r] * cols + (c - 1)]; };  // 1-based column
+  const int n = rows;
+  std::vector<float> pix(n), lam(n), cs(n), ac(n), def0(n), ddf(n), dphi(n), tilt(n), expo(n), occ(n);
+  float dose_mean = 0.f;
+  for (int r = 0; r < n; ++r) dose_mean += T(r, 14);
+  dose_mean /= (float)n;
+  std::vector<float> elastic(n);
+  float el_max = 0.f;
+  for (int r = 0; r < n; ++r) {
+    pix[r] = T(r, 16) * (float)sampling * 1e10f;
+    cs[r] = T(r, 17) * 1e3f;
+    lam[r] = T(r, 18) * 1e10f;
+    ac[r] = T(r, 19);
+    def0[r] = -T(r, 15) * 1e10f;
+    ddf[r] = T(r, 12) * 1e10f;
+    dphi[r] = T(r, 13) * 180.0f / 3.14159265358979323846f;
+    tilt[r] = T(r, 4);
+    expo[r] = T(r, 11);
+    // fractionOfElastics = exp(-thickness / (cosd(tilt) * 400)), thickness 75 nm, normalised (:44-46)
+    elastic[r] = expf(-75.0f / (cosf(tilt[r] * 3.14159265358979323846f / 180.0f) * 400.0f));
+    el_max = std::max(el_max, elastic[r]);
+  }
+  for (int r = 0; r < n; ++r) occ[r] = (elastic[r] / el_max) * (T(r, 14) / dose_mean);
+  // originVol = ceil((reconGeometry(1, 1:3) + 1) / 2), reconShift = reconGeometry(2, :) (:17-20)
+  double origin[3], rshift[3];
+  for (int d = 0; d < 3; ++d) {
+    origin[d] = ceil((recon_geometry[d] + 1.0) / 2.0);
+    rshift[d] = recon_geometry[3 + d];
+  }
+  const long nv = (long)size[0] * size[1] * size[2];
+  cudaStream_t st = emc::as_stream(stream);
+  std::vector<float> df1(n), df2(n);
+  for (int p = 0; p < count; ++p) {
+    const double v[3] = {xyz[3 * (size_t)p] - origin[0] + rshift[0], xyz[3 * (size_t)p + 1] - origin[1] + rshift[1],
+                         xyz[3 * (size_t)p + 2] - origin[2] + rshift[2]};
+    for (int r = 0; r < n; ++r) {
+      // rTilt = defineMatrix(tilt, 'TILT', 'forwardVector') = [c 0 s; 0 1 0; -s 0 c]; z of rTilt * v (:27-30)
+      const float a = tilt[r] * (3.14159265358979323846f / 180.0f);
+      const float z = -sinf(a) * (float)v[0] + cosf(a) * (float)v[2];
+      const float d = def0[r] - z * pix[r];
+      df1[r] = d + ddf[r];
+      df2[r] = d - ddf[r];
+    }
+    EMC_TRY(emc_sf3d(0, 1, size, pix.data(), lam.data(), cs.data(), df1.data(), df2.data(), dphi.data(), ac.data(),
+                     (unsigned)n, tilt.data(), expo.data(), occ.data(), d_out + (size_t)p * nv, stream));
+  }
+  // SF3D - (min(SF3D(:)) - 1e-4) (:55)
+  unsigned* keys = nullptr;
+  EMC_CUDA(cudaMallocAsync((void**)&keys, sizeof(unsigned) * count, st));
+  emc_status rs = EMC_OK;
+  if (cudaMemsetAsync(keys, 0xff, sizeof(unsigned) * count, st) != cudaSuccess) rs = EMC_E_CUDA;
+  const int gx = (int)std::max<long>(1, std::min<long>((nv + 255) / 256, 64));
+  for (int p0 = 0; p0 < count && rs == EMC_OK; p0 += 65535) {
+    const int cnt = std::min(65535, count - p0);
+    emc::k_vol_min<<<dim3(gx, cnt), 256, 0, st>>>(d_out + (size_t)p0 * nv, nv, keys + p0);
+    emc::k_vol_sub_min<<<dim3(gx, cnt), 256, 0, st>>>(d_out + (size_t)p0 * nv, nv, keys + p0, 1e-4f);
+    if (cudaGetLastError() != cudaSuccess) rs = EMC_E_CUDA;
+  }
+  if (rs == EMC_E_CUDA) emc::set_error("emc_sf3d_particles: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaFreeAsync(keys, st);
   return rs;
 }
 

@@ -389,6 +389,65 @@ EMC_API emc_status emc_average_reset(emc_average_t a, void* stream);
 EMC_API emc_status emc_average_boxes(emc_average_t a, int* n, int* nw);
 EMC_API emc_status emc_average_destroy(emc_average_t a);
 
+/* BH_weightMaskMex(SIZE, SAMPLING, TLT, xyzSubTomo, reconGeometry) (masking/BH_weightMaskMex.m:1-60)
+ * for count particles: the tilt table (rows x cols, row-major as emc_tlt_read; columns as
+ * :16-30) is sorted on column 1 and cast to single; each particle's defocus is offset by the
+ * height of its position along every tilt's beam; the volumes come from emc_sf3d (full grid, CTF
+ * squared) and are shifted by -(min - 1e-4).  xyz: [count][3]; recon_geometry: the 2 x 3
+ * reconGeometry, row-major (size, then shift); d_out: [count][size^3]. */
+EMC_API emc_status emc_sf3d_particles(const unsigned size[3], double sampling, const double* tlt, int rows,
+                                      int cols, const double* xyz, const double recon_geometry[6], int count,
+                                      float* d_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Data formats either side of the path: MRC volumes, tilt tables, windows   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int nx, ny, nz, mode;      /* mode 0 (int8), 1 (int16), 2 (float32), 6 (uint16) are read */
+  int mx, my, mz;            /* sampling (cell divisions) */
+  float cell[3];             /* cell dimensions, Angstrom */
+  float pixel_size[3];       /* cell / m */
+  float dmin, dmax, dmean, rms;
+  float origin[3];
+  int ext_bytes;             /* extended header bytes */
+  int imod_stamp, imod_flags;
+  long data_offset;          /* 1024 + ext_bytes */
+  int byte_swapped;          /* 1 when the file has the other byte order */
+} emc_mrc_header;
+
+/* The header words MRCImage reads (@MRCImage/private/readHeader.m:1-176), with its byte-order
+ * detection (a negative or > 65535 size means the file is byte-swapped). */
+EMC_API emc_status emc_mrc_read_header(const char* path, emc_mrc_header* out);
+/* getVolume(mrc, [x1 x2], [y1 y2], [z1 z2]) (@MRCImage/getVolume.m:150-298): box = {x1, x2, y1,
+ * y2, z1, z2}, 1-based inclusive, zeros (or box NULL) for a whole axis; converted to float (mode 0
+ * read as signed int8, as getVolume does).  h_out: (x2-x1+1)(y2-y1+1)(z2-z1+1) floats, x fastest. */
+EMC_API emc_status emc_mrc_read(const char* path, const int* box, float* h_out);
+/* Same box straight into device memory: sections stream through two pinned staging buffers and are
+ * converted to float on the GPU while the next block is read.  Synchronises the stream. */
+EMC_API emc_status emc_mrc_read_device(const char* path, const int* box, float* d_out, void* stream);
+/* SAVE_IMG(vol, name, pixelSize[, origin]) for float32 volumes (@MRCImage/SAVE_IMG.m): mode 2, cell =
+ * n * pixel size, min / max / mean and the std(std(std(vol))) rms of SAVE_IMG in the header. */
+EMC_API emc_status emc_mrc_write(const char* path, const float* h_vol, int nx, int ny, int nz,
+                                 const float pixel_size[3], const float origin[3]);
+/* A whitespace-separated numeric table such as <tilt>_ctf.tlt (columns per
+ * masking/BH_weightMaskMex.m:16-30); out (may be NULL): rows x cols doubles, row-major. */
+EMC_API emc_status emc_tlt_read(const char* path, double* out, int max_rows, int* rows, int* cols);
+/* BH_isWindowValid(volumeSize, windowSize, maskRadius, center) (logicals/BH_isWindowValid.m):
+ * start = 0-based volume index of window voxel 0 (the window holds vol(start + i), zero outside),
+ * pad_low / pad_top = the zero padding, shift = center - floor(center), valid = 0 for 'noUse'
+ * (available extent < 2 (maskRadius + 6) - 2 on some axis).  Output pointers may be NULL. */
+EMC_API emc_status emc_window_bounds(const int volume_size[3], const int window_size[3], double mask_radius,
+                                     const double center[3], int start[3], int pad_low[3], int pad_top[3],
+                                     double shift[3], int* valid);
+/* Extracts count windows (BH_average3d.m:1304-1341: crop + BH_padZeros3d with zeros) from a device
+ * volume nx*ny*nz in one launch: d_out [count][wz][wy][wx]; centers [count][3] in the reference's
+ * 1-based volume coordinates; shifts [count][3] and valid [count] (host, may be NULL) as
+ * emc_window_bounds. */
+EMC_API emc_status emc_extract_windows(const float* d_vol, int nx, int ny, int nz, const int window_size[3],
+                                       const double* centers, int count, double mask_radius, float* d_out,
+                                       double* shifts, int* valid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

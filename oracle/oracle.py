@@ -432,3 +432,116 @@ def average_np(particles, mask, rotations, halves, shifts=None, weights=None, we
         avg = sums[h] / counts[h] if counts[h] else np.full((n,) * 3, np.nan)
         out[h] = (avg, wsums[h] if nw else None, counts[h])
     return out, kept
+
+
+# ------------------------------------------------------------------ data formats
+_MRC_DTYPES = {0: "i1", 1: "i2", 2: "f4", 6: "u2"}
+
+
+def mrc_write_np(path, vol, mode=2, big_endian=False, ext_bytes=0, pixel=1.0):
+    """Writes an MRC file with numpy (any of the modes getVolume reads), for tests; header words at
+    the offsets @MRCImage/private/readHeader.m reads them."""
+    e = ">" if big_endian else "<"
+    v = np.asarray(vol)
+    nz, ny, nx = v.shape
+    hdr = bytearray(1024)
+    import struct
+    struct.pack_into(e + "10i", hdr, 0, nx, ny, nz, mode, 0, 0, 0, nx, ny, nz)
+    struct.pack_into(e + "6f", hdr, 40, nx * pixel, ny * pixel, nz * pixel, 90, 90, 90)
+    struct.pack_into(e + "3i", hdr, 64, 1, 2, 3)
+    struct.pack_into(e + "3f", hdr, 76, float(v.min()), float(v.max()), float(v.mean()))
+    struct.pack_into(e + "i", hdr, 92, ext_bytes)
+    hdr[208:212] = b"MAP "
+    with open(path, "wb") as f:
+        f.write(bytes(hdr))
+        f.write(b"\0" * ext_bytes)
+        f.write(np.ascontiguousarray(v, dtype=e + _MRC_DTYPES[mode]).tobytes())
+
+
+def mrc_read_np(path, box=None):
+    """Restatement of getVolume (@MRCImage/getVolume.m:150-298) with readHeader's byte-order test
+    (@MRCImage/private/readHeader.m:18-40) and data offset 1024 + extended bytes (:176)."""
+    import struct
+    raw = open(path, "rb").read()
+    e = "<"
+    nx, ny, nz = struct.unpack_from("<3i", raw, 0)
+    if nx < 0 or ny < 0 or nz < 0 or (nx > 65535 and ny > 65535 and nz > 65535):
+        e = ">"
+        nx, ny, nz = struct.unpack_from(">3i", raw, 0)
+    mode = struct.unpack_from(e + "i", raw, 12)[0]
+    ext = struct.unpack_from(e + "i", raw, 92)[0]
+    data = np.frombuffer(raw, dtype=e + _MRC_DTYPES[mode], count=nx * ny * nz, offset=1024 + ext)
+    v = data.reshape(nz, ny, nx).astype(np.float32)
+    if box is not None:
+        x1, x2, y1, y2, z1, z2 = [int(b) for b in box]
+        x1, y1, z1 = x1 or 1, y1 or 1, z1 or 1
+        x2, y2, z2 = x2 or nx, y2 or ny, z2 or nz
+        v = v[z1 - 1:z2, y1 - 1:y2, x1 - 1:x2]
+    return v
+
+
+def window_bounds_np(volume_size, window_size, mask_radius, center):
+    """BH_isWindowValid (logicals/BH_isWindowValid.m): 0-based start of the window, pads, shift, valid."""
+    vs, ws = np.asarray(volume_size, float), np.asarray(window_size, float)
+    min_size = (mask_radius + 6) * 2
+    win_low = np.ceil((ws - 1) / 2)
+    win_top = win_low - np.mod(ws - 1, 2)
+    c = np.floor(center)
+    low = c - win_low
+    top = vs - (c + win_top)
+    pad_low = (np.abs(low) + 1) * (low <= 0)
+    pad_top = np.abs(top) * (top <= 0)
+    valid = not np.any(ws - pad_low - pad_top - min_size < -2)
+    return (low - 1).astype(int), pad_low.astype(int), pad_top.astype(int), np.asarray(center) - c, valid
+
+
+def extract_window_np(vol, window_size, center, mask_radius):
+    """Crop [LOW, TOP] of BH_isWindowValid and BH_padZeros3d with zeros (BH_average3d.m:1304-1341)."""
+    nz, ny, nx = vol.shape
+    start, pl, pt, sh, ok = window_bounds_np((nx, ny, nz), window_size, mask_radius, center)
+    wx, wy, wz = window_size
+    out = np.zeros((wz, wy, wx), dtype=vol.dtype)
+    for k in range(wz):
+        z = start[2] + k
+        if not 0 <= z < nz:
+            continue
+        for j in range(wy):
+            y = start[1] + j
+            if not 0 <= y < ny:
+                continue
+            x0, x1 = max(0, start[0]), min(nx, start[0] + wx)
+            if x1 > x0:
+                out[k, j, x0 - start[0]:x1 - start[0]] = vol[z, y, x0:x1]
+    return out, sh, ok
+
+
+def sf3d_particles_np(size, sampling, tlt, xyz, recon_geometry):
+    """BH_weightMaskMex (masking/BH_weightMaskMex.m:1-60) restated: single-precision host arithmetic,
+    the SF3D volume from the C oracle of mexSF3D, then SF3D - (min - 1e-4)."""
+    order = np.argsort(np.asarray(tlt)[:, 0], kind="stable")
+    T = np.asarray(tlt)[order].astype(np.float32)
+    f = np.float32
+    pix = T[:, 15] * f(sampling) * f(1e10)
+    cs = T[:, 16] * f(1e3)
+    lam = T[:, 17] * f(1e10)
+    ac = T[:, 18]
+    def0 = -T[:, 14] * f(1e10)
+    ddf = T[:, 11] * f(1e10)
+    dphi = T[:, 12] * f(180.0) / f(np.pi)
+    tilt = T[:, 3]
+    expo = T[:, 10]
+    dose = T[:, 13] / np.mean(T[:, 13], dtype=np.float32)
+    el = np.exp(f(-75.0) / (np.cos(tilt * f(np.pi / 180)) * f(400.0)))
+    el = el / el.max()
+    occ = el * dose
+    rg = np.asarray(recon_geometry, dtype=np.float64).reshape(2, 3)
+    origin = np.ceil((rg[0] + 1) / 2)
+    out = []
+    for p in np.asarray(xyz, dtype=np.float64).reshape(-1, 3):
+        v = p - origin + rg[1]
+        a = tilt * f(np.pi / 180)
+        z = -np.sin(a) * f(v[0]) + np.cos(a) * f(v[2])
+        d = def0 - z * pix
+        vol = sf3d(size, pix, lam, cs, d + ddf, d - ddf, dphi, ac, tilt, expo, occ, squared=True)
+        out.append(vol - (vol.min() - 1e-4))
+    return np.array(out)
