@@ -610,6 +610,89 @@ def run_average(args):
                              "sample": "%d particles through the FP64 restatement (C rotation, numpy sums)" % k}}
 
 
+def run_formats(args):
+    """The data paths either side of the search: a 512x512x256 float32 tomogram (256 MiB) read from an
+    MRC file into HBM, 2,000 64^3 windows extracted from it (BH_isWindowValid + zero padding), and
+    per-particle SF3D weights (BH_weightMaskMex, 41 tilts, 64^3) for 64 positions."""
+    import tempfile
+
+    import torch
+
+    from emclarity_b200 import api
+    from oracle import oracle as O
+    rng = np.random.default_rng(21)
+    nz, ny, nx = 256, 512, 512
+    tomo_h = rng.standard_normal((nz, ny, nx), dtype=np.float32)
+    tmpdir = tempfile.mkdtemp(prefix="emc_bench_")
+    path = os.path.join(tmpdir, "tomo.mrc")
+    api.mrc_write(path, tomo_h, pixel_size=2.17)
+    d_tomo = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda")
+    for _ in range(2):
+        api.mrc_read_device(path, out=d_tomo)  # the file is in the page cache after the first read
+    reps = max(3, args.steps)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    for _ in range(reps):
+        api.mrc_read_device(path, out=d_tomo)
+    torch.cuda.synchronize()
+    read_s = (time.time() - t0) / reps
+    t0 = time.time()
+    O.mrc_read_np(path)
+    read_cpu_s = time.time() - t0
+    # window extraction
+    k, w = 2000, 64
+    centers = np.stack([rng.uniform(1, nx, k), rng.uniform(1, ny, k), rng.uniform(1, nz, k)], axis=1)
+    api.extract_windows(d_tomo, (w, w, w), centers[:8], 20.0)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        out, _, _ = api.extract_windows(d_tomo, (w, w, w), centers, 20.0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ext_ms = e0.elapsed_time(e1) / reps
+    del out
+    t0 = time.time()
+    for c in centers[:20]:
+        O.extract_window_np(tomo_h, (w, w, w), c, 20.0)
+    ext_cpu = 20 / (time.time() - t0)
+    # per-particle SF3D weights
+    nt = 41
+    t = np.zeros((nt, 22))
+    t[:, 0] = np.arange(nt) + 1
+    t[:, 3] = np.linspace(-60, 60, nt)
+    t[:, 10] = np.linspace(0, 120, nt)
+    t[:, 11], t[:, 12], t[:, 13] = 4.1e-8, -1.05, 1.0
+    t[:, 14], t[:, 15], t[:, 16], t[:, 17], t[:, 18] = -3e-6, 2.17e-10, 2.7e-3, 1.968697e-12, 0.085
+    xyz = np.stack([rng.uniform(1, 512, 64), rng.uniform(1, 512, 64), rng.uniform(1, 256, 64)], axis=1)
+    rg = np.array([[512, 512, 256], [0.0, 0.0, 0.0]])
+    api.sf3d_particles((64, 64, 64), 1.0, t, xyz[:2], rg)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    api.sf3d_particles((64, 64, 64), 1.0, t, xyz, rg)
+    torch.cuda.synchronize()
+    sf_s = time.time() - t0
+    t0 = time.time()
+    O.sf3d_particles_np((64, 64, 64), 1.0, t, xyz[:2], rg)
+    sf_cpu = 2 / (time.time() - t0)
+    os.remove(path)
+    os.rmdir(tmpdir)
+    pk, which = measured_peaks()
+    ext_bytes = 2 * 4 * w ** 3 * k  # read + write of every window
+    return {"metric": "windows/s extracted (64^3 from a 512x512x256 tomogram in HBM)", "value": k / (ext_ms / 1e3),
+            "unit": "windows/s", "n_gpus": 1, "steps": reps, "ms_per_step": ext_ms, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "MRC read 512x512x256 float32 to HBM, 2,000 64^3 windows, 64 SF3D weights"},
+            "roofline": {"bound": "hbm", "achieved": ext_bytes / (ext_ms / 1e3) / 1e9, "peak": pk, "unit": "GB/s",
+                         "frac": ext_bytes / (ext_ms / 1e3) / 1e9 / pk, "peak_source": which},
+            "mrc_read_device": {"gb_per_s": tomo_h.nbytes / read_s / 1e9, "ms": read_s * 1e3,
+                                "cpu_numpy_gb_per_s": tomo_h.nbytes / read_cpu_s / 1e9,
+                                "note": "file in the page cache; bound by the host read + PCIe"},
+            "sf3d_particles": {"value": 64 / sf_s, "unit": "particles/s", "cpu_restatement": sf_cpu},
+            "cpu_baseline": {"value": ext_cpu, "unit": "windows/s", "cores": 1, "kind": "port",
+                             "sample": "20 windows through the numpy restatement"}}
+
+
 def _rodrigues(axis, deg):
     a = np.asarray(axis, dtype=np.float64)
     a = a / np.linalg.norm(a)
@@ -717,13 +800,13 @@ def main():
     ap.add_argument("--particles", type=int, default=1200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--planes", type=int, default=0, help="pass-A z-planes per CTA (0: timed choice)")
-    ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine", "average"])
+    ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine", "average", "formats"])
     args = ap.parse_args()
     if args.impl == "ours" and args.workload != "batched64":
         import torch
         torch.cuda.set_device(0)
         fn = {"mixed": run_mixed, "bf16": lambda a: run_mixed(a, "bf16"), "tsearch": run_tsearch,
-              "refine": run_refine, "average": run_average}[args.workload]
+              "refine": run_refine, "average": run_average, "formats": run_formats}[args.workload]
         print(json.dumps(fn(args)))
         return
     if args.impl == "reference":

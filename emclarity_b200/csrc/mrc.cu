@@ -241,18 +241,27 @@ struct WindowArgs {
 
 // out[p][k][j][i] = vol(start + (i, j, k)) inside the volume, 0 outside (BH_isWindowValid +
 // BH_padZeros3d with a zero fill).  start: 0-based volume index of window voxel 0, per window.
-__global__ void k_extract(const float* __restrict__ vol, WindowArgs a, const int* __restrict__ start,
-                          float* __restrict__ out) {
+// One warp per window row: the row's source segment is contiguous, so loads and stores coalesce
+// and no per-element index division is needed.
+__global__ void __launch_bounds__(256) k_extract(const float* __restrict__ vol, WindowArgs a,
+                                                 const int* __restrict__ start, float* __restrict__ out) {
   const int p = blockIdx.y;
-  const long nw = (long)a.w[0] * a.w[1] * a.w[2];
   const int sx = start[3 * p], sy = start[3 * p + 1], sz = start[3 * p + 2];
-  float* dst = out + (long)p * nw;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nw; i += (long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % a.w[0]), y = (int)((i / a.w[0]) % a.w[1]), z = (int)(i / ((long)a.w[0] * a.w[1]));
-    const long gx = sx + x, gy = sy + y, gz = sz + z;
-    dst[i] = (gx >= 0 && gy >= 0 && gz >= 0 && gx < a.vx && gy < a.vy && gz < a.vz)
-                 ? __ldg(vol + (gz * a.vy + gy) * a.vx + gx)
-                 : 0.f;
+  const long nrows = (long)a.w[1] * a.w[2];
+  float* dst = out + (long)p * nrows * a.w[0];
+  const int lane = threadIdx.x & 31;
+  const long warp = blockIdx.x * (long)(blockDim.x >> 5) + (threadIdx.x >> 5);
+  const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
+  // the valid x range of every row of this window
+  const long x_top = a.vx - sx;
+  const int x_lo = sx < 0 ? -sx : 0, x_hi = x_top < a.w[0] ? (int)x_top : a.w[0];
+  for (long row = warp; row < nrows; row += nwarps) {
+    const int j = (int)(row % a.w[1]), k = (int)(row / a.w[1]);
+    const long gy = sy + j, gz = sz + k;
+    float* d = dst + row * a.w[0];
+    const bool in_yz = gy >= 0 && gz >= 0 && gy < a.vy && gz < a.vz;
+    const long base = (gz * a.vy + gy) * a.vx + sx;  // dereferenced only for in-volume voxels
+    for (int i = lane; i < a.w[0]; i += 32) d[i] = (in_yz && i >= x_lo && i < x_hi) ? __ldg(vol + base + i) : 0.f;
   }
 }
 
@@ -542,7 +551,8 @@ emc_status emc_extract_windows(const float* d_vol, int nx, int ny, int nz, const
     a.vz = nz;
     for (int d = 0; d < 3; ++d) a.w[d] = window_size[d];
     const long nw = (long)window_size[0] * window_size[1] * window_size[2];
-    const int gx = (int)std::max<long>(1, std::min<long>((nw + 1023) / 1024, 256));
+    const long nrows = (long)window_size[1] * window_size[2];
+    const int gx = (int)std::max<long>(1, std::min<long>((nrows + 7) / 8, 64));  // 8 warps (rows) per block
     for (int p0 = 0; p0 < count && rs == EMC_OK; p0 += 65535) {
       const int cnt = std::min(65535, count - p0);
       emc::k_extract<<<dim3(gx, cnt), 256, 0, st>>>(d_vol, a, d_start + 3 * (size_t)p0, d_out + (size_t)p0 * nw);
