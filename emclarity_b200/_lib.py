@@ -104,6 +104,9 @@ SIGNATURES = {
     "emc_tsearch_create": (_i, [_vp, _i, _i, _i, C.POINTER(_vp), _vp]),
     "emc_tsearch_run": (_i, [_vp, _vp, _i, _pd, _i, _vp, _vp, _vp]),
     "emc_tsearch_destroy": (_i, [_vp]),
+    "emc_tsearch_peaks": (_i, [_vp, _vp, _i, _i, _i, _pf, _i, _f, _pd, _i, _i, _i, _f, _f, _pd, _pi, _vp]),
+    "emc_moving_average": (_i, [_vp, _i, _i, _i, _i, _vp, _vp]),
+    "emc_local_normalize": (_i, [_vp, _i, _i, _i, _i, _vp]),
     "emc_symmetry_matrices": (_i, [C.c_char_p, _pd, _pi]),
     "emc_average_create": (_i, [_i, _vp, _f, _i, _pd, _i, _i, C.POINTER(_vp), _vp]),
     "emc_average_add": (_i, [_vp, _vp, _i, _pd, _pf, _pf, _pi, _vp, _i, _pi, _pi, _vp]),

@@ -388,6 +388,39 @@ class TemplateSearch:
             pass
 
 
+def tsearch_peaks(mag, ang, removal_mask, rm_dim, angle_list, max_peaks, max_tries=10000, high_thr=0.0,
+                  sampling=1.0, mask_cutoff=0.98):
+    """Greedy peak picking of BH_templateSearch3d_2 (nPeaks = 1) on CUDA maps (mag is modified);
+    returns the (k, 10) rows (x, y, z, e1, e2, e3, 0, 0, 0, score)."""
+    nz, ny, nx = mag.shape
+    rm = np.ascontiguousarray(removal_mask, dtype=np.float32)
+    al = np.ascontiguousarray(angle_list, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((max(1, int(max_peaks)), 10))
+    nf = C.c_int(0)
+    L.call("emc_tsearch_peaks", _need_cuda(mag, "mag"), _need_cuda(ang, "ang"), nx, ny, nz,
+           rm.ctypes.data_as(C.POINTER(C.c_float)), int(rm_dim), float(mask_cutoff),
+           al.ctypes.data_as(C.POINTER(C.c_double)), al.shape[0], int(max_peaks), int(max_tries), float(high_thr),
+           float(sampling), out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(nf), _stream())
+    return out[:nf.value]
+
+
+def moving_average(vol, feature_size, out=None):
+    """BH_movingAverage_2(vol, featureSize) on a CUDA volume."""
+    nz, ny, nx = vol.shape
+    if out is None:
+        out = torch.empty_like(vol)
+    L.call("emc_moving_average", _need_cuda(vol, "vol"), nx, ny, nz, int(feature_size), _need_cuda(out, "out"),
+           _stream())
+    return out
+
+
+def local_normalize(vol, feature_size):
+    """In place (x - avg) / sqrt(avg(x^2) - avg^2) (BH_templateSearch3d_2.m:558-561)."""
+    nz, ny, nx = vol.shape
+    L.call("emc_local_normalize", _need_cuda(vol, "vol"), nx, ny, nz, int(feature_size), _stream())
+    return vol
+
+
 # --------------------------------------------------------------------------- averaging
 def symmetry_matrices(symmetry):
     """The operators interpolator applies for 'C<n>', 'D<n>' or 'O' as (k, 3, 3) float64 arrays

@@ -344,6 +344,30 @@ EMC_API emc_status emc_tsearch_run(emc_tsearch_t h, const float* d_template, int
                            float* d_peak, float* d_angle, void* stream);
 EMC_API emc_status emc_tsearch_destroy(emc_tsearch_t h);
 
+/* Template-search post-processing (BH_templateSearch3d_2.m:1100-1275, nPeaks = 1): greedy peak
+ * picking on the (padded) score map d_mag (modified in place) with the angle-index map d_ang
+ * (1-based indices into angle_list, <= 0 = none).  Repeats, while fewer than max_peaks peaks are
+ * recorded, fewer than max_tries iterations were made and the map maximum exceeds high_thr:
+ * take the first maximum; if its angle index is > 0, record
+ * sampling * (c + centre of mass of the 3^3 box - rm_dim) (c 1-based), the angle_list row and the
+ * maximum, and zero the (2 rm_dim + 1)^3 box where the removal mask (h_removal, that size, host),
+ * rotated by the row's angles (defineMatrix(row, 'Bah', 'forward'), zero border), is >= mask_cutoff;
+ * otherwise zero that voxel.  angle_list: n_angles x 3 (the [phi, theta, psi - phi] rows of
+ * ANGLE_LIST).  h_peaks: max_peaks x 10 doubles (x, y, z, e1, e2, e3, 0, 0, 0, score), *n_found
+ * rows filled (the reference then keeps rows with x > 0). */
+EMC_API emc_status emc_tsearch_peaks(float* d_mag, const float* d_ang, int nx, int ny, int nz,
+                                     const float* h_removal, int rm_dim, float mask_cutoff,
+                                     const double* angle_list, int n_angles, int max_peaks, int max_tries,
+                                     float high_thr, float sampling, double* h_peaks, int* n_found,
+                                     void* stream);
+/* BH_movingAverage_2(img, featureSize) (statistics/BH_movingAverage_2.m): separable Gaussian
+ * moving average (length featureSize, sigma 3, symmetric boundaries). */
+EMC_API emc_status emc_moving_average(const float* d_in, int nx, int ny, int nz, int feature_size,
+                                      float* d_out, void* stream);
+/* The local normalisation of BH_templateSearch3d_2.m:558-561, in place:
+ * x <- (x - avg(x)) / sqrt(avg(x^2) - avg(x)^2) with avg = emc_moving_average. */
+EMC_API emc_status emc_local_normalize(float* d_vol, int nx, int ny, int nz, int feature_size, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Subtomogram averaging (transformations/BH_average3d.m:1207-1500)           */
 /* ------------------------------------------------------------------------ */

@@ -545,3 +545,76 @@ def sf3d_particles_np(size, sampling, tlt, xyz, recon_geometry):
         vol = sf3d(size, pix, lam, cs, d + ddf, d - ddf, dphi, ac, tilt, expo, occ, squared=True)
         out.append(vol - (vol.min() - 1e-4))
     return np.array(out)
+
+
+# ------------------------------------------------------------------ template-search pre / post
+def moving_average_np(img, feature_size):
+    """BH_movingAverage_2 (statistics/BH_movingAverage_2.m): padarray(img, ceil(L/2), 'both', 'symmetric'),
+    separable convn(..., 'same') with the EMC_gaussianKernel([1, L], 3) row kernel along x, y, z, crop."""
+    L = int(feature_size)
+    t = np.arange(L) - (L - 1) / 2.0
+    w = np.exp(-0.5 * (t / 3.0) ** 2)
+    w /= w.sum()
+    p = int(np.ceil(L / 2))
+    v = np.pad(np.asarray(img, dtype=np.float64), p, mode="symmetric")
+    h = L // 2
+    for axis in (2, 1, 0):  # x, y, z of a (z, y, x) array
+        full = np.apply_along_axis(lambda r: np.convolve(r, w, mode="full"), axis, v)
+        idx = [slice(None)] * 3
+        idx[axis] = slice(h, h + v.shape[axis])  # 'same': central part starting at floor(L/2)
+        v = full[tuple(idx)]
+    return v[p:-p, p:-p, p:-p]
+
+
+def local_normalize_np(img, feature_size):
+    """BH_templateSearch3d_2.m:558-561: (x - avg) ./ sqrt(avg(x.^2) - avg.^2)."""
+    x = np.asarray(img, dtype=np.float64)
+    a = moving_average_np(x, feature_size)
+    a2 = moving_average_np(x * x, feature_size)
+    return (x - a) / np.sqrt(a2 - a * a)
+
+
+def tsearch_peaks_np(mag, ang, removal, rm_dim, angle_list, max_peaks, max_tries=10000, high_thr=0.0, sampling=1.0,
+                     mask_cutoff=0.98):
+    """The peak loop of alignment/BH_templateSearch3d_2.m:1100-1275 with nPeaks = 1 (FP64 restatement)."""
+    mag = np.array(mag, dtype=np.float64)
+    ang = np.asarray(ang)
+    nz, ny, nx = mag.shape
+    peaks = []
+    tries = 0
+    while len(peaks) < max_peaks and tries < max_tries:
+        flat = mag.ravel()
+        if np.all(np.isnan(flat)):
+            break
+        coord = int(np.nanargmax(flat))
+        mx = flat[coord]
+        if not mx > high_thr:
+            break
+        tries += 1
+        z, y, x = np.unravel_index(coord, mag.shape)
+        a = ang[z, y, x]
+        if a > 0:
+            box = mag[max(0, z - 1):z + 2, max(0, y - 1):y + 2, max(0, x - 1):x + 2]
+            zz, yy, xx = np.meshgrid(np.arange(max(0, z - 1), min(nz, z + 2)) - z,
+                                     np.arange(max(0, y - 1), min(ny, y + 2)) - y,
+                                     np.arange(max(0, x - 1), min(nx, x + 2)) - x, indexing="ij")
+            sw = box.sum()
+            cm = np.array([(box * xx).sum(), (box * yy).sum(), (box * zz).sum()]) / sw
+            e = np.asarray(angle_list[int(a) - 1], dtype=np.float64)
+            row = np.zeros(10)
+            row[0:3] = sampling * (np.array([x + 1, y + 1, z + 1]) + cm - rm_dim)
+            row[3:6] = e
+            row[9] = mx
+            peaks.append(row)
+            R = define_matrix_np(e, "forward")
+            rmask = rotate(removal, R, (0, 0, 0), "forward", interp=2)
+            r = 2 * rm_dim + 1
+            for bz in range(r):
+                for by in range(r):
+                    for bx in range(r):
+                        X, Y, Z = x - rm_dim + bx, y - rm_dim + by, z - rm_dim + bz
+                        if 0 <= X < nx and 0 <= Y < ny and 0 <= Z < nz and not rmask[bz, by, bx] < mask_cutoff:
+                            mag[Z, Y, X] = 0.0
+        else:
+            mag[z, y, x] = 0.0
+    return np.array(peaks).reshape(-1, 10)

@@ -66,3 +66,10 @@ def test_average_restatement_symmetry_is_invariant():
     a, _ = O.average_np([p], m, [np.eye(3)], [1], symmetry=syms)
     b, _ = O.average_np([p], m, [r90], [1], symmetry=syms)
     assert np.allclose(a[1][0], b[1][0], atol=1e-9)
+
+
+def test_moving_average_restatement_basics():
+    """Constant volumes stay constant (the weights sum to one, symmetric borders)."""
+    v = np.full((12, 14, 16), 3.5)
+    assert np.allclose(O.moving_average_np(v, 7), 3.5)
+    assert np.allclose(O.moving_average_np(v, 6), 3.5)
