@@ -249,11 +249,17 @@ __device__ __forceinline__ float2 twiddle(const float2* tw, int m) {
 // Physical slot of line element i.  With PAD, one spare slot follows every 8 elements: the
 // radix-8 first stage writes elements 8j + r, which without the gap would put the 8 lanes of a
 // team on 2 shared-memory banks.  padded_len(L) slots hold a padded line.
+// PAD = 2 leaves the gap after every 16 elements instead, for lines whose first radix is 16
+// (elements 16 j + r).
 template <int PAD>
 __host__ __device__ __forceinline__ constexpr int lpos(int i) {
-  return PAD ? i + (i >> 3) : i;
+  return PAD == 0 ? i : (PAD == 1 ? i + (i >> 3) : i + (i >> 4));
 }
-__host__ __device__ constexpr int padded_len(int L) { return L + L / 8; }
+__host__ __device__ constexpr int padded_len(int L, int pad = 1) {
+  return pad == 0 ? L : (pad == 1 ? L + L / 8 : L + L / 16);
+}
+// The padding that spreads the first stage's writes of a length-L line over the banks.
+__host__ __device__ constexpr int line_pad(int L) { return radix_of(L, 0) >= 16 ? 2 : 1; }
 
 // Per-lane twiddles of stage S (NS = product of the earlier radices), kept in registers.  Lane
 // `lane` of a team always handles butterflies j = lane + b P, whose twiddle exponents depend on

@@ -13,8 +13,11 @@ namespace emc {
 // nrows real rows of length L (pitch in_pitch floats) -> complex rows of length
 // L/2+1 (pitch out_pitch float2).  Two rows share one complex FFT: z = a + i b.
 // Teams per CTA of the row kernels: at most 256 threads and ~32 KB of line buffers.
+// Line buffers hold padded lines (lpos<line_pad(L)>, see fft.cuh) against bank conflicts.
+__host__ __device__ constexpr int row_line_len(int L) { return padded_len(L, line_pad(L)) + 1; }
 __host__ __device__ constexpr int rows_teams(int L, int P) {
-  return (256 / P) < (4096 / (L + 1)) ? (256 / P) : ((4096 / (L + 1)) > 0 ? (4096 / (L + 1)) : 1);
+  return (256 / P) < (4096 / row_line_len(L)) ? (256 / P)
+                                               : ((4096 / row_line_len(L)) > 0 ? (4096 / row_line_len(L)) : 1);
 }
 
 template <int L, int P>
@@ -22,8 +25,9 @@ __global__ void __launch_bounds__(256) k_rows_r2c(const float* __restrict__ in, 
                                                   float2* __restrict__ out, long out_pitch, long nrows,
                                                   const float2* __restrict__ g_tw) {
   constexpr int TEAMS = rows_teams(L, P);
+  constexpr int PAD = line_pad(L);
   __shared__ float2 s_tw[L];
-  __shared__ float2 s_line[TEAMS][L + 1];
+  __shared__ float2 s_line[TEAMS][row_line_len(L)];
   load_twiddles<L>(s_tw, g_tw);
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
@@ -34,18 +38,15 @@ __global__ void __launch_bounds__(256) k_rows_r2c(const float* __restrict__ in, 
     const long ra = 2 * pair, rb = 2 * pair + 1;
     const bool has_b = rb < nrows;
     float2* buf = s_line[team];
-    if (active) {
-      const float* a = in + ra * in_pitch;
-      const float* b = in + rb * in_pitch;
-      for (int n = lane; n < L; n += P) buf[n] = make_float2(__ldg(a + n), has_b ? __ldg(b + n) : 0.f);
-    }
-    __syncwarp();
-    fft_line<L, -1, P>(buf, 1, lane, s_tw, active);
+    const float* a = in + ra * in_pitch;
+    const float* b = in + rb * in_pitch;
+    fft_line_in<L, -1, P, PAD>([&](int n) { return make_float2(__ldg(a + n), has_b ? __ldg(b + n) : 0.f); }, buf,
+                               1, lane, s_tw, active);
     if (active) {
       float2* oa = out + ra * out_pitch;
       float2* ob = out + rb * out_pitch;
       for (int k = lane; k <= L / 2; k += P) {
-        const float2 zk = buf[k], zm = buf[(L - k) % L];
+        const float2 zk = buf[lpos<PAD>(k)], zm = buf[lpos<PAD>((L - k) % L)];
         oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         if (has_b) ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
       }
@@ -63,8 +64,9 @@ __global__ void __launch_bounds__(256) k_rows_c2r(const float2* __restrict__ in,
                                                   float* __restrict__ out, long out_pitch, long nrows,
                                                   const float2* __restrict__ g_tw) {
   constexpr int TEAMS = rows_teams(L, P);
+  constexpr int PAD = line_pad(L);
   __shared__ float2 s_tw[L];
-  __shared__ float2 s_line[TEAMS][L + 1];
+  __shared__ float2 s_line[TEAMS][row_line_len(L)];
   load_twiddles<L>(s_tw, g_tw);
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
@@ -75,26 +77,25 @@ __global__ void __launch_bounds__(256) k_rows_c2r(const float2* __restrict__ in,
     const long ra = 2 * pair, rb = 2 * pair + 1;
     const bool has_b = rb < nrows;
     float2* buf = s_line[team];
-    if (active) {
-      const float2* a = in + ra * in_pitch;
-      const float2* b = in + rb * in_pitch;
-      for (int n = lane; n < L; n += P) {
-        const bool lower = n <= L / 2;
-        const int k = lower ? n : L - n;
-        float2 A = a[k];
-        float2 B = has_b ? b[k] : make_float2(0.f, 0.f);
-        if (k == 0 || 2 * k == L) { A.y = 0.f; B.y = 0.f; }
-        if (!lower) { A.y = -A.y; B.y = -B.y; }
-        buf[n] = make_float2(A.x - B.y, A.y + B.x);
-      }
-    }
-    __syncwarp();
-    fft_line<L, 1, P>(buf, 1, lane, s_tw, active);
+    const float2* a = in + ra * in_pitch;
+    const float2* b = in + rb * in_pitch;
+    // Hermitian extension of rows a and b packed as a + i b
+    fft_line_in<L, 1, P, PAD>(
+        [&](int n) {
+          const bool lower = n <= L / 2;
+          const int k = lower ? n : L - n;
+          float2 A = a[k];
+          float2 B = has_b ? b[k] : make_float2(0.f, 0.f);
+          if (k == 0 || 2 * k == L) { A.y = 0.f; B.y = 0.f; }
+          if (!lower) { A.y = -A.y; B.y = -B.y; }
+          return make_float2(A.x - B.y, A.y + B.x);
+        },
+        buf, 1, lane, s_tw, active);
     if (active) {
       float* oa = out + ra * out_pitch;
       float* ob = out + rb * out_pitch;
       for (int n = lane; n < L; n += P) {
-        const float2 z = buf[n];
+        const float2 z = buf[lpos<PAD>(n)];
         oa[n] = z.x;
         if (has_b) ob[n] = z.y;
       }
@@ -113,8 +114,9 @@ __global__ void __launch_bounds__(P * T) k_cols(const float2* __restrict__ in, f
                                                 const float2* __restrict__ g_tw) {
   extern __shared__ float2 smem[];
   float2* s_tw = smem;
-  float2* tile = smem + L;  // [L][T+1]
+  float2* tile = smem + L;  // [padded L][T+1], element n of line t at lpos<PAD>(n) * TP + t
   constexpr int TP = T + 1;
+  constexpr int PAD = line_pad(L);
   load_twiddles<L>(s_tw, g_tw);
   const long i0 = (long)blockIdx.x * T;
   const int nt = P * T;
@@ -123,16 +125,33 @@ __global__ void __launch_bounds__(P * T) k_cols(const float2* __restrict__ in, f
     const float2* src = in + o * outer_pitch + i0;
     float2* dst = out + o * outer_pitch + i0;
     __syncthreads();
-    for (int idx = threadIdx.x; idx < L * T; idx += nt) {
-      const int n = idx / T, t = idx % T;
-      if (i0 + t < inner) tile[n * TP + t] = src[(long)n * stride + t];
+    {
+      // groups of up to 8 loads in flight before their shared-memory stores
+      constexpr int IT = (L * T + P * T - 1) / (P * T);
+      constexpr int GRP = IT < (L > 256 ? 4 : 8) ? IT : (L > 256 ? 4 : 8);
+#pragma unroll
+      for (int k0 = 0; k0 < IT; k0 += GRP) {
+        float2 v[GRP];
+#pragma unroll
+        for (int k = 0; k < GRP; ++k) {
+          const int idx = threadIdx.x + (k0 + k) * nt;
+          const int n = idx / T, t = idx % T;
+          if (k0 + k < IT && idx < L * T && i0 + t < inner) v[k] = src[(long)n * stride + t];
+        }
+#pragma unroll
+        for (int k = 0; k < GRP; ++k) {
+          const int idx = threadIdx.x + (k0 + k) * nt;
+          const int n = idx / T, t = idx % T;
+          if (k0 + k < IT && idx < L * T && i0 + t < inner) tile[lpos<PAD>(n) * TP + t] = v[k];
+        }
+      }
     }
     __syncthreads();
-    fft_line<L, SIGN, P>(tile + team, TP, lane, s_tw, i0 + team < inner);
+    fft_line<L, SIGN, P, PAD>(tile + team, TP, lane, s_tw, i0 + team < inner);
     __syncthreads();
     for (int idx = threadIdx.x; idx < L * T; idx += nt) {
       const int n = idx / T, t = idx % T;
-      if (i0 + t < inner) dst[(long)n * stride + t] = tile[n * TP + t];
+      if (i0 + t < inner) dst[(long)n * stride + t] = tile[lpos<PAD>(n) * TP + t];
     }
   }
 }
@@ -141,7 +160,7 @@ template <int L>
 struct ColsCfg {
   static constexpr int P = team_size(L);
   static constexpr int T = (512 / P) < 32 ? (512 / P) : 32;
-  static constexpr size_t smem = sizeof(float2) * (L + (size_t)L * (T + 1));
+  static constexpr size_t smem = sizeof(float2) * (L + (size_t)padded_len(L, line_pad(L)) * (T + 1));
 };
 
 // Host launchers (defined in fft_passes.cu); return EMC_OK or an error status.

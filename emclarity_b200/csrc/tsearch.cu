@@ -7,9 +7,16 @@
 //   X   = T .* conj(fftn(g))
 //   cc  = real(ifftn(X)) / std(cc)     std from the spectrum by Parseval, accumulated in FP64
 //   peak(peak < cc) = cc, angle = o
-// The template volume is never materialised at full size: its spectrum is built with a pruned
-// forward transform (rows and planes that are identically zero are skipped), and the MIP update
-// is fused into the last inverse pass.
+// The template volume is never materialised at full size.  Per orientation:
+//   k_ts_rows    samples the rotated template straight into the x transforms of its t x t rows
+//                (two rows per complex FFT), written into a t-plane buffer whose other rows stay 0;
+//   k_cols (y)   the y transforms of those t planes;
+//   k_ts_zfused  per tile of (ky, kx) z-lines: forward z transform of the t non-zero planes
+//                (the rest are zeros), X = T .* conj(G) with the FP64 map statistics, inverse z;
+//   k_cols (y)   inverse y;  k_ts_c2r_mip: C2R along x fused with the std normalisation and the
+//                MIP update.
+// Per orientation this reads the tomogram spectrum once and moves the full-size spectrum through
+// HBM four times (z out, y in / out, x in) instead of the seven passes of an unfused pipeline.
 #include <math.h>
 
 #include <algorithm>
@@ -28,61 +35,145 @@ struct TsGeom {
   float m[9];       // sampling matrix rows
 };
 
-// Rotated template written into the rows it occupies of a real buffer laid out as
-// [t (z) planes][ny][nx] for the z planes pl[2]..pl[2]+t-1 only (rows outside the template's
-// y/x footprint are zero).
-__global__ void k_ts_place(const float* __restrict__ tmpl, const TsGeom g, float* __restrict__ slab) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  const int zl = blockIdx.z;
-  if (x >= g.nx) return;
-  float v = 0.f;
-  const int px = x - g.pl[0], py = y - g.pl[1];
-  if (px >= 0 && px < g.t && py >= 0 && py < g.t) {
-    const int c = g.t / 2;
-    // 'forward' with shift [1,1,1]: u = p - c - 1
-    const float u = (float)(px - c) - 1.f, w1 = (float)(py - c) - 1.f, w2 = (float)(zl - c) - 1.f;
-    const float sx = fmaf(g.m[0], u, fmaf(g.m[1], w1, g.m[2] * w2)) + (float)c;
-    const float sy = fmaf(g.m[3], u, fmaf(g.m[4], w1, g.m[5] * w2)) + (float)c;
-    const float sz = fmaf(g.m[6], u, fmaf(g.m[7], w1, g.m[8] * w2)) + (float)c;
-    v = sample_linear(tmpl, g.t, g.t, g.t, sx, sy, sz);
+// Rotated template sampled into the x transforms of its rows: pair p of the t * ceil(t/2) row
+// pairs is rows (2q, 2q+1) of template plane zl; the line z[n] = a[n] + i b[n] holds the template
+// at x = n - pl[0] (zero outside), and the two half spectra go to rows pl[1] + 2q (+1) of plane zl
+// of ht ([t][ny][nxh]).  Sampling: 'forward' with shift [1,1,1], u = p - c - 1
+// (BH_templateSearch3d_2.m:744), interpn-style trilinear.
+template <int L, int P>
+__global__ void __launch_bounds__(256) k_ts_rows(const float* __restrict__ tmpl, const TsGeom g,
+                                                 float2* __restrict__ ht, const float2* __restrict__ g_tw) {
+  constexpr int TEAMS = rows_teams(L, P);
+  constexpr int PAD = line_pad(L);
+  __shared__ float2 s_tw[L];
+  __shared__ float2 s_line[TEAMS][row_line_len(L)];
+  load_twiddles<L>(s_tw, g_tw);
+  __syncthreads();
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  const int hp = (g.t + 1) / 2;
+  const long npairs = (long)g.t * hp;
+  const int c = g.t / 2;
+  for (long pair0 = (long)blockIdx.x * TEAMS; pair0 < npairs; pair0 += (long)gridDim.x * TEAMS) {
+    const long pair = pair0 + team;
+    const bool active = pair < npairs;
+    const int zl = active ? (int)(pair / hp) : 0, q = active ? (int)(pair % hp) : 0;
+    const int ya = 2 * q, yb = 2 * q + 1;
+    const bool has_b = yb < g.t;
+    float2* buf = s_line[team];
+    if (active) {
+      const float w2 = (float)(zl - c) - 1.f;
+      const float wa = (float)(ya - c) - 1.f, wb = (float)(yb - c) - 1.f;
+      for (int n = lane; n < L; n += P) {
+        const int px = n - g.pl[0];
+        float va = 0.f, vb = 0.f;
+        if (px >= 0 && px < g.t) {
+          const float u = (float)(px - c) - 1.f;
+          {
+            const float sx = fmaf(g.m[0], u, fmaf(g.m[1], wa, g.m[2] * w2)) + (float)c;
+            const float sy = fmaf(g.m[3], u, fmaf(g.m[4], wa, g.m[5] * w2)) + (float)c;
+            const float sz = fmaf(g.m[6], u, fmaf(g.m[7], wa, g.m[8] * w2)) + (float)c;
+            va = sample_linear(tmpl, g.t, g.t, g.t, sx, sy, sz);
+          }
+          if (has_b) {
+            const float sx = fmaf(g.m[0], u, fmaf(g.m[1], wb, g.m[2] * w2)) + (float)c;
+            const float sy = fmaf(g.m[3], u, fmaf(g.m[4], wb, g.m[5] * w2)) + (float)c;
+            const float sz = fmaf(g.m[6], u, fmaf(g.m[7], wb, g.m[8] * w2)) + (float)c;
+            vb = sample_linear(tmpl, g.t, g.t, g.t, sx, sy, sz);
+          }
+        }
+        buf[lpos<PAD>(n)] = make_float2(va, vb);
+      }
+    }
+    __syncwarp();
+    fft_line<L, -1, P, PAD>(buf, 1, lane, s_tw, active);
+    if (active) {
+      float2* oa = ht + ((size_t)zl * g.ny + g.pl[1] + ya) * g.nxh;
+      float2* ob = oa + g.nxh;
+      for (int k = lane; k <= L / 2; k += P) {
+        const float2 zk = buf[lpos<PAD>(k)], zm = buf[lpos<PAD>((L - k) % L)];
+        oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        if (has_b) ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+      }
+    }
+    __syncwarp();
   }
-  slab[((long)zl * g.ny + y) * g.nx + x] = v;
 }
 
-// Expand the t forward-transformed planes (z = pl[2] .. pl[2]+t-1) into the full z extent with
-// zeros elsewhere, so that the z pass can run in place.
-__global__ void k_ts_zero_planes(float2* __restrict__ G, const TsGeom g) {
-  const long plane = (long)g.ny * g.nxh;
-  const long total = plane * g.nz;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int z = (int)(i / plane);
-    if (z < g.pl[2] || z >= g.pl[2] + g.t) G[i] = make_float2(0.f, 0.f);
-  }
-}
-
-// X = T .* conj(G) in place in G; FP64 sums for the map statistics: sum_full |X|^2 and X(0).
-__global__ void k_ts_multiply(const float2* __restrict__ T, float2* __restrict__ G, const TsGeom g,
-                              double* __restrict__ stats) {
+// Per tile of TT consecutive (ky, kx) z-lines: G = FFT_z of the t planes at z = pl[2].. (zeros
+// elsewhere), X = T .* conj(G), inverse FFT_z into s.  stats[0] += sum over the full spectrum of
+// |X|^2 (Hermitian weights), stats[1] = X(0).
+template <int L, int P, int TT>
+__global__ void __launch_bounds__(P * TT) k_ts_zfused(const float2* __restrict__ gt, const float2* __restrict__ T,
+                                                      float2* __restrict__ s, const TsGeom g,
+                                                      double* __restrict__ stats, const float2* __restrict__ g_tw) {
+  extern __shared__ float2 smem[];
+  float2* s_tw = smem;
+  float2* tile = smem + L;  // [padded L][TT+1], element n of line t at lpos<PAD>(n) * TP + t
+  constexpr int TP = TT + 1;
+  constexpr int PAD = line_pad(L);
   __shared__ double red[32];
-  const long total = (long)g.nz * g.ny * g.nxh;
+  load_twiddles<L>(s_tw, g_tw);
+  const long inner = (long)g.ny * g.nxh, stride = inner;
+  const long i0 = (long)blockIdx.x * TT;
+  constexpr int NT = P * TT;
+  constexpr int IT = (L * TT + NT - 1) / NT;
+  {
+    float2 v[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int idx = threadIdx.x + k * NT;
+      const int n = idx / TT, t = idx % TT;
+      const long i = i0 + t;
+      v[k] = make_float2(0.f, 0.f);
+      if (idx < L * TT && i < inner && n >= g.pl[2] && n < g.pl[2] + g.t) v[k] = gt[(long)(n - g.pl[2]) * stride + i];
+    }
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int idx = threadIdx.x + k * NT;
+      if (idx < L * TT) tile[lpos<PAD>(idx / TT) * TP + idx % TT] = v[k];
+    }
+  }
+  // the tomogram spectrum of this tile, fetched while the forward transform runs
+  float2 tv[IT];
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    const int idx = threadIdx.x + k * NT;
+    const int n = idx / TT, t = idx % TT;
+    tv[k] = (idx < L * TT && i0 + t < inner) ? __ldg(T + (long)n * stride + i0 + t) : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  const bool line_active = i0 + team < inner;
+  fft_line<L, -1, P, PAD>(tile + team, TP, lane, s_tw, line_active);
+  __syncthreads();
   double e = 0.0;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const float2 x = cmulc(T[i], G[i]);
-    G[i] = x;
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    const int idx = threadIdx.x + k * NT;
+    const int n = idx / TT, t = idx % TT;
+    const long i = i0 + t;
+    if (idx >= L * TT || i >= inner) continue;
+    const float2 x = cmulc(tv[k], tile[lpos<PAD>(n) * TP + t]);
+    tile[lpos<PAD>(n) * TP + t] = x;
     const int kx = (int)(i % g.nxh);
     e += (kx == 0 || 2 * kx == g.nx ? 1.0 : 2.0) * ((double)x.x * x.x + (double)x.y * x.y);
-    if (i == 0) stats[1] = (double)x.x;
+    if (i == 0 && n == 0) stats[1] = (double)x.x;
   }
-  double v = e;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-    atomicAdd(stats, t);
+    double tot = 0.0;
+    for (int w = 0; w < NT / 32; ++w) tot += red[w];
+    atomicAdd(stats, tot);
+  }
+  fft_line<L, 1, P, PAD>(tile + team, TP, lane, s_tw, line_active);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < L * TT; idx += NT) {
+    const int n = idx / TT, t = idx % TT;
+    const long i = i0 + t;
+    if (i < inner) s[(long)n * stride + i] = tile[lpos<PAD>(n) * TP + t];
   }
 }
 
@@ -93,9 +184,10 @@ __global__ void __launch_bounds__(256) k_ts_c2r_mip(const float2* __restrict__ i
                                                     float* __restrict__ peak, float* __restrict__ angle,
                                                     const float2* __restrict__ g_tw) {
   constexpr int TEAMS = rows_teams(L, P);
+  constexpr int PAD = line_pad(L);
   constexpr int LH = L / 2 + 1;
   __shared__ float2 s_tw[L];
-  __shared__ float2 s_line[TEAMS][L + 1];
+  __shared__ float2 s_line[TEAMS][row_line_len(L)];
   load_twiddles<L>(s_tw, g_tw);
   // map statistics from the spectrum: mean = X(0), sum m^2 = nvox * sum_full |X|^2
   const double mean = stats[1];
@@ -110,31 +202,40 @@ __global__ void __launch_bounds__(256) k_ts_c2r_mip(const float2* __restrict__ i
     const long ra = 2 * pair, rb = 2 * pair + 1;
     const bool has_b = rb < nrows;
     float2* buf = s_line[team];
+    const float2* a = in + ra * LH;
+    const float2* b = in + rb * LH;
+    // Hermitian extension of rows a and b packed as a + i b
+    fft_line_in<L, 1, P, PAD>(
+        [&](int n) {
+          const bool lower = n <= L / 2;
+          const int k = lower ? n : L - n;
+          float2 A = a[k];
+          float2 B = has_b ? b[k] : make_float2(0.f, 0.f);
+          if (k == 0 || 2 * k == L) { A.y = 0.f; B.y = 0.f; }
+          if (!lower) { A.y = -A.y; B.y = -B.y; }
+          return make_float2(A.x - B.y, A.y + B.x);
+        },
+        buf, 1, lane, s_tw, active);
     if (active) {
-      const float2* a = in + ra * LH;
-      const float2* b = in + rb * LH;
-      for (int n = lane; n < L; n += P) {
-        const bool lower = n <= L / 2;
-        const int k = lower ? n : L - n;
-        float2 A = a[k];
-        float2 B = has_b ? b[k] : make_float2(0.f, 0.f);
-        if (k == 0 || 2 * k == L) { A.y = 0.f; B.y = 0.f; }
-        if (!lower) { A.y = -A.y; B.y = -B.y; }
-        buf[n] = make_float2(A.x - B.y, A.y + B.x);
+      // the current maxima of both rows first (all loads in flight), then compare and update
+      constexpr int NE = (L + P - 1) / P;
+      float pa[NE], pb[NE];
+#pragma unroll
+      for (int k = 0; k < NE; ++k) {
+        const int n = lane + k * P;
+        pa[k] = n < L ? peak[ra * L + n] : 0.f;
+        pb[k] = (has_b && n < L) ? peak[rb * L + n] : 0.f;
       }
-    }
-    __syncwarp();
-    fft_line<L, 1, P>(buf, 1, lane, s_tw, active);
-    if (active) {
-      for (int n = lane; n < L; n += P) {
-        const float2 z = buf[n];
-        const long ia = ra * L + n;
+#pragma unroll
+      for (int k = 0; k < NE; ++k) {
+        const int n = lane + k * P;
+        if (n >= L) break;
+        const float2 z = buf[lpos<PAD>(n)];
         const float va = z.x * inv_sd;
-        if (peak[ia] < va) { peak[ia] = va; angle[ia] = angle_id; }
+        if (pa[k] < va) { peak[ra * L + n] = va; angle[ra * L + n] = angle_id; }
         if (has_b) {
-          const long ib = rb * L + n;
           const float vb = z.y * inv_sd;
-          if (peak[ib] < vb) { peak[ib] = vb; angle[ib] = angle_id; }
+          if (pb[k] < vb) { peak[rb * L + n] = vb; angle[rb * L + n] = angle_id; }
         }
       }
     }
@@ -183,6 +284,54 @@ static emc_status c2r_mip_any(int L, const float2* in, long nrows, const double*
   return EMC_E_UNSUPPORTED;
 }
 
+template <int L>
+static emc_status launch_ts_rows(const float* tmpl, const TsGeom& g, float2* ht, cudaStream_t st) {
+  constexpr int P = team_size(L);
+  constexpr int TEAMS = rows_teams(L, P);
+  const float2* tw = device_twiddles(L);
+  if (!tw) return EMC_E_CUDA;
+  const long npairs = (long)g.t * ((g.t + 1) / 2);
+  const int grid = (int)std::max(1L, std::min((npairs + TEAMS - 1) / TEAMS, 8L * device_sm_count()));
+  k_ts_rows<L, P><<<grid, TEAMS * P, 0, st>>>(tmpl, g, ht, tw);
+  EMC_LAUNCH_CHECK();
+  return EMC_OK;
+}
+
+static emc_status ts_rows_any(int L, const float* tmpl, const TsGeom& g, float2* ht, cudaStream_t st) {
+  switch (L) {
+#define X(n) case n: return launch_ts_rows<n>(tmpl, g, ht, st);
+    EMC_FOR_EACH_LENGTH(X)
+#undef X
+  }
+  set_error("template search: edge %d not supported", L);
+  return EMC_E_UNSUPPORTED;
+}
+
+template <int L>
+static emc_status launch_ts_zfused(const float2* gt, const float2* T, float2* s, const TsGeom& g, double* stats,
+                                   cudaStream_t st) {
+  using C = ColsCfg<L>;
+  const float2* tw = device_twiddles(L);
+  if (!tw) return EMC_E_CUDA;
+  auto kern = k_ts_zfused<L, C::P, C::T>;
+  if (C::smem > 48 * 1024) EMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem));
+  const long inner = (long)g.ny * g.nxh;
+  kern<<<(unsigned)((inner + C::T - 1) / C::T), C::P * C::T, C::smem, st>>>(gt, T, s, g, stats, tw);
+  EMC_LAUNCH_CHECK();
+  return EMC_OK;
+}
+
+static emc_status ts_zfused_any(int L, const float2* gt, const float2* T, float2* s, const TsGeom& g, double* stats,
+                                cudaStream_t st) {
+  switch (L) {
+#define X(n) case n: return launch_ts_zfused<n>(gt, T, s, g, stats, st);
+    EMC_FOR_EACH_LENGTH(X)
+#undef X
+  }
+  set_error("template search: edge %d not supported", L);
+  return EMC_E_UNSUPPORTED;
+}
+
 }  // namespace emc
 
 struct emc_tsearch_s {
@@ -190,8 +339,8 @@ struct emc_tsearch_s {
   float2* T = nullptr;      // tomogram spectrum with the phase ramp
   float2* G = nullptr;      // template spectrum / product
   float2* S = nullptr;      // C2R scratch
-  float* slab = nullptr;    // t real planes of the placed template
-  int slab_t = 0;
+  float2* ht = nullptr;     // x transforms of the template rows: [t][ny][nxh], other rows 0
+  int ht_t = 0;
   double* stats = nullptr;  // per orientation: sum |X|^2, X(0)
 };
 
@@ -253,11 +402,14 @@ emc_status emc_tsearch_run(emc_tsearch_t h, const float* d_template, int t, cons
   cudaStream_t st = emc::as_stream(stream);
   const int nx = h->nx, ny = h->ny, nz = h->nz, nxh = nx / 2 + 1;
   const long nvox = (long)nx * ny * nz;
-  if (h->slab_t != t) {
-    if (h->slab) cudaFree(h->slab);
-    h->slab = nullptr;
-    EMC_CUDA(cudaMalloc(&h->slab, sizeof(float) * (size_t)t * ny * nx));
-    h->slab_t = t;
+  if (h->ht_t != t) {
+    if (h->ht) cudaFree(h->ht);
+    h->ht = nullptr;
+    h->ht_t = 0;
+    const size_t bytes = sizeof(float2) * (size_t)t * ny * nxh;
+    EMC_CUDA(cudaMalloc(&h->ht, bytes));
+    EMC_CUDA(cudaMemsetAsync(h->ht, 0, bytes, st));  // rows outside the template stay zero
+    h->ht_t = t;
   }
   emc::TsGeom g;
   g.nx = nx; g.ny = ny; g.nz = nz; g.nxh = nxh; g.t = t;
@@ -273,22 +425,13 @@ emc_status emc_tsearch_run(emc_tsearch_t h, const float* d_template, int t, cons
     EMC_TRY(emc_define_matrix(ang, 0, M));
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) g.m[3 * i + j] = (float)M[i + 3 * j];
-    // 1. rotated template into its t planes
-    emc::k_ts_place<<<dim3((nx + 127) / 128, ny, t), 128, 0, st>>>(d_template, g, h->slab);
-    EMC_LAUNCH_CHECK();
-    // 2. pruned forward transform: x rows and y columns of the t planes, then z over all planes
-    float2* Gp = h->G + (size_t)g.pl[2] * ny * nxh;
-    EMC_TRY(emc::launch_rows_r2c(nx, h->slab, nx, Gp, nxh, (long)t * ny, st));
-    EMC_TRY(emc::launch_cols(ny, -1, Gp, Gp, nxh, nxh, t, (long)ny * nxh, st));
-    emc::k_ts_zero_planes<<<blocks, 256, 0, st>>>(h->G, g);
-    EMC_LAUNCH_CHECK();
-    EMC_TRY(emc::launch_cols(nz, -1, h->G, h->G, (long)ny * nxh, (long)ny * nxh, 1, (long)nz * ny * nxh, st));
-    // 3. X = T conj(G) and its statistics
+    // 1. rotated template sampled into the x transforms of its rows, 2. y transforms of its planes
+    EMC_TRY(emc::ts_rows_any(nx, d_template, g, h->ht, st));
+    EMC_TRY(emc::launch_cols(ny, -1, h->ht, h->G, nxh, nxh, t, (long)ny * nxh, st));
+    // 3. z transform of the t planes, X = T conj(G) and its statistics, inverse z
     EMC_CUDA(cudaMemsetAsync(h->stats, 0, 2 * sizeof(double), st));
-    emc::k_ts_multiply<<<blocks, 256, 0, st>>>(h->T, h->G, g, h->stats);
-    EMC_LAUNCH_CHECK();
-    // 4. inverse z and y, then C2R along x fused with std normalisation and the MIP update
-    EMC_TRY(emc::launch_cols(nz, 1, h->G, h->S, (long)ny * nxh, (long)ny * nxh, 1, (long)nz * ny * nxh, st));
+    EMC_TRY(emc::ts_zfused_any(nz, h->G, h->T, h->S, g, h->stats, st));
+    // 4. inverse y, then C2R along x fused with std normalisation and the MIP update
     EMC_TRY(emc::launch_cols(ny, 1, h->S, h->S, nxh, nxh, nz, (long)ny * nxh, st));
     EMC_TRY(emc::c2r_mip_any(nx, h->S, (long)ny * nz, h->stats, nvox, (float)(o + 1), d_peak, d_angle, st));
   }
@@ -300,7 +443,7 @@ emc_status emc_tsearch_destroy(emc_tsearch_t h) {
   cudaFree(h->T);
   cudaFree(h->G);
   cudaFree(h->S);
-  cudaFree(h->slab);
+  cudaFree(h->ht);
   cudaFree(h->stats);
   delete h;
   return EMC_OK;
