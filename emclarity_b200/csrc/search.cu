@@ -16,40 +16,6 @@
 
 namespace emc {
 
-struct EvalResult {
-  float cc;
-  int peak[3];
-};
-
-// Decodes the per-evaluation keys of one chunk into EvalResult rows and folds each
-// evaluation into its particle's best-orientation key.
-__global__ void k_search_decode(const SearchChunkArgs a, int n, EvalResult* __restrict__ results,
-                                unsigned long long* __restrict__ best_keys) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= a.n_items) return;
-  const EvalItem it = a.items[e];
-  const DevParticle& pt = a.parts[it.particle];
-  const unsigned long long key = a.keys[e];
-  EvalResult r;
-  const int c = n / 2;
-  if (key == 0ull) {
-    r.cc = __int_as_float(0x7fc00000);
-    r.peak[0] = r.peak[1] = r.peak[2] = 0;
-  } else {
-    r.cc = key_to_float((unsigned int)(key >> 32));
-    const unsigned int lin = 0xffffffffu - (unsigned int)(key & 0xffffffffull);
-    r.peak[0] = (int)(lin % n) - c;
-    r.peak[1] = (int)((lin / n) % n) - c;
-    r.peak[2] = (int)(lin / ((unsigned)n * n)) - c;
-  }
-  const long out = pt.eval_base + (it.orient - pt.orient_begin);
-  results[out] = r;
-  if (key != 0ull) {
-    const unsigned long long bk = ((unsigned long long)ordered_key(r.cc) << 32) | (0xffffffffu - (unsigned)it.orient);
-    atomicMax(best_keys + it.particle, bk);
-  }
-}
-
 __global__ void k_search_best(const DevParticle* __restrict__ parts, int np, const EvalResult* __restrict__ results,
                               const unsigned long long* __restrict__ best_keys, emc_search_hit* __restrict__ out) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -306,7 +272,9 @@ struct emc_search_s {
   emc::DevBuf<double> d_dmat;
   int norient = 0;
   int radius = 0, interp = EMC_INTERP_LINEAR, chunk_evals = 0;
-  size_t scratch_budget = 48ull << 20;
+  // S1 + S2 scratch of a chunk, sized to about two thirds of the L2 (86 MB of 126 MB: 64 evaluations at
+  // 64^3, radius 7) so that pass B finds pass A's slabs in L2; set at creation from the device's L2
+  size_t scratch_budget = 86ull << 20;
 
   emc::DevBuf<emc::DevParticle> d_parts;
   emc::DevBuf<emc::EvalItem> d_items;
@@ -315,6 +283,7 @@ struct emc_search_s {
   emc::DevBuf<float2> s1, s2;
   emc::DevBuf<emc::EvalStats> stats;
   emc::DevBuf<unsigned long long> keys;
+  emc::DevBuf<unsigned> done;
 
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -359,6 +328,12 @@ emc_status emc_search_create(emc_search_t* out) {
   EMC_CHECK_ARG(out, "emc_search_create: null argument");
   emc_search_s* s = new (std::nothrow) emc_search_s();
   EMC_CHECK_ARG(s, "emc_search_create: host allocation failed");
+  {
+    int dev = 0, l2 = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) == cudaSuccess &&
+        l2 > 0)
+      s->scratch_budget = (size_t)l2 / 3 * 2;
+  }
   if (cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete s;
     emc::set_error("emc_search_create: stream creation failed");
@@ -466,6 +441,9 @@ static emc::SearchChunkArgs chunk_args(emc_search_t s, const Chunk& c) {
   a.n_items = c.count;
   a.radius = effective_radius(s, c.n);
   a.interp = s->interp;
+  a.done = s->done.p;
+  a.results = s->d_results.p;
+  a.best_keys = s->d_best_keys.p;
   return a;
 }
 
@@ -519,11 +497,13 @@ static emc_status tune_planes(emc_search_t s, const Chunk& c, cudaStream_t st) {
 static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks, int np, long total_evals,
                                 float* d_cc, int* d_peak, emc_search_hit* d_best, cudaStream_t st) {
   EMC_CUDA(cudaMemsetAsync(s->d_best_keys.p, 0, sizeof(unsigned long long) * np, st));
+  // per-evaluation scratch starts clear; the last pass-C CTA of each evaluation clears it again
+  EMC_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(emc::EvalStats) * s->stats.cap, st));
+  EMC_CUDA(cudaMemsetAsync(s->keys.p, 0, sizeof(unsigned long long) * s->keys.cap, st));
+  EMC_CUDA(cudaMemsetAsync(s->done.p, 0, sizeof(unsigned) * s->done.cap, st));
   long launches = 0;
   for (const Chunk& c : chunks) {
     const emc::SearchChunkArgs a = chunk_args(s, c);
-    EMC_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(emc::EvalStats) * c.count, st));
-    EMC_CUDA(cudaMemsetAsync(s->keys.p, 0, sizeof(unsigned long long) * c.count, st));
     cudaEvent_t* ev = nullptr;
     if (s->profiling) {
       const int slot = s->ev_next;
@@ -533,10 +513,8 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
       s->ev_pending[slot] = true;
     }
     EMC_TRY(emc::launch_chunk_any(c.n, c.dtype, planes_slot(s, c.n, c.dtype), a, st, ev));
-    emc::k_search_decode<<<(c.count + 255) / 256, 256, 0, st>>>(a, c.n, s->d_results.p, s->d_best_keys.p);
-    EMC_LAUNCH_CHECK();
-    if (ev) EMC_CUDA(cudaEventRecord(ev[4], st));
-    launches += 4;
+    if (ev) EMC_CUDA(cudaEventRecord(ev[4], st));  // decode runs inside pass C
+    launches += 3;
     if (s->profiling) {
       for (int k = 0; k < 4; ++k) s->prof_launches[k] += 1;
       s->prof_evals += c.count;
@@ -637,6 +615,7 @@ emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, in
   EMC_TRY(s->d_best_keys.reserve(np));
   EMC_TRY(s->stats.reserve(max_chunk));
   EMC_TRY(s->keys.reserve(max_chunk));
+  EMC_TRY(s->done.reserve(max_chunk));
   {
     // split scratch between S1 and S2 proportionally to the largest chunk of each size
     size_t s1n = 0, s2n = 0;
@@ -809,6 +788,7 @@ emc_status emc_search_destroy(emc_search_t s) {
   s->s2.release();
   s->stats.release();
   s->keys.release();
+  s->done.release();
   if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
   delete s;
   return EMC_OK;

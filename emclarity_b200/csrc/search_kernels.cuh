@@ -161,6 +161,12 @@ struct EvalStats {
   double sum_r, sum_r2, energy_spec, pad;
 };
 
+// Result of one evaluation: normalised CC at the peak and the integer shift.
+struct EvalResult {
+  float cc;
+  int peak[3];
+};
+
 struct SearchChunkArgs {
   const EvalItem* items;     // [E]
   const DevParticle* parts;
@@ -173,7 +179,36 @@ struct SearchChunkArgs {
   int n_items;
   int radius;
   int interp;
+  // With `done` set, the last pass-C CTA of an evaluation decodes it into results / best_keys
+  // and clears its stats, key and counter for the next chunk.
+  unsigned* done = nullptr;                  // [E] pass-C CTAs finished
+  EvalResult* results = nullptr;             // [total evaluations of the run]
+  unsigned long long* best_keys = nullptr;   // [particles]
 };
+
+// Decodes evaluation e of a chunk from its peak key and folds it into its particle's
+// best-orientation key (cc, then the first orientation on ties).
+__device__ __forceinline__ void decode_eval(const SearchChunkArgs& a, int n, int e, unsigned long long key) {
+  const EvalItem it = a.items[e];
+  const DevParticle& pt = a.parts[it.particle];
+  EvalResult r;
+  const int c = n / 2;
+  if (key == 0ull) {
+    r.cc = __int_as_float(0x7fc00000);
+    r.peak[0] = r.peak[1] = r.peak[2] = 0;
+  } else {
+    r.cc = key_to_float((unsigned int)(key >> 32));
+    const unsigned int lin = 0xffffffffu - (unsigned int)(key & 0xffffffffull);
+    r.peak[0] = (int)(lin % n) - c;
+    r.peak[1] = (int)((lin / n) % n) - c;
+    r.peak[2] = (int)(lin / ((unsigned)n * n)) - c;
+  }
+  a.results[pt.eval_base + (it.orient - pt.orient_begin)] = r;
+  if (key != 0ull) {
+    const unsigned long long bk = ((unsigned long long)ordered_key(r.cc) << 32) | (0xffffffffu - (unsigned)it.orient);
+    atomicMax(a.best_keys + it.particle, bk);
+  }
+}
 
 // Sampling matrix rows of RotMat' with RotMat = prior * D (FP64 composition).
 __device__ __forceinline__ void compose_sampling_matrix(const double* prior, const double* d, float m[9]) {
@@ -648,6 +683,17 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const S
   if ((threadIdx.x & 31) == 0 && best) atomicMax(&s_best, best);
   __syncthreads();
   if (threadIdx.x == 0 && s_best) atomicMax(&a.keys[e], s_best);
+  if (a.done && threadIdx.x == 0) {
+    // the last CTA of this evaluation (every other one has published its maximum) decodes it
+    __threadfence();
+    if (atomicAdd(&a.done[e], 1u) == (unsigned)(w - 1)) {
+      __threadfence();
+      const unsigned long long key = atomicExch(&a.keys[e], 0ull);
+      decode_eval(a, N, e, key);
+      a.stats[e] = EvalStats{0.0, 0.0, 0.0, 0.0};
+      a.done[e] = 0u;
+    }
+  }
 }
 
 }  // namespace emc

@@ -262,8 +262,10 @@ EMC_API emc_status emc_search_destroy(emc_search_t s);
  * launches eagerly instead of through the graph and brackets each pass launch with CUDA events
  * on the calling stream.  emc_search_timings returns, summed over all runs since the last
  * reset, the device time in ms of pass A (rotate + xy R2C), pass B (z FFT, multiply, inverse z),
- * pass C (inverse xy + peak) and the decode step, their launch counts, and the number of CC
- * evaluations.  launches_last_run: kernels launched by the most recent run. */
+ * pass C (inverse xy + peak, and the decode of each evaluation by its last pass-C CTA) and a
+ * fourth slot (the time between pass C's end and the chunk's end, now only event overhead),
+ * their launch counts, and the number of CC evaluations.  launches_last_run: kernels launched by
+ * the most recent run. */
 EMC_API emc_status emc_search_set_profiling(emc_search_t s, int enable);
 EMC_API emc_status emc_search_timings(emc_search_t s, double ms[4], long launches[4], long* evals,
                                       long* launches_last_run, int reset);
