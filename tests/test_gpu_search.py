@@ -255,3 +255,23 @@ def test_planes_per_cta_options_agree(built_lib, cuda, store):
     s.set_planes(64, 0)
     assert s.planes(64, store)[0] == 0
     s.close()
+
+
+@pytest.mark.parametrize("radius", [12, 15])
+def test_large_peak_radius_matches_oracle(plain_case, radius):
+    """Peak windows up to the largest supported radius (15: 31 rows / 16 row pairs in pass C)."""
+    from emclarity_b200 import api
+    case, g = plain_case
+    grid = case.grid[::20]
+    q, e = api.particle_spectrum(g["particle"], g["weight"])
+    s = api.Search(peak_radius=radius)
+    rid = s.add_reference(g["ref"], g["mask"])
+    s.set_orientations(grid)
+    cc, pk, best = s.run_host([s.particle(q, e.item(), rid, orient_count=len(grid))])
+    part = g["particle"].cpu().numpy()
+    w = g["weight"].cpu().numpy()
+    qo, eo = O.particle_spectrum(part, w)
+    cc_o, pk_o = O.search(case.ref, qo, eo, api.search_matrices(grid), mask=case.mask, radius=radius)
+    compare(cc, pk, cc_o, pk_o)
+    assert np.all(np.sum(pk.astype(float) ** 2, axis=1) <= radius * radius)
+    s.close()

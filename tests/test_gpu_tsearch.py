@@ -19,7 +19,7 @@ def make_tomo(shape, tmpl, positions, rng):
     return tomo
 
 
-@pytest.mark.parametrize("shape,t", [((48, 64, 64), 16), ((32, 48, 96), 12)])
+@pytest.mark.parametrize("shape,t", [((48, 64, 64), 16), ((32, 48, 96), 12), ((48, 72, 80), 15)])
 def test_template_search_against_oracle(built_lib, cuda, shape, t):
     from emclarity_b200 import api, synthetic
     rng = np.random.default_rng(41)
