@@ -154,6 +154,86 @@ __global__ void __launch_bounds__(256) k_avg_rotate(const float* __restrict__ vo
   }
 }
 
+// The same rotation with a 3-D thread layout: one CTA per 8^3 output brick of one particle, each
+// warp on a 4x4x2 voxel tile, two voxels per thread.  A rotated 4x4x2 tile reads a compact source
+// neighbourhood, so the warp's 256 corner loads touch far fewer sectors than a rotated 32-voxel
+// row does.  Per voxel the arithmetic (avg_sample, the symmetry sum, the division) is that of
+// k_avg_rotate, so the rotated volumes are bit-identical.
+constexpr int kBrick = 8;
+
+__global__ void __launch_bounds__(256) k_avg_rotate_tiled(const float* __restrict__ vols, long vol_stride,
+                                                          const int* __restrict__ vol_index, int n,
+                                                          const float* __restrict__ mats,
+                                                          const AvgParticle* __restrict__ parts, int use_shift,
+                                                          const float* __restrict__ mask, float bin_thr,
+                                                          float* __restrict__ out, AvgStats* __restrict__ stats) {
+  __shared__ double red[3][32];
+  const int p = blockIdx.y;
+  const AvgParticle pr = parts[p];
+  const int vi = vol_index ? vol_index[p] : p;
+  const long nv = (long)n * n * n;
+  float* dst = out + (long)p * nv;
+  const int nb = (n + kBrick - 1) / kBrick;
+  const int b = blockIdx.x;
+  const int t = threadIdx.x;
+  const int x = (b % nb) * kBrick + ((t & 3) | (((t >> 5) & 1) << 2));
+  const int y = ((b / nb) % nb) * kBrick + (((t >> 2) & 3) | (((t >> 6) & 1) << 2));
+  const int zb = (b / (nb * nb)) * kBrick + (((t >> 4) & 1) | (((t >> 7) & 1) << 1));
+  const int c = n / 2;
+  const float zero[3] = {0.f, 0.f, 0.f};
+  const float* sh = use_shift ? pr.shift : zero;
+  const float* src = vols + (long)(vi < 0 ? 0 : vi) * vol_stride;
+  const float* m0 = mats + (long)p * kAvgMaxSym * 9;
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int z = zb + 4 * q;
+    if (x >= n || y >= n || z >= n) continue;
+    const long i = ((long)z * n + y) * n + x;
+    float r = 0.f;
+    if (vi >= 0) {
+      const float u = (float)(x - c), v = (float)(y - c), w = (float)(z - c);
+      float acc = 0.f;
+      for (int k = 0; k < pr.nsym; ++k) acc += avg_sample(src, n, m0 + 9 * k, u, v, w, sh, c);
+      r = pr.nsym > 1 ? acc / (float)pr.nsym : acc;
+    }
+    dst[i] = r;
+    if (mask && vi >= 0) {
+      const float mk = __ldg(mask + i);
+      if (mk > bin_thr) {
+        s1 += (double)r;
+        s2 += (double)r * (double)r;
+      }
+      s3 += (double)r * (double)mk;
+    }
+  }
+  if (!mask) return;
+  const int lane = t & 31, warp = t >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+    s3 += __shfl_xor_sync(0xffffffffu, s3, off);
+  }
+  if (lane == 0) {
+    red[0][warp] = s1;
+    red[1][warp] = s2;
+    red[2][warp] = s3;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) {
+      t1 += red[0][wi];
+      t2 += red[1][wi];
+      t3 += red[2][wi];
+    }
+    atomicAdd(&stats[p].s1, t1);
+    atomicAdd(&stats[p].s2, t2);
+    atomicAdd(&stats[p].s3, t3);
+  }
+}
+
 // mean / rms inside the binary mask and the finite check of mean(r_normalised(:)); counts the
 // kept particles of each half set.
 __global__ void k_avg_coef(const AvgStats* __restrict__ stats, const AvgParticle* __restrict__ parts, int count,
@@ -453,14 +533,17 @@ emc_status emc_average_add(emc_average_t a, const float* d_particles, int count,
     EMC_CUDA(cudaMemcpyAsync(a->parts, parts.data(), sizeof(emc::AvgParticle) * nb, cudaMemcpyHostToDevice, st));
     if (a->nw) EMC_CUDA(cudaMemcpyAsync(a->widx, widx.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st));
     EMC_CUDA(cudaMemsetAsync(a->stats, 0, sizeof(emc::AvgStats) * nb, st));
-    const int gx = std::max(1, std::min<int>((int)((a->nv + 1023) / 1024), 256));
-    emc::k_avg_rotate<<<dim3(gx, nb), 256, 0, st>>>(d_particles + (size_t)b0 * a->nv, a->nv, nullptr, a->n, a->mats,
-                                                    a->parts, 1, a->mask, a->bin_thr, a->rot, a->stats);
+    const int bricks = ((a->n + emc::kBrick - 1) / emc::kBrick) * ((a->n + emc::kBrick - 1) / emc::kBrick) *
+                       ((a->n + emc::kBrick - 1) / emc::kBrick);
+    emc::k_avg_rotate_tiled<<<dim3(bricks, nb), 256, 0, st>>>(d_particles + (size_t)b0 * a->nv, a->nv, nullptr, a->n,
+                                                              a->mats, a->parts, 1, a->mask, a->bin_thr, a->rot,
+                                                              a->stats);
     EMC_LAUNCH_CHECK();
     if (a->nw) {
-      const int gw = std::max(1, std::min<int>((int)((a->nvw + 1023) / 1024), 256));
-      emc::k_avg_rotate<<<dim3(gw, nb), 256, 0, st>>>(d_wedges, a->nvw, a->widx, a->nw, a->mats, a->parts, 0,
-                                                      nullptr, 0.f, a->wrot, nullptr);
+      const int wb = ((a->nw + emc::kBrick - 1) / emc::kBrick) * ((a->nw + emc::kBrick - 1) / emc::kBrick) *
+                     ((a->nw + emc::kBrick - 1) / emc::kBrick);
+      emc::k_avg_rotate_tiled<<<dim3(wb, nb), 256, 0, st>>>(d_wedges, a->nvw, a->widx, a->nw, a->mats, a->parts, 0,
+                                                            nullptr, 0.f, a->wrot, nullptr);
       EMC_LAUNCH_CHECK();
     }
     emc::k_avg_coef<<<(nb + 127) / 128, 128, 0, st>>>(a->stats, a->parts, nb, a->n_bin, a->mask_sum, (double)a->nv,
