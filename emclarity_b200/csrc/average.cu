@@ -11,11 +11,11 @@
 //   * adds r .* peakWgt and w .* peakWgt to the sums of its half set (:1462-1482),
 // and the half-set average is sum / count (:1703-1707).
 //
-// B200 layout: a batch of particles is rotated into a scratch slab [batch][n^3] (one thread per
-// voxel, FP64 statistics per particle reduced with one atomic per block), a per-particle kernel
-// turns the statistics into (mean, rms, keep), and an output-stationary pass adds the batch to
-// the half-set sums voxel by voxel in the reference's particle order (so the FP32 sums round
-// the same way whatever the batch split).  No atomics touch the sums: results are deterministic.
+// B200 layout: a batch of particles is rotated into a scratch slab [batch][n^3] (8^3 output
+// bricks per CTA, 4x4x2 voxel tiles per warp, FP64 statistics per particle reduced with one atomic
+// per block), a per-particle kernel turns the statistics into (mean, rms, keep), and an
+// output-stationary pass adds the batch to the half-set sums voxel by voxel in the reference's
+// particle order (so the FP32 sums round the same way whatever the batch split).  No atomics touch the sums: results are deterministic.
 #include <algorithm>
 #include <cmath>
 #include <new>
@@ -88,80 +88,13 @@ __device__ __forceinline__ float avg_sample(const float* __restrict__ src, int n
 }
 
 // Rotates particle blockIdx.y of the batch into out[blockIdx.y]; with `mask`, accumulates the
-// particle's statistics.  mats: [batch][kAvgMaxSym][9] rows of A * S_k.
-__global__ void __launch_bounds__(256) k_avg_rotate(const float* __restrict__ vols, long vol_stride,
-                                                    const int* __restrict__ vol_index, int n,
-                                                    const float* __restrict__ mats,
-                                                    const AvgParticle* __restrict__ parts, int use_shift,
-                                                    const float* __restrict__ mask, float bin_thr,
-                                                    float* __restrict__ out, AvgStats* __restrict__ stats) {
-  __shared__ double red[3][32];
-  const int p = blockIdx.y;
-  const AvgParticle pr = parts[p];
-  const int vi = vol_index ? vol_index[p] : p;
-  const long nv = (long)n * n * n;
-  float* dst = out + (long)p * nv;
-  double s1 = 0.0, s2 = 0.0, s3 = 0.0;
-  if (vi >= 0) {
-    const float* src = vols + (long)vi * vol_stride;
-    const float* m0 = mats + (long)p * kAvgMaxSym * 9;
-    const float zero[3] = {0.f, 0.f, 0.f};
-    const float* t = use_shift ? pr.shift : zero;
-    const int c = n / 2;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nv; i += (long)gridDim.x * blockDim.x) {
-      const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((long)n * n));
-      const float u = (float)(x - c), v = (float)(y - c), w = (float)(z - c);
-      float acc = 0.f;
-      for (int k = 0; k < pr.nsym; ++k) acc += avg_sample(src, n, m0 + 9 * k, u, v, w, t, c);
-      const float r = pr.nsym > 1 ? acc / (float)pr.nsym : acc;
-      dst[i] = r;
-      if (mask) {
-        const float mk = __ldg(mask + i);
-        if (mk > bin_thr) {
-          s1 += (double)r;
-          s2 += (double)r * (double)r;
-        }
-        s3 += (double)r * (double)mk;
-      }
-    }
-  } else {
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nv; i += (long)gridDim.x * blockDim.x) dst[i] = 0.f;
-  }
-  if (!mask) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    s3 += __shfl_xor_sync(0xffffffffu, s3, o);
-  }
-  if (lane == 0) {
-    red[0][warp] = s1;
-    red[1][warp] = s2;
-    red[2][warp] = s3;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t1 = 0.0, t2 = 0.0, t3 = 0.0;
-    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) {
-      t1 += red[0][wi];
-      t2 += red[1][wi];
-      t3 += red[2][wi];
-    }
-    atomicAdd(&stats[p].s1, t1);
-    atomicAdd(&stats[p].s2, t2);
-    atomicAdd(&stats[p].s3, t3);
-  }
-}
-
-// The same rotation with a 3-D thread layout: one CTA per 8^3 output brick of one particle, each
-// warp on a 4x4x2 voxel tile, two voxels per thread.  A rotated 4x4x2 tile reads a compact source
-// neighbourhood, so the warp's 256 corner loads touch far fewer sectors than a rotated 32-voxel
-// row does.  Per voxel the arithmetic (avg_sample, the symmetry sum, the division) is that of
-// k_avg_rotate, so the rotated volumes are bit-identical.
+// particle's statistics.  mats: [batch][kAvgMaxSym][9] rows of A * S_k.  One CTA per 8^3 output
+// brick (blockIdx.x), each warp on a 4x4x2 voxel tile, two voxels per thread: a rotated 4x4x2
+// tile reads a compact source neighbourhood, so the warp's 256 corner loads touch far fewer
+// sectors than a rotated 32-voxel row would.  Symmetry copies are summed in operator order.
 constexpr int kBrick = 8;
 
-__global__ void __launch_bounds__(256) k_avg_rotate_tiled(const float* __restrict__ vols, long vol_stride,
+__global__ void __launch_bounds__(256) k_avg_rotate(const float* __restrict__ vols, long vol_stride,
                                                           const int* __restrict__ vol_index, int n,
                                                           const float* __restrict__ mats,
                                                           const AvgParticle* __restrict__ parts, int use_shift,
@@ -535,14 +468,14 @@ emc_status emc_average_add(emc_average_t a, const float* d_particles, int count,
     EMC_CUDA(cudaMemsetAsync(a->stats, 0, sizeof(emc::AvgStats) * nb, st));
     const int bricks = ((a->n + emc::kBrick - 1) / emc::kBrick) * ((a->n + emc::kBrick - 1) / emc::kBrick) *
                        ((a->n + emc::kBrick - 1) / emc::kBrick);
-    emc::k_avg_rotate_tiled<<<dim3(bricks, nb), 256, 0, st>>>(d_particles + (size_t)b0 * a->nv, a->nv, nullptr, a->n,
+    emc::k_avg_rotate<<<dim3(bricks, nb), 256, 0, st>>>(d_particles + (size_t)b0 * a->nv, a->nv, nullptr, a->n,
                                                               a->mats, a->parts, 1, a->mask, a->bin_thr, a->rot,
                                                               a->stats);
     EMC_LAUNCH_CHECK();
     if (a->nw) {
       const int wb = ((a->nw + emc::kBrick - 1) / emc::kBrick) * ((a->nw + emc::kBrick - 1) / emc::kBrick) *
                      ((a->nw + emc::kBrick - 1) / emc::kBrick);
-      emc::k_avg_rotate_tiled<<<dim3(wb, nb), 256, 0, st>>>(d_wedges, a->nvw, a->widx, a->nw, a->mats, a->parts, 0,
+      emc::k_avg_rotate<<<dim3(wb, nb), 256, 0, st>>>(d_wedges, a->nvw, a->widx, a->nw, a->mats, a->parts, 0,
                                                             nullptr, 0.f, a->wrot, nullptr);
       EMC_LAUNCH_CHECK();
     }
