@@ -68,4 +68,19 @@ const float2* device_twiddles(int L);  // returns nullptr on failure (error text
 // Device-side number of SMs (cached per device).
 int device_sm_count();
 
+#ifdef __CUDACC__
+// Asynchronous global -> shared copies of 8 bytes (cp.async, no register staging).  A thread's
+// copies are complete after cp_async_wait<N>() leaves at most N of its committed groups pending;
+// a barrier then publishes them to the other threads.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+#endif
+
 }  // namespace emc

@@ -46,15 +46,20 @@ static emc_status cols_t(const float2* in, float2* out, long stride, long inner,
   const float2* tw = device_twiddles(L);
   if (!tw) return EMC_E_CUDA;
   auto kern = k_cols<L, SIGN, C::P, C::T>;
-  static bool attr_set[64] = {false};
+  static int resident[64] = {0};  // CTAs per SM, per device
   int dev = 0;
   cudaGetDevice(&dev);
-  if (C::smem > 48 * 1024 && dev < 64 && !attr_set[dev]) {
-    EMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem));
-    attr_set[dev] = true;
+  if (dev >= 64) return EMC_E_CUDA;
+  if (!resident[dev]) {
+    if (C::smem > 48 * 1024)
+      EMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem));
+    int nb = 0;
+    EMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, C::P * C::T, C::smem));
+    resident[dev] = std::max(nb, 1);
   }
-  dim3 grid((unsigned)((inner + C::T - 1) / C::T), (unsigned)std::min<long>(outer, 65535));
-  kern<<<grid, C::P * C::T, C::smem, st>>>(in, out, stride, inner, outer, outer_pitch, tw);
+  const long units = (inner + C::T - 1) / C::T * outer;
+  const long ctas = std::min<long>(units, (long)resident[dev] * device_sm_count());
+  kern<<<(unsigned)ctas, C::P * C::T, C::smem, st>>>(in, out, stride, inner, outer, outer_pitch, tw);
   EMC_LAUNCH_CHECK();
   return EMC_OK;
 }

@@ -107,52 +107,58 @@ __global__ void __launch_bounds__(256) k_rows_c2r(const float2* __restrict__ in,
 // ----------------------------------------------------------------- strided columns
 // Complex lines along a strided axis: element n of line (o, i) lives at
 // base + o*outer_pitch + i + n*stride, for i in [0, inner), o in [0, outer).
-// One CTA transforms a tile of T consecutive i for one o; in == out is allowed.
+// A unit of work is a tile of T consecutive i of one o; in == out is allowed (units are disjoint).
+// Persistent CTAs walk the units with a stride of gridDim.x and double-buffer them in shared
+// memory: the cp.async copies of the next tile are in flight while the current tile is
+// transformed and written back, so the loads of a one-CTA-per-SM kernel overlap its FFT.
 template <int L, int SIGN, int P, int T>
 __global__ void __launch_bounds__(P * T) k_cols(const float2* __restrict__ in, float2* __restrict__ out,
                                                 long stride, long inner, long outer, long outer_pitch,
                                                 const float2* __restrict__ g_tw) {
   extern __shared__ float2 smem[];
-  float2* s_tw = smem;
-  float2* tile = smem + L;  // [padded L][T+1], element n of line t at lpos<PAD>(n) * TP + t
   constexpr int TP = T + 1;
   constexpr int PAD = line_pad(L);
+  constexpr int TILE = padded_len(L, PAD) * TP;  // element n of line t at lpos<PAD>(n) * TP + t
+  float2* s_tw = smem;
+  float2* tiles = smem + L;  // [2][TILE]
   load_twiddles<L>(s_tw, g_tw);
-  const long i0 = (long)blockIdx.x * T;
-  const int nt = P * T;
+  const long ntile = (inner + T - 1) / T;
+  const long units = ntile * outer;
+  constexpr int NT = P * T;
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
-  for (long o = blockIdx.y; o < outer; o += gridDim.y) {
+  auto issue = [&](long u, float2* tile) {
+    const long o = u / ntile, i0 = (u % ntile) * T;
     const float2* src = in + o * outer_pitch + i0;
-    float2* dst = out + o * outer_pitch + i0;
-    __syncthreads();
-    {
-      // groups of up to 8 loads in flight before their shared-memory stores
-      constexpr int IT = (L * T + P * T - 1) / (P * T);
-      constexpr int GRP = IT < (L > 256 ? 4 : 8) ? IT : (L > 256 ? 4 : 8);
-#pragma unroll
-      for (int k0 = 0; k0 < IT; k0 += GRP) {
-        float2 v[GRP];
-#pragma unroll
-        for (int k = 0; k < GRP; ++k) {
-          const int idx = threadIdx.x + (k0 + k) * nt;
-          const int n = idx / T, t = idx % T;
-          if (k0 + k < IT && idx < L * T && i0 + t < inner) v[k] = src[(long)n * stride + t];
-        }
-#pragma unroll
-        for (int k = 0; k < GRP; ++k) {
-          const int idx = threadIdx.x + (k0 + k) * nt;
-          const int n = idx / T, t = idx % T;
-          if (k0 + k < IT && idx < L * T && i0 + t < inner) tile[lpos<PAD>(n) * TP + t] = v[k];
-        }
-      }
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < L * T; idx += NT) {
+      const int n = idx / T, t = idx % T;
+      if (i0 + t < inner) cp_async8(tile + lpos<PAD>(n) * TP + t, src + (long)n * stride + t);
     }
-    __syncthreads();
+    cp_async_commit();
+  };
+  long u = blockIdx.x;
+  if (u < units) issue(u, tiles);
+  int cur = 0;
+  for (; u < units; u += gridDim.x) {
+    const long un = u + gridDim.x;
+    if (un < units) {
+      issue(un, tiles + (cur ^ 1) * TILE);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();  // tile `cur` (and the twiddles) visible to every thread
+    float2* tile = tiles + cur * TILE;
+    const long o = u / ntile, i0 = (u % ntile) * T;
     fft_line<L, SIGN, P, PAD>(tile + team, TP, lane, s_tw, i0 + team < inner);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < L * T; idx += nt) {
+    float2* dst = out + o * outer_pitch + i0;
+    for (int idx = threadIdx.x; idx < L * T; idx += NT) {
       const int n = idx / T, t = idx % T;
       if (i0 + t < inner) dst[(long)n * stride + t] = tile[lpos<PAD>(n) * TP + t];
     }
+    __syncthreads();  // tile `cur` has been read; the next iteration's copies land in it
+    cur ^= 1;
   }
 }
 
@@ -160,7 +166,7 @@ template <int L>
 struct ColsCfg {
   static constexpr int P = team_size(L);
   static constexpr int T = (512 / P) < 32 ? (512 / P) : 32;
-  static constexpr size_t smem = sizeof(float2) * (L + (size_t)padded_len(L, line_pad(L)) * (T + 1));
+  static constexpr size_t smem = sizeof(float2) * (L + 2 * (size_t)padded_len(L, line_pad(L)) * (T + 1));
 };
 
 // Host launchers (defined in fft_passes.cu); return EMC_OK or an error status.

@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(P * TT) k_ts_zfused(const float2* __restrict__
   float2* tile = smem + L;  // [padded L][TT+1], element n of line t at lpos<PAD>(n) * TP + t
   constexpr int TP = TT + 1;
   constexpr int PAD = line_pad(L);
+  static_assert((P * TT) % 32 == 0, "the statistics reduction needs whole warps");
   __shared__ double red[32];
   load_twiddles<L>(s_tw, g_tw);
   const long inner = (long)g.ny * g.nxh, stride = inner;
@@ -313,10 +314,21 @@ static emc_status launch_ts_zfused(const float2* gt, const float2* T, float2* s,
   using C = ColsCfg<L>;
   const float2* tw = device_twiddles(L);
   if (!tw) return EMC_E_CUDA;
-  auto kern = k_ts_zfused<L, C::P, C::T>;
-  if (C::smem > 48 * 1024) EMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem));
+  // Narrow tiles (8 lines, or one warp when the team is smaller than 4 lanes) keep several CTAs
+  // resident per SM, so one CTA's loads overlap another's transforms.
+  constexpr int TT = C::P >= 4 ? 8 : 32 / C::P;
+  auto kern = k_ts_zfused<L, C::P, TT>;
+  constexpr size_t smem = sizeof(float2) * (L + (size_t)padded_len(L, line_pad(L)) * (TT + 1));
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64) return EMC_E_CUDA;
+  if (smem > 48 * 1024 && !attr_set[dev]) {
+    EMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[dev] = true;
+  }
   const long inner = (long)g.ny * g.nxh;
-  kern<<<(unsigned)((inner + C::T - 1) / C::T), C::P * C::T, C::smem, st>>>(gt, T, s, g, stats, tw);
+  kern<<<(unsigned)((inner + TT - 1) / TT), C::P * TT, smem, st>>>(gt, T, s, g, stats, tw);
   EMC_LAUNCH_CHECK();
   return EMC_OK;
 }
