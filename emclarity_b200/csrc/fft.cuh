@@ -258,8 +258,14 @@ __host__ __device__ __forceinline__ constexpr int lpos(int i) {
 __host__ __device__ constexpr int padded_len(int L, int pad = 1) {
   return pad == 0 ? L : (pad == 1 ? L + L / 8 : L + L / 16);
 }
-// The padding that spreads the first stage's writes of a length-L line over the banks.
-__host__ __device__ constexpr int line_pad(int L) { return radix_of(L, 0) >= 16 ? 2 : 1; }
+// The padding that spreads the first stage's writes of a length-L line over the banks.  512
+// (8 x 8 x 8) and 192 (8 x 8 x 3) also take the 16-element gap: their later stages read with
+// strides of 64, where the 8-element gap leaves half-warps two or three ways on one bank (a
+// half-warp model of the stage accesses gives 1.17 / 1.18 times the conflict-free wavefront
+// count against 1.67 / 1.45 with the 8-element gap).
+__host__ __device__ constexpr int line_pad(int L) {
+  return radix_of(L, 0) >= 16 || L == 512 || L == 192 ? 2 : 1;
+}
 
 // Per-lane twiddles of stage S (NS = product of the earlier radices), kept in registers.  Lane
 // `lane` of a team always handles butterflies j = lane + b P, whose twiddle exponents depend on
