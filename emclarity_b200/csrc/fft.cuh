@@ -226,6 +226,13 @@ __host__ __device__ constexpr int max_radix(int L, int s = 0) {
   return radix_of(L, s) <= 1 ? 1
          : (radix_of(L, s) > max_radix(L, s + 1) ? radix_of(L, s) : max_radix(L, s + 1));
 }
+// Complex values a lane of a P-lane team holds in the largest stage of a length-L line.
+__host__ __device__ constexpr int stage_values(int L, int P, int s = 0) {
+  return radix_of(L, s) <= 1 ? 0
+         : ((L / radix_of(L, s) + P - 1) / P) * radix_of(L, s) > stage_values(L, P, s + 1)
+             ? ((L / radix_of(L, s) + P - 1) / P) * radix_of(L, s)
+             : stage_values(L, P, s + 1);
+}
 __host__ __device__ constexpr int min_butterflies(int L) { return radix_of(L, 0) == 0 ? 0 : L / max_radix(L); }
 
 // Default team size: a power of two no larger than the smallest butterfly count, <= 32.

@@ -102,8 +102,14 @@ __global__ void __launch_bounds__(256) k_ts_rows(const float* __restrict__ tmpl,
 // Per tile of TT consecutive (ky, kx) z-lines: G = FFT_z of the t planes at z = pl[2].. (zeros
 // elsewhere), X = T .* conj(G), inverse FFT_z into s.  stats[0] += sum over the full spectrum of
 // |X|^2 (Hermitian weights), stats[1] = X(0).
+// Resident CTAs per SM asked of the compiler: 20 warps' worth when a lane holds at most 16 complex
+// values per stage (the register cap then leaves room for them), else no constraint.
+constexpr int zfused_min_blocks(int L, int P, int TT) {
+  return stage_values(L, P) <= 16 && 640 / (P * TT) > 1 ? 640 / (P * TT) : 1;
+}
+
 template <int L, int P, int TT>
-__global__ void __launch_bounds__(P * TT) k_ts_zfused(const float2* __restrict__ gt, const float2* __restrict__ T,
+__global__ void __launch_bounds__(P * TT, zfused_min_blocks(L, P, TT)) k_ts_zfused(const float2* __restrict__ gt, const float2* __restrict__ T,
                                                       float2* __restrict__ s, const TsGeom g,
                                                       double* __restrict__ stats, const float2* __restrict__ g_tw) {
   extern __shared__ float2 smem[];
