@@ -250,7 +250,11 @@ struct SearchCfg {
   // boxes, whose FFT codelets need more registers
   static constexpr int SMEM_CTAS_A = (int)((228 * 1024) / (SMEM_A + 1024));
   static constexpr int MINB_A = N <= 64 ? 0 : (SMEM_CTAS_A < 2 ? SMEM_CTAS_A : 2);
-  static constexpr size_t SMEM_B = sizeof(float2) * ((size_t)PY * NH + N);
+  // pass B prefetches its particle-spectrum and weight slabs into shared memory where that still
+  // leaves four CTAs per SM (64^3); the larger boxes load them after the forward transform
+  static constexpr bool PREF_B = N <= 64;
+  static constexpr size_t SMEM_B =
+      sizeof(float2) * ((size_t)PY * NH + N) + (PREF_B ? (sizeof(float2) + sizeof(float)) * (size_t)N * NH : 0);
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
 };
 
@@ -506,6 +510,23 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
   const float2* __restrict__ q = pt.spec;
   const int w = 2 * a.radius + 1;
 
+  // (PREF_B) this thread's elements i of the particle spectrum and of the reference weight at this
+  // ky, copied asynchronously while the slab loads and the forward transform run
+  float2* s_q = s_tw + N;                                  // [N * NH]
+  float* s_w = reinterpret_cast<float*>(s_q + N * NH);     // [N * NH]
+  if constexpr (C::PREF_B) {
+    constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      const int i = threadIdx.x + k * C::NT_BC;
+      if (i < N * NH) {
+        const size_t gi = ((size_t)(i / NH) * N + ky) * NH + i % NH;
+        cp_async8(s_q + i, q + gi);
+        if (wref) cp_async4(s_w + i, wref + gi);
+      }
+    }
+    cp_async_commit();
+  }
   load_twiddles<N>(s_tw, g_tw);
   const float2* src = a.s1 + (size_t)e * N * N * NH + (size_t)ky * NH;
   {
@@ -534,11 +555,15 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
   double en = 0.0;
   {
     constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
-    float2 qv[IT];
+    float2 qv[C::PREF_B ? 1 : IT];
+    if constexpr (C::PREF_B) {
+      cp_async_wait<0>();  // this thread's own copies; no other thread reads them
+    } else {
 #pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * C::NT_BC;
-      if (i < N * NH) qv[k] = __ldg(q + ((size_t)(i / NH) * N + ky) * NH + i % NH);
+      for (int k = 0; k < IT; ++k) {
+        const int i = threadIdx.x + k * C::NT_BC;
+        if (i < N * NH) qv[k] = __ldg(q + ((size_t)(i / NH) * N + ky) * NH + i % NH);
+      }
     }
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
@@ -549,12 +574,12 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
       float2& slot = tile[lpos<1>(z) * NH + kx];
       float2 r = slot;
       if (wref) {
-        const float wv = __ldg(wref + gi);
+        const float wv = C::PREF_B ? s_w[i] : __ldg(wref + gi);
         r.x *= wv;
         r.y *= wv;
         if (gi != 0) en += (kx == 0 || 2 * kx == N ? 1.0 : 2.0) * ((double)r.x * r.x + (double)r.y * r.y);
       }
-      float2 x = cmulc(qv[k], r);
+      float2 x = cmulc(C::PREF_B ? s_q[i] : qv[C::PREF_B ? 0 : k], r);
       if (gi == 0) x = make_float2(0.f, 0.f);
       slot = x;
     }
