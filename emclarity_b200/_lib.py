@@ -86,12 +86,14 @@ SIGNATURES = {
     "emc_xcf_rotational": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _pd, _vp]),
     "emc_xcf_translational": (_i, [_vp, _vp, _i, _i, _i, _vp, _i, _pd, _pd, _vp, _vp]),
     "emc_particle_spectrum": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "emc_particle_spectra": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "emc_particle_template": (_i, [_i, _vp, _vp, _vp]),
     "emc_search_create": (_i, [C.POINTER(_vp)]),
     "emc_search_add_reference": (_i, [_vp, _vp, _i, _vp, _vp, _i, _pi, _vp]),
     "emc_search_set_orientations": (_i, [_vp, _pd, _i]),
     "emc_search_configure": (_i, [_vp, _i, _i, _i]),
     "emc_search_run": (_i, [_vp, C.POINTER(ParticleDesc), _i, _vp, _vp, _vp, _vp]),
+    "emc_search_run_energies": (_i, [_vp, C.POINTER(ParticleDesc), _i, _vp, _vp, _vp, _vp, _vp]),
     "emc_search_run_host": (_i, [_vp, C.POINTER(ParticleDesc), _i, _pf, _pi, C.POINTER(SearchHit), _vp]),
     "emc_search_destroy": (_i, [_vp]),
     "emc_search_set_profiling": (_i, [_vp, _i]),

@@ -230,6 +230,26 @@ def particle_spectrum(particle, weight=None, bandpass=None):
     return q, e
 
 
+def particle_spectra(particles, weights=None, bandpass=None, out=None, energies=None):
+    """particle_spectrum over a batch: particles [B, n, n, n], weights [B, n, n, n/2+1] or None,
+    bandpass one shared half spectrum or None.  Returns (spectra [B, n, n, n/2+1] complex64,
+    energies [B] float64), written into `out` / `energies` when given."""
+    count, n = particles.shape[0], particles.shape[-1]
+    if weights is not None and (weights.shape[0] != count or weights[0].numel() != n * n * (n // 2 + 1)):
+        raise ValueError("weights must hold one half spectrum per particle")
+    if out is None:
+        out = torch.empty((count, n, n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    if energies is None:
+        energies = torch.empty(count, dtype=torch.float64, device="cuda")
+    if out.shape[0] < count or energies.numel() < count:
+        raise ValueError("out / energies hold fewer than %d particles" % count)
+    L.call("emc_particle_spectra", n, count, _need_cuda(particles, "particles"),
+           _need_cuda(weights, "weights") if weights is not None else None,
+           _need_cuda(bandpass, "bandpass") if bandpass is not None else None,
+           _need_cuda(out, "out", torch.complex64), _need_cuda(energies, "energies", torch.float64), _stream())
+    return out, energies
+
+
 def particle_template(q):
     """h = unnormalised inverse transform of Q (the real-space particle template)."""
     n = q.shape[0]
@@ -282,14 +302,23 @@ class Search:
         d.orient_count = int(orient_count)
         return d
 
-    def run(self, particles, cc=None, peak=None, best=None, stream=None):
-        """Device outputs: cc (float32 [pairs]), peak (int32 [pairs, 3]), best (int32 [np, 5] view of hits)."""
+    def run(self, particles, cc=None, peak=None, best=None, stream=None, energies=None):
+        """Device outputs: cc (float32 [pairs]), peak (int32 [pairs, 3]), best (int32 [np, 5] view of hits).
+        energies: optional CUDA float64 [np] (as written by particle_spectrum); when given, the
+        search reads particle p's energy from it on the device and ignores the descriptors' values."""
+        if energies is not None and (not isinstance(energies, torch.Tensor) or energies.dtype != torch.float64
+                                     or energies.numel() < len(particles)):
+            raise ValueError("energies must be a float64 tensor with one value per particle")
         arr = (L.ParticleDesc * len(particles))(*particles)
         self._keep = [arr]
-        L.call("emc_search_run", self._h, arr, len(particles),
-               _need_cuda(cc, "cc") if cc is not None else None,
-               _need_cuda(peak, "peak", torch.int32) if peak is not None else None,
-               _need_cuda(best, "best", torch.int32) if best is not None else None, _stream(stream))
+        outs = (_need_cuda(cc, "cc") if cc is not None else None,
+                _need_cuda(peak, "peak", torch.int32) if peak is not None else None,
+                _need_cuda(best, "best", torch.int32) if best is not None else None, _stream(stream))
+        if energies is None:
+            L.call("emc_search_run", self._h, arr, len(particles), *outs)
+        else:
+            L.call("emc_search_run_energies", self._h, arr, len(particles),
+                   _need_cuda(energies, "energies", torch.float64), *outs)
 
     def run_host(self, particles):
         """Host outputs: (cc [pairs], peak [pairs, 3], best list of (cc, orient, peak))."""

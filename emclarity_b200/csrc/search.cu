@@ -36,6 +36,13 @@ __global__ void k_search_best(const DevParticle* __restrict__ parts, int np, con
   out[p] = h;
 }
 
+// Particle energies taken from device memory (written there by emc_particle_spectrum) when the run
+// executes, for emc_search_run_energies.
+__global__ void k_search_energies(DevParticle* __restrict__ parts, int np, const double* __restrict__ energy) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < np) parts[p].energy = energy[p];
+}
+
 __global__ void k_search_scatter(const EvalResult* __restrict__ results, long n, float* __restrict__ cc,
                                  int* __restrict__ peak) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -233,9 +240,14 @@ struct DevBuf {
   }
 };
 
+// Weights particle blockIdx.y of a batch (spectra, weights and energies advance by nhalf, nhalf and
+// 1 per particle; wgt_stride 0 shares one weight) and accumulates its energy.
 __global__ void k_particle_weight(float2* __restrict__ q, const float* __restrict__ wgt, const float* __restrict__ bp,
-                                  long nhalf, int nh, int n, double* __restrict__ energy) {
+                                  long nhalf, int nh, int n, double* __restrict__ energy, long wgt_stride = 0) {
   __shared__ double red[32];
+  q += (long)blockIdx.y * nhalf;
+  if (wgt) wgt += (long)blockIdx.y * wgt_stride;
+  energy += blockIdx.y;
   double e = 0.0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nhalf; i += (long)gridDim.x * blockDim.x) {
     float f = 1.f;
@@ -285,6 +297,7 @@ struct emc_search_s {
   emc::DevBuf<unsigned long long> keys;
   emc::DevBuf<unsigned> done;
 
+  const double* run_energy = nullptr;  // device energies of the run being recorded (or null)
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t gexec = nullptr;
   std::vector<char> gkey;
@@ -502,6 +515,11 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
   EMC_CUDA(cudaMemsetAsync(s->keys.p, 0, sizeof(unsigned long long) * s->keys.cap, st));
   EMC_CUDA(cudaMemsetAsync(s->done.p, 0, sizeof(unsigned) * s->done.cap, st));
   long launches = 0;
+  if (s->run_energy) {
+    emc::k_search_energies<<<(np + 255) / 256, 256, 0, st>>>(s->d_parts.p, np, s->run_energy);
+    EMC_LAUNCH_CHECK();
+    ++launches;
+  }
   for (const Chunk& c : chunks) {
     const emc::SearchChunkArgs a = chunk_args(s, c);
     cudaEvent_t* ev = nullptr;
@@ -535,8 +553,8 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
   return EMC_OK;
 }
 
-emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, int np, float* d_cc, int* d_peak,
-                          emc_search_hit* d_best, void* stream) {
+static emc_status search_run(emc_search_t s, const emc_particle_desc* particles, int np, const double* d_energy,
+                             float* d_cc, int* d_peak, emc_search_hit* d_best, void* stream) {
   EMC_CHECK_ARG(s && particles && np > 0, "emc_search_run: bad argument");
   EMC_CHECK_ARG(s->norient > 0, "emc_search_run: no orientations set");
   cudaStream_t st = emc::as_stream(stream);
@@ -552,7 +570,7 @@ emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, in
     EMC_CHECK_ARG(d.orient_begin >= 0 && d.orient_count >= 0 && d.orient_begin + d.orient_count <= s->norient,
                   "particle %d: orientation slice [%d, %d) outside [0, %d)", p, d.orient_begin,
                   d.orient_begin + d.orient_count, s->norient);
-    EMC_CHECK_ARG(d.energy > 0.0, "particle %d: energy must be > 0", p);
+    EMC_CHECK_ARG(d_energy || d.energy > 0.0, "particle %d: energy must be > 0", p);
     emc::DevParticle& q = parts[p];
     q.spec = reinterpret_cast<const float2*>(d.spectrum);
     q.energy = d.energy;
@@ -576,8 +594,9 @@ emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, in
     const size_t nref = s->refs.size();
     memcpy(k + 40, &nref, 8);
     memcpy(k + 48, &st, 8);
-    memset(k + 56, 0, 8);
+    memcpy(k + 56, &d_energy, 8);
   }
+  s->run_energy = d_energy;
   if (!s->profiling && !s->gkey.empty() && s->gkey == key && s->gexec && !s->refs_dirty) {
     EMC_CUDA(cudaGraphLaunch(s->gexec, st));
     return EMC_OK;
@@ -675,6 +694,18 @@ emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, in
   s->gkey = key;
   EMC_CUDA(cudaGraphLaunch(s->gexec, st));
   return EMC_OK;
+}
+
+emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, int np, float* d_cc, int* d_peak,
+                          emc_search_hit* d_best, void* stream) {
+  return search_run(s, particles, np, nullptr, d_cc, d_peak, d_best, stream);
+}
+
+emc_status emc_search_run_energies(emc_search_t s, const emc_particle_desc* particles, int np,
+                                   const double* d_energy, float* d_cc, int* d_peak, emc_search_hit* d_best,
+                                   void* stream) {
+  EMC_CHECK_ARG(d_energy, "emc_search_run_energies: null energy array");
+  return search_run(s, particles, np, d_energy, d_cc, d_peak, d_best, stream);
 }
 
 emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particles, int np, float* h_cc, int* h_peak,
@@ -805,6 +836,23 @@ emc_status emc_particle_spectrum(int n, const float* d_particle, const float* d_
   const long nhalf = (long)(n / 2 + 1) * n * n;
   const int blocks = (int)std::min<long>((nhalf + 255) / 256, 2L * emc::device_sm_count());
   emc::k_particle_weight<<<blocks, 256, 0, st>>>(q, d_weight, d_bandpass, nhalf, n / 2 + 1, n, d_energy);
+  EMC_LAUNCH_CHECK();
+  return EMC_OK;
+}
+
+emc_status emc_particle_spectra(int n, int count, const float* d_particles, const float* d_weights,
+                                const float* d_bandpass, float* d_spectra_out, double* d_energies, void* stream) {
+  EMC_CHECK_ARG(d_particles && d_spectra_out && d_energies && count > 0, "emc_particle_spectra: bad argument");
+  EMC_CHECK_ARG(emc::fft_length_supported(n) && n >= 2, "emc_particle_spectra: box %d not supported", n);
+  EMC_CHECK_ARG(count <= 65535, "emc_particle_spectra: at most 65535 particles per call (got %d)", count);
+  cudaStream_t st = emc::as_stream(stream);
+  float2* q = reinterpret_cast<float2*>(d_spectra_out);
+  EMC_TRY(emc::fft3_r2c(d_particles, q, n, n, n, count, st));
+  EMC_CUDA(cudaMemsetAsync(d_energies, 0, sizeof(double) * count, st));
+  const long nhalf = (long)(n / 2 + 1) * n * n;
+  const int bx = (int)std::max<long>(1, std::min<long>((nhalf + 255) / 256, (2L * emc::device_sm_count() + count - 1) / count));
+  emc::k_particle_weight<<<dim3(bx, count), 256, 0, st>>>(q, d_weights, d_bandpass, nhalf, n / 2 + 1, n, d_energies,
+                                                          nhalf);
   EMC_LAUNCH_CHECK();
   return EMC_OK;
 }

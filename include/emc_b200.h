@@ -228,6 +228,15 @@ typedef struct {
 EMC_API emc_status emc_particle_spectrum(int n, const float* d_particle, const float* d_weight,
                                  const float* d_bandpass, float* d_spectrum_out,
                                  double* d_energy, void* stream);
+/* emc_particle_spectrum over `count` particles in one call (three FFT passes and one weighting
+ * launch for the whole batch instead of five launches per particle): d_particles [count][n^3],
+ * d_weights [count][(n/2+1)*n*n] or NULL, d_bandpass one shared half spectrum or NULL,
+ * d_spectra_out [count][(n/2+1)*n*n] complex, d_energies [count].  The per-particle loop of
+ * BH_alignRaw3d_v2.m:1089-1100 (particle weight, BH_bandLimitCenterNormalize) batched; each
+ * particle's result equals emc_particle_spectrum's. */
+EMC_API emc_status emc_particle_spectra(int n, int count, const float* d_particles,
+                                const float* d_weights, const float* d_bandpass,
+                                float* d_spectra_out, double* d_energies, void* stream);
 
 EMC_API emc_status emc_search_create(emc_search_t* out);
 /* Registers a reference volume (n^3 floats, device), an optional real-space mask
@@ -253,6 +262,15 @@ EMC_API emc_status emc_search_configure(emc_search_t s, int peak_radius, int int
  * launch sequence is captured in a CUDA graph and replayed on identical calls. */
 EMC_API emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, int n_particles,
                           float* d_cc, int* d_peak, emc_search_hit* d_best, void* stream);
+/* emc_search_run with the particle energies read on the device: d_energy[p] replaces
+ * particles[p].energy (which is ignored) and is read when the run executes on the stream,
+ * so spectra from emc_particle_spectrum can feed the search with no host round trip in
+ * between.  No counterpart in the reference, where the energy is a MATLAB scalar computed
+ * on the host per particle (BH_alignRaw3d_v2.m:1098-1100 via BH_bandLimitCenterNormalize);
+ * a particle whose energy is not > 0 scores CC = 0. */
+EMC_API emc_status emc_search_run_energies(emc_search_t s, const emc_particle_desc* particles,
+                                   int n_particles, const double* d_energy, float* d_cc,
+                                   int* d_peak, emc_search_hit* d_best, void* stream);
 /* Same as emc_search_run with host output buffers (copies inside, synchronises). */
 EMC_API emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particles,
                                int n_particles, float* h_cc, int* h_peak,

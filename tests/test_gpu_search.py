@@ -275,3 +275,58 @@ def test_large_peak_radius_matches_oracle(plain_case, radius):
     compare(cc, pk, cc_o, pk_o)
     assert np.all(np.sum(pk.astype(float) ** 2, axis=1) <= radius * radius)
     s.close()
+
+
+def test_device_energies_match_host_energies(plain_case):
+    """emc_search_run_energies reads E_P from device memory; the descriptors' energies are ignored
+    (here deliberately wrong), and the results equal those of emc_search_run with host energies."""
+    from emclarity_b200 import api
+    case, g = plain_case
+    grid = case.grid[::4]
+    shifts = [(0, 0, 0), (1, -2, 0), (0, 3, -1)]
+    qs, es = [], []
+    for k in range(3):
+        part = torch.roll(g["particle"], shifts=shifts[k], dims=(0, 1, 2)).contiguous()
+        q, e = api.particle_spectrum(part, g["weight"])
+        qs.append(q)
+        es.append(e)
+    energies = torch.cat(es)
+    s = api.Search(peak_radius=case.peak_radius)
+    rid = s.add_reference(g["ref"], g["mask"])
+    s.set_orientations(grid)
+    n_or = len(grid)
+    outs = []
+    cc = torch.empty(3 * n_or, device="cuda")
+    pk = torch.empty((3 * n_or, 3), dtype=torch.int32, device="cuda")
+    best = torch.empty((3, 5), dtype=torch.int32, device="cuda")
+    for use_dev in (False, True, True):  # the second device run replays the cached graph
+        descs = [s.particle(qs[k], 1.0 if use_dev else es[k].item(), rid, orient_count=n_or) for k in range(3)]
+        cc.fill_(-5.0)
+        s.run(descs, cc=cc, peak=pk, best=best, energies=energies if use_dev else None)
+        torch.cuda.synchronize()
+        outs.append((cc.cpu().numpy(), pk.cpu().numpy(), best.cpu().numpy()))
+    with pytest.raises(ValueError):
+        s.run(descs, energies=energies.float())
+    s.close()
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0])
+        assert np.array_equal(o[1], outs[0][1])
+        assert np.array_equal(o[2], outs[0][2])
+
+
+def test_batched_particle_spectra_match_single(plain_case):
+    """emc_particle_spectra over a batch equals emc_particle_spectrum particle by particle (same FFT
+    passes per line; energies are FP64 sums whose order may differ)."""
+    from emclarity_b200 import api
+    case, g = plain_case
+    parts = torch.stack([torch.roll(g["particle"], shifts=(k, -k, 2 * k), dims=(0, 1, 2)) for k in range(5)])
+    weights = torch.stack([g["weight"] * (1.0 + 0.1 * k) for k in range(5)]).contiguous()
+    for bp in (None, weights[4].contiguous()):
+        qs, es = api.particle_spectra(parts.contiguous(), weights, bandpass=bp)
+        for k in range(5):
+            q1, e1 = api.particle_spectrum(parts[k].contiguous(), weights[k].contiguous(), bandpass=bp)
+            assert torch.equal(torch.view_as_real(qs[k]), torch.view_as_real(q1))
+            assert abs(es[k].item() - e1.item()) <= 1e-12 * abs(e1.item())
+    qn, en = api.particle_spectra(parts[:2].contiguous())
+    q0, e0 = api.particle_spectrum(parts[1].contiguous())
+    assert torch.equal(torch.view_as_real(qn[1]), torch.view_as_real(q0))
