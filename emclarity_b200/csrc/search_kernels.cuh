@@ -250,9 +250,11 @@ struct SearchCfg {
   // boxes, whose FFT codelets need more registers
   static constexpr int SMEM_CTAS_A = (int)((228 * 1024) / (SMEM_A + 1024));
   static constexpr int MINB_A = N <= 64 ? 0 : (SMEM_CTAS_A < 2 ? SMEM_CTAS_A : 2);
-  // pass B prefetches its particle-spectrum and weight slabs into shared memory where that still
-  // leaves four CTAs per SM (64^3); the larger boxes load them after the forward transform
-  static constexpr bool PREF_B = N <= 64;
+  // pass B prefetches its particle-spectrum and weight slabs into shared memory (64^3: four CTAs
+  // per SM; 96^3: the prefetch also frees the registers that held them, 68 instead of 105, so two
+  // CTAs fit instead of one); at 128^3 the slabs would leave shared memory for one CTA only and
+  // measured no faster, so they are loaded after the forward transform there
+  static constexpr bool PREF_B = N <= 96;
   static constexpr size_t SMEM_B =
       sizeof(float2) * ((size_t)PY * NH + N) + (PREF_B ? (sizeof(float2) + sizeof(float)) * (size_t)N * NH : 0);
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
