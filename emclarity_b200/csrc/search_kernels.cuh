@@ -250,13 +250,21 @@ struct SearchCfg {
   // boxes, whose FFT codelets need more registers
   static constexpr int SMEM_CTAS_A = (int)((228 * 1024) / (SMEM_A + 1024));
   static constexpr int MINB_A = N <= 64 ? 0 : (SMEM_CTAS_A < 2 ? SMEM_CTAS_A : 2);
-  // pass B prefetches its particle-spectrum and weight slabs into shared memory (64^3: four CTAs
-  // per SM; 96^3: the prefetch also frees the registers that held them, 68 instead of 105, so two
-  // CTAs fit instead of one); at 128^3 the slabs would leave shared memory for one CTA only and
-  // measured no faster, so they are loaded after the forward transform there
-  static constexpr bool PREF_B = N <= 96;
+  // Pass B: a CTA transforms the z lines of one ky and one of KS_B parts of the kx columns (NHB
+  // columns at most, tile pitch TPB odd so the spread of lines over banks stays a permutation).
+  // It prefetches its particle-spectrum and weight slabs into shared memory (64^3: four CTAs per
+  // SM; 96^3: the prefetch also frees the registers that held them, 68 instead of 105, so two
+  // CTAs fit instead of one).  128^3 splits the columns in two: with the whole ky row a CTA needed
+  // 544 threads and 95 registers (one CTA per SM, latency-bound); half rows fit two per SM.
+  static constexpr bool PREF_B = true;
+  static constexpr int KS_B = N >= 128 ? 2 : 1;
+  static constexpr int NHB = (NH + KS_B - 1) / KS_B;
+  static constexpr int TPB = NHB | 1;
+  static constexpr int NT_B = ((NHB * P + 31) / 32) * 32;
+  static constexpr int TEAMS_B = NT_B / P;
+  static constexpr int GRID_BX = N * KS_B;
   static constexpr size_t SMEM_B =
-      sizeof(float2) * ((size_t)PY * NH + N) + (PREF_B ? (sizeof(float2) + sizeof(float)) * (size_t)N * NH : 0);
+      sizeof(float2) * ((size_t)PY * TPB + N) + (PREF_B ? (sizeof(float2) + sizeof(float)) * (size_t)N * NHB : 0);
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
 };
 
@@ -295,7 +303,8 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
   using C = SearchCfg<N, GG>;
   constexpr int G = C::G, NT = C::NT_A, NH = C::NH;
   constexpr int SEG = N / 32;                     // row segments per lane
-  constexpr int RU = SEG >= 3 ? 1 : 4 / SEG;      // rows per warp per step: U = RU * SEG loads in flight
+  constexpr int RU = SEG >= 3 ? 2 : 4 / SEG;      // rows per warp per step: U = RU * SEG loads in flight
+  // (two rows at 96^3 / 128^3: 6 / 8 cells in flight; 128^3 pass A 149 us per 9 evaluations from 156)
   constexpr int U = RU * SEG;
   constexpr int WARPS = NT / 32;
   constexpr int ROWS = G * N;
@@ -494,35 +503,40 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
 
 // ------------------------------------------------------------------ pass B
 template <int N>
-__global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const SearchChunkArgs a,
-                                                                       const float2* __restrict__ g_tw) {
+__global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const SearchChunkArgs a,
+                                                                      const float2* __restrict__ g_tw) {
   using C = SearchCfg<N>;
-  constexpr int NH = C::NH, P = C::P;
+  constexpr int NH = C::NH, P = C::P, TPB = C::TPB, NT = C::NT_B;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tile = reinterpret_cast<float2*>(smem_raw);  // [PY][NH], row z at lpos<1>(z)
-  float2* s_tw = tile + (size_t)C::PY * NH;
+  float2* tile = reinterpret_cast<float2*>(smem_raw);  // [PY][TPB], row z at lpos<1>(z), local column
+  float2* s_tw = tile + (size_t)C::PY * TPB;
   __shared__ double red[32];
 
   const int e = blockIdx.y;
   if (e >= a.n_items) return;
-  const int ky = blockIdx.x;
+  const int ky = blockIdx.x / C::KS_B;
+  // this CTA's columns: kx in [k0, k0 + cnt); element i = z * NHB + local column (constant divisor),
+  // local columns >= cnt (the short last part) skipped
+  const int k0 = C::KS_B == 1 ? 0 : (int)(blockIdx.x % C::KS_B) * C::NHB;
+  const int cnt = C::KS_B == 1 ? NH : min(C::NHB, NH - k0);
+  constexpr int NB = C::NHB;
   const EvalItem it = a.items[e];
   const DevParticle& pt = a.parts[it.particle];
   const float* __restrict__ wref = a.refs[pt.ref].wref;
   const float2* __restrict__ q = pt.spec;
   const int w = 2 * a.radius + 1;
+  constexpr int IT = (N * NB + NT - 1) / NT;
 
-  // (PREF_B) this thread's elements i of the particle spectrum and of the reference weight at this
-  // ky, copied asynchronously while the slab loads and the forward transform run
-  float2* s_q = s_tw + N;                                  // [N * NH]
-  float* s_w = reinterpret_cast<float*>(s_q + N * NH);     // [N * NH]
+  // (PREF_B) this thread's elements i of the particle spectrum and of the reference weight,
+  // copied asynchronously while the slab loads and the forward transform run
+  float2* s_q = s_tw + N;                                     // [N * NHB]
+  float* s_w = reinterpret_cast<float*>(s_q + N * C::NHB);    // [N * NHB]
   if constexpr (C::PREF_B) {
-    constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * C::NT_BC;
-      if (i < N * NH) {
-        const size_t gi = ((size_t)(i / NH) * N + ky) * NH + i % NH;
+      const int i = threadIdx.x + k * NT;
+      if (i < N * NB && i % NB < cnt) {
+        const size_t gi = ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB;
         cp_async8(s_q + i, q + gi);
         if (wref) cp_async4(s_w + i, wref + gi);
       }
@@ -530,50 +544,50 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
     cp_async_commit();
   }
   load_twiddles<N>(s_tw, g_tw);
-  const float2* src = a.s1 + (size_t)e * N * N * NH + (size_t)ky * NH;
+  const float2* src = a.s1 + (size_t)e * N * N * NH + (size_t)ky * NH + k0;
   {
     // all of a thread's loads in flight before the first shared-memory store
-    constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
     float2 v[IT];
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * C::NT_BC;
-      if (i < N * NH) v[k] = src[(size_t)(i / NH) * N * NH + i % NH];
+      const int i = threadIdx.x + k * NT;
+      if (i < N * NB && i % NB < cnt) v[k] = src[(size_t)(i / NB) * N * NH + i % NB];
     }
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * C::NT_BC;
-      if (i < N * NH) tile[lpos<1>(i / NH) * NH + i % NH] = v[k];
+      const int i = threadIdx.x + k * NT;
+      if (i < N * NB && i % NB < cnt) tile[lpos<1>(i / NB) * TPB + i % NB] = v[k];
     }
   }
   __syncthreads();
+  // lines li in [0, TPB) -> local column (8 li) mod TPB (a permutation: TPB is odd), which puts the
+  // teams of a warp on different banks; columns >= cnt are idle
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
-  for (int base = 0; base < NH; base += C::TEAMS_BC) {
+  for (int base = 0; base < TPB; base += C::TEAMS_B) {
     const int li = base + team;
-    const int kx = li < NH ? spread_kx<NH>(li) : 0;
-    fft_line<N, -1, P, 1>(tile + kx, NH, lane, s_tw, li < NH);
+    const int kl = li < TPB ? (li * 8) % TPB : 0;
+    fft_line<N, -1, P, 1>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt);
   }
   __syncthreads();
   double en = 0.0;
   {
-    constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
     float2 qv[C::PREF_B ? 1 : IT];
     if constexpr (C::PREF_B) {
       cp_async_wait<0>();  // this thread's own copies; no other thread reads them
     } else {
 #pragma unroll
       for (int k = 0; k < IT; ++k) {
-        const int i = threadIdx.x + k * C::NT_BC;
-        if (i < N * NH) qv[k] = __ldg(q + ((size_t)(i / NH) * N + ky) * NH + i % NH);
+        const int i = threadIdx.x + k * NT;
+        if (i < N * NB && i % NB < cnt) qv[k] = __ldg(q + ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB);
       }
     }
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * C::NT_BC;
-      if (i >= N * NH) continue;
-      const int z = i / NH, kx = i % NH;
+      const int i = threadIdx.x + k * NT;
+      if (i >= N * NB || i % NB >= cnt) continue;
+      const int z = i / NB, kl = i % NB, kx = k0 + kl;
       const size_t gi = ((size_t)z * N + ky) * NH + kx;
-      float2& slot = tile[lpos<1>(z) * NH + kx];
+      float2& slot = tile[lpos<1>(z) * TPB + kl];
       float2 r = slot;
       if (wref) {
         const float wv = C::PREF_B ? s_w[i] : __ldg(wref + gi);
@@ -591,17 +605,18 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_z_mul(const Sear
     if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
   }
   __syncthreads();
-  for (int base = 0; base < NH; base += C::TEAMS_BC) {
+  for (int base = 0; base < TPB; base += C::TEAMS_B) {
     const int li = base + team;
-    const int kx = li < NH ? spread_kx<NH>(li) : 0;
-    fft_line<N, 1, P, 1>(tile + kx, NH, lane, s_tw, li < NH);
+    const int kl = li < TPB ? (li * 8) % TPB : 0;
+    fft_line<N, 1, P, 1>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt);
   }
   __syncthreads();
-  float2* dst = a.s2 + (size_t)e * w * N * NH + (size_t)ky * NH;
-  for (int i = threadIdx.x; i < w * NH; i += C::NT_BC) {
-    const int j = i / NH, kx = i % NH;
+  float2* dst = a.s2 + (size_t)e * w * N * NH + (size_t)ky * NH + k0;
+  for (int i = threadIdx.x; i < w * NB; i += NT) {
+    const int j = i / NB, kl = i % NB;
+    if (kl >= cnt) continue;
     const int z = (j - a.radius + N) % N;
-    dst[(size_t)j * N * NH + kx] = tile[lpos<1>(z) * NH + kx];
+    dst[(size_t)j * N * NH + kl] = tile[lpos<1>(z) * TPB + kl];
   }
 }
 
