@@ -621,8 +621,10 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const Searc
 }
 
 // ------------------------------------------------------------------ pass C
+// 64^3: 4 resident CTAs per SM asked of the compiler (56 registers, no spill; 68 before): a chunk's
+// 990 CTAs then take two waves instead of three (22.0 us per chunk from 24.6)
 template <int N>
-__global__ void __launch_bounds__(SearchCfg<N>::NT_BC) k_search_inv_peak(const SearchChunkArgs a,
+__global__ void __launch_bounds__(SearchCfg<N>::NT_BC, N <= 64 ? 4 : 0) k_search_inv_peak(const SearchChunkArgs a,
                                                                           const float2* __restrict__ g_tw) {
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, P = C::P;
