@@ -284,9 +284,13 @@ struct emc_search_s {
   emc::DevBuf<double> d_dmat;
   int norient = 0;
   int radius = 0, interp = EMC_INTERP_LINEAR, chunk_evals = 0;
-  // S1 + S2 scratch of a chunk, sized to about two thirds of the L2 (86 MB of 126 MB: 64 evaluations at
-  // 64^3, radius 7) so that pass B finds pass A's slabs in L2; set at creation from the device's L2
-  size_t scratch_budget = 86ull << 20;
+  // S1 + S2 scratch of a chunk: 768 MiB (about 600 evaluations at 64^3, 190 at 96^3, 84 at 128^3 with
+  // radius 7), or an eighth of the free device memory if that is less.  Measured: evaluations/s rise
+  // with the chunk until about this size (64^3: 370 k at 66 evaluations, the two-thirds-of-L2
+  // sizing, 400 k at 592, 403 k at 888; 96^3: 80 k at 21, 88 k at 168; 128^3: 31 k at 9, 34 k at
+  // 72): larger chunks amortise the passes' launch tails, and the slabs that then spill from L2
+  // cost HBM bandwidth the passes leave unused
+  size_t scratch_budget = 768ull << 20;
 
   emc::DevBuf<emc::DevParticle> d_parts;
   emc::DevBuf<emc::EvalItem> d_items;
@@ -342,10 +346,9 @@ emc_status emc_search_create(emc_search_t* out) {
   emc_search_s* s = new (std::nothrow) emc_search_s();
   EMC_CHECK_ARG(s, "emc_search_create: host allocation failed");
   {
-    int dev = 0, l2 = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) == cudaSuccess &&
-        l2 > 0)
-      s->scratch_budget = (size_t)l2 / 3 * 2;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b / 8 < s->scratch_budget)
+      s->scratch_budget = std::max<size_t>(free_b / 8, 16ull << 20);
   }
   if (cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete s;
