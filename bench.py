@@ -321,13 +321,13 @@ def L_call_spectrum(api, part, w, q, e):
 
 
 def profiled_traffic():
-    """DRAM bytes per pipeline launch from the committed ncu summary (None if absent)."""
+    """DRAM bytes per CC evaluation from the committed ncu summary (None if absent)."""
     p = os.path.join(ROOT, "profiles", "search_batched64_passes.md")
     try:
         with open(p) as f:
             for line in f:
-                if line.startswith("traffic_bytes_per_pipeline_launch:"):
-                    return int(line.split(":")[1])
+                if line.startswith("traffic_bytes_per_evaluation:"):
+                    return float(line.split(":")[1])
     except (OSError, ValueError):
         pass
     return None
@@ -345,12 +345,14 @@ def roofline(prof):
     total = sum(prof["ms"].values())
     for k in passes:
         passes[k]["share"] = prof["ms"][k] / total if total else None
-    traffic = profiled_traffic()
+    per_eval = profiled_traffic()
+    traffic = per_eval * evals_per_launch if per_eval else None
     return ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
              "peak_source": which + " (MEASURED_PEAKS.json hbm_gbs)" if which == "measured" else which,
              "traffic": traffic, "traffic_algorithmic": b,
-             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, --cache-control none, bytes per "
-                               "pipeline launch (profiles/search_batched64_passes.md)" if traffic else None,
+             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, --cache-control none, per CC "
+                               "evaluation of a full chunk (profiles/search_batched64_passes.md) x evaluations per "
+                               "launch" if traffic else None,
              "kernel": "fused search pipeline (fwd_xy + z_mul + inv_peak per chunk)",
              "algorithmic_bytes_per_eval": bytes_per_eval(BOX), "evals_per_launch": evals_per_launch,
              "us_per_launch": per_launch_ms * 1e3}, passes)
