@@ -15,7 +15,8 @@
 // bricks per CTA, 4x4x2 voxel tiles per warp, FP64 statistics per particle reduced with one atomic
 // per block), a per-particle kernel turns the statistics into (mean, rms, keep), and an
 // output-stationary pass adds the batch to the half-set sums voxel by voxel in the reference's
-// particle order (so the FP32 sums round the same way whatever the batch split).  No atomics touch the sums: results are deterministic.
+// particle order (so the FP32 sums round the same way whatever the batch split).  No atomics touch
+// the sums: results are deterministic.
 #include <algorithm>
 #include <cmath>
 #include <new>
@@ -167,6 +168,23 @@ __global__ void __launch_bounds__(256) k_avg_rotate(const float* __restrict__ vo
   }
 }
 
+// Copies a batch's parameters from the mapped host staging into device memory (the symmetry
+// matrices of each particle, its AvgParticle record and its wedge index).
+__global__ void k_avg_stage_in(const float* __restrict__ mats_h, const AvgParticle* __restrict__ parts_h,
+                               const int* __restrict__ widx_h, int nb, int nsym, float* __restrict__ mats,
+                               AvgParticle* __restrict__ parts, int* __restrict__ widx) {
+  const int per = 9 * nsym;
+  const long total = (long)nb * per;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long i = t / per, r = t % per;
+    mats[i * kAvgMaxSym * 9 + r] = mats_h[i * kAvgMaxSym * 9 + r];
+  }
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nb; i += (long)gridDim.x * blockDim.x) {
+    parts[i] = parts_h[i];
+    widx[i] = widx_h[i];
+  }
+}
+
 // mean / rms inside the binary mask and the finite check of mean(r_normalised(:)); counts the
 // kept particles of each half set.
 __global__ void k_avg_coef(const AvgStats* __restrict__ stats, const AvgParticle* __restrict__ parts, int count,
@@ -297,6 +315,11 @@ struct emc_average_s {
   emc::AvgCoef* coef = nullptr;
   int* kept = nullptr;
   int* widx = nullptr;
+  // Per-batch parameters (mats, parts, widx, in that order) staged in pinned host memory mapped into
+  // the device's address space: a kernel pulls them into mats / parts / widx over PCIe, so they take
+  // no copy-engine slot behind a caller's large host-to-device copy on another stream.
+  unsigned char* h_stage = nullptr;
+  const unsigned char* d_stage = nullptr;
 };
 
 namespace {
@@ -316,6 +339,11 @@ void avg_free(emc_average_s* a) {
   cudaFree(a->coef);
   cudaFree(a->kept);
   cudaFree(a->widx);
+  if (a->h_stage) cudaFreeHost(a->h_stage);
+}
+
+size_t stage_bytes(int batch) {
+  return (sizeof(float) * 9 * emc::kAvgMaxSym + sizeof(emc::AvgParticle) + sizeof(int)) * (size_t)batch;
 }
 
 int grid_for(long n) { return (int)std::max<long>(1, std::min<long>((n + 255) / 256, 8L * emc::device_sm_count())); }
@@ -371,6 +399,15 @@ emc_status emc_average_create(int n, const float* d_mask, float bin_threshold, i
   alloc((void**)&a->coef, sizeof(emc::AvgCoef) * a->batch);
   alloc((void**)&a->kept, sizeof(int) * a->batch);
   alloc((void**)&a->widx, sizeof(int) * a->batch);
+  if (rs == EMC_OK) {
+    void* dp = nullptr;
+    if (cudaHostAlloc((void**)&a->h_stage, stage_bytes(a->batch), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer(&dp, a->h_stage, 0) != cudaSuccess) {
+      emc::set_error("emc_average_create: mapped host staging (%zu bytes) failed", stage_bytes(a->batch));
+      rs = EMC_E_OOM;
+    }
+    a->d_stage = reinterpret_cast<const unsigned char*>(dp);
+  }
   double* d_ms = nullptr;
   alloc((void**)&d_ms, 2 * sizeof(double));
   if (rs == EMC_OK) {
@@ -432,9 +469,16 @@ emc_status emc_average_add(emc_average_t a, const float* d_particles, int count,
                     wedge_index[p]);
   }
   cudaStream_t st = emc::as_stream(stream);
-  std::vector<float> mats((size_t)a->batch * emc::kAvgMaxSym * 9, 0.f);
-  std::vector<emc::AvgParticle> parts(a->batch);
-  std::vector<int> widx(a->batch);
+  // host views of the mapped staging (every batch ends with a stream synchronisation, so the
+  // device has read a batch's parameters before the next batch overwrites them)
+  float* mats = reinterpret_cast<float*>(a->h_stage);
+  emc::AvgParticle* parts = reinterpret_cast<emc::AvgParticle*>(a->h_stage + sizeof(float) * 9 * emc::kAvgMaxSym *
+                                                                                (size_t)a->batch);
+  int* widx = reinterpret_cast<int*>(parts + a->batch);
+  const float* d_mats_h = reinterpret_cast<const float*>(a->d_stage);
+  const emc::AvgParticle* d_parts_h = reinterpret_cast<const emc::AvgParticle*>(
+      a->d_stage + sizeof(float) * 9 * emc::kAvgMaxSym * (size_t)a->batch);
+  const int* d_widx_h = reinterpret_cast<const int*>(d_parts_h + a->batch);
   std::vector<int> kept_h(a->batch);
   for (int b0 = 0; b0 < count; b0 += a->batch) {
     const int nb = std::min(a->batch, count - b0);
@@ -443,7 +487,7 @@ emc_status emc_average_add(emc_average_t a, const float* d_particles, int count,
       const double* A = rot + 9 * (size_t)p;  // column-major 3x3
       for (int k = 0; k < a->nsym; ++k) {
         const double* S = a->sym.data() + 9 * k;
-        float* m = mats.data() + ((size_t)i * emc::kAvgMaxSym + k) * 9;
+        float* m = mats + ((size_t)i * emc::kAvgMaxSym + k) * 9;
         // row r of A * S (column-major product)
         for (int r = 0; r < 3; ++r)
           for (int cidx = 0; cidx < 3; ++cidx) {
@@ -461,10 +505,9 @@ emc_status emc_average_add(emc_average_t a, const float* d_particles, int count,
       pr.pad = 0;
       widx[i] = pr.wedge;
     }
-    EMC_CUDA(cudaMemcpyAsync(a->mats, mats.data(), sizeof(float) * 9 * emc::kAvgMaxSym * nb, cudaMemcpyHostToDevice,
-                             st));
-    EMC_CUDA(cudaMemcpyAsync(a->parts, parts.data(), sizeof(emc::AvgParticle) * nb, cudaMemcpyHostToDevice, st));
-    if (a->nw) EMC_CUDA(cudaMemcpyAsync(a->widx, widx.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st));
+    emc::k_avg_stage_in<<<64, 256, 0, st>>>(d_mats_h, d_parts_h, d_widx_h, nb, a->nsym, a->mats, a->parts,
+                                             a->widx);
+    EMC_LAUNCH_CHECK();
     EMC_CUDA(cudaMemsetAsync(a->stats, 0, sizeof(emc::AvgStats) * nb, st));
     const int bricks = ((a->n + emc::kBrick - 1) / emc::kBrick) * ((a->n + emc::kBrick - 1) / emc::kBrick) *
                        ((a->n + emc::kBrick - 1) / emc::kBrick);
