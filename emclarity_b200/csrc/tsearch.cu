@@ -184,7 +184,18 @@ __global__ void __launch_bounds__(P * TT, zfused_min_blocks(L, P, TT)) k_ts_zfus
   }
 }
 
-// Last inverse pass (C2R along x) fused with the std normalisation and the MIP update.
+// Last inverse pass (C2R along x) fused with the std normalisation and the MIP update.  Each team
+// (one warp at L = 512) walks its row pairs with the next pair's two spectrum rows copied into a
+// second shared buffer (cp.async) while the current pair is transformed, and issues the current
+// maxima's loads before its transform, so neither load waits in front of the arithmetic.
+template <int L, int P>
+struct C2rMipSmem {
+  static constexpr int TEAMS = rows_teams(L, P);
+  static constexpr int LH = L / 2 + 1;
+  static constexpr size_t bytes =
+      sizeof(float2) * ((size_t)L + (size_t)TEAMS * row_line_len(L) + 2 * (size_t)TEAMS * 2 * LH);
+};
+
 template <int L, int P>
 __global__ void __launch_bounds__(256) k_ts_c2r_mip(const float2* __restrict__ in, long nrows,
                                                     const double* __restrict__ stats, long nvox, float angle_id,
@@ -193,8 +204,11 @@ __global__ void __launch_bounds__(256) k_ts_c2r_mip(const float2* __restrict__ i
   constexpr int TEAMS = rows_teams(L, P);
   constexpr int PAD = line_pad(L);
   constexpr int LH = L / 2 + 1;
-  __shared__ float2 s_tw[L];
-  __shared__ float2 s_line[TEAMS][row_line_len(L)];
+  constexpr int RLL = row_line_len(L);
+  extern __shared__ float2 c2r_smem[];
+  float2* s_tw = c2r_smem;
+  float2* s_lines = s_tw + L;                  // [TEAMS][RLL]
+  float2* s_spec = s_lines + TEAMS * RLL;      // [2][TEAMS][2 * LH]: rows a, b of a pair
   load_twiddles<L>(s_tw, g_tw);
   // map statistics from the spectrum: mean = X(0), sum m^2 = nvox * sum_full |X|^2
   const double mean = stats[1];
@@ -203,14 +217,40 @@ __global__ void __launch_bounds__(256) k_ts_c2r_mip(const float2* __restrict__ i
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
   const long npairs = (nrows + 1) / 2;
-  for (long pair0 = (long)blockIdx.x * TEAMS; pair0 < npairs; pair0 += (long)gridDim.x * TEAMS) {
+  const long stride = (long)gridDim.x * TEAMS;
+  float2* buf = s_lines + team * RLL;
+  // rows 2 pair, 2 pair + 1 of the spectrum into sb (one commit group per call, possibly empty)
+  auto prefetch = [&](long pair, float2* sb) {
+    if (pair < npairs) {
+      const long ra = 2 * pair, rb = 2 * pair + 1;
+      for (int k = lane; k < LH; k += P) {
+        cp_async8(sb + k, in + ra * LH + k);
+        if (rb < nrows) cp_async8(sb + LH + k, in + rb * LH + k);
+      }
+    }
+    cp_async_commit();
+  };
+  int cur = 0;
+  prefetch((long)blockIdx.x * TEAMS + team, s_spec + (size_t)team * 2 * LH);
+  for (long pair0 = (long)blockIdx.x * TEAMS; pair0 < npairs; pair0 += stride) {
     const long pair = pair0 + team;
     const bool active = pair < npairs;
     const long ra = 2 * pair, rb = 2 * pair + 1;
     const bool has_b = rb < nrows;
-    float2* buf = s_line[team];
-    const float2* a = in + ra * LH;
-    const float2* b = in + rb * LH;
+    prefetch(pair + stride, s_spec + ((size_t)(cur ^ 1) * TEAMS + team) * 2 * LH);
+    // the current maxima of both rows, in flight during the transform
+    constexpr int NE = (L + P - 1) / P;
+    float pa[NE], pb[NE];
+#pragma unroll
+    for (int k = 0; k < NE; ++k) {
+      const int n = lane + k * P;
+      pa[k] = (active && n < L) ? peak[ra * L + n] : 0.f;
+      pb[k] = (active && has_b && n < L) ? peak[rb * L + n] : 0.f;
+    }
+    cp_async_wait<1>();  // this pair's rows (the next pair's may still be in flight)
+    __syncwarp();
+    const float2* a = s_spec + ((size_t)cur * TEAMS + team) * 2 * LH;
+    const float2* b = a + LH;
     // Hermitian extension of rows a and b packed as a + i b
     fft_line_in<L, 1, P, PAD>(
         [&](int n) {
@@ -224,15 +264,6 @@ __global__ void __launch_bounds__(256) k_ts_c2r_mip(const float2* __restrict__ i
         },
         buf, 1, lane, s_tw, active);
     if (active) {
-      // the current maxima of both rows first (all loads in flight), then compare and update
-      constexpr int NE = (L + P - 1) / P;
-      float pa[NE], pb[NE];
-#pragma unroll
-      for (int k = 0; k < NE; ++k) {
-        const int n = lane + k * P;
-        pa[k] = n < L ? peak[ra * L + n] : 0.f;
-        pb[k] = (has_b && n < L) ? peak[rb * L + n] : 0.f;
-      }
 #pragma unroll
       for (int k = 0; k < NE; ++k) {
         const int n = lane + k * P;
@@ -246,8 +277,10 @@ __global__ void __launch_bounds__(256) k_ts_c2r_mip(const float2* __restrict__ i
         }
       }
     }
-    __syncwarp();
+    __syncwarp();  // this pair's spectrum rows have been read; the next prefetch reuses the buffer
+    cur ^= 1;
   }
+  cp_async_wait<0>();
 }
 
 __global__ void k_ts_init(float* __restrict__ peak, float* __restrict__ angle, long n) {
@@ -274,8 +307,17 @@ static emc_status launch_c2r_mip(const float2* in, long nrows, const double* sta
   const float2* tw = device_twiddles(L);
   if (!tw) return EMC_E_CUDA;
   const long npairs = (nrows + 1) / 2;
+  constexpr size_t smem = C2rMipSmem<L, P>::bytes;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64) return EMC_E_CUDA;
+  if (smem > 48 * 1024 && !attr_set[dev]) {
+    EMC_CUDA(cudaFuncSetAttribute(k_ts_c2r_mip<L, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[dev] = true;
+  }
   const int grid = (int)std::max(1L, std::min((npairs + TEAMS - 1) / TEAMS, 8L * device_sm_count()));
-  k_ts_c2r_mip<L, P><<<grid, TEAMS * P, 0, st>>>(in, nrows, stats, nvox, angle_id, peak, angle, tw);
+  k_ts_c2r_mip<L, P><<<grid, TEAMS * P, smem, st>>>(in, nrows, stats, nvox, angle_id, peak, angle, tw);
   EMC_LAUNCH_CHECK();
   return EMC_OK;
 }
