@@ -276,6 +276,19 @@ __device__ __forceinline__ int spread_kx(int li) {
   return (li * 8) % NH;
 }
 
+// Column of line li of a strided-FFT round over `cols` columns of a tile whose row pitch is 1 (mod
+// 16) float2, for teams of 8 lanes: the two teams of a half-warp (lines 2p, 2p+1) get columns 8
+// apart, so their accesses (8 lanes each on 8 consecutive banks of the line's rows) fall on
+// complementary bank halves in every Stockham stage.  Columns past the last complete block of 16
+// keep their own index.  (8 li mod cols put some half-warp pairs 7 or 9 banks apart: 1.33 times
+// the conflict-free wavefronts in pass B's z transforms at 64^3.)
+__device__ __forceinline__ int pair_spread(int li, int cols) {
+  const int full = (cols >> 4) << 4;
+  if (li >= full) return li;
+  const int p = li >> 1;
+  return ((p >> 3) << 4) + (p & 7) + ((li & 1) << 3);
+}
+
 template <typename Tv>
 __device__ __forceinline__ Tv block_sum(Tv v, Tv* red) {
 #pragma unroll
@@ -565,7 +578,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const Searc
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
   for (int base = 0; base < TPB; base += C::TEAMS_B) {
     const int li = base + team;
-    const int kl = li < TPB ? (li * 8) % TPB : 0;
+    const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
     fft_line<N, -1, P, 1>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt);
   }
   __syncthreads();
@@ -607,7 +620,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const Searc
   __syncthreads();
   for (int base = 0; base < TPB; base += C::TEAMS_B) {
     const int li = base + team;
-    const int kl = li < TPB ? (li * 8) % TPB : 0;
+    const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
     fft_line<N, 1, P, 1>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt);
   }
   __syncthreads();
@@ -666,7 +679,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC, N <= 64 ? 4 : 0) k_search
   tc.init(s_tw, lane);
   for (int base = 0; base < NH; base += C::TEAMS_BC) {
     const int li = base + team;
-    const int kx = li < NH ? spread_kx<NH>(li) : 0;
+    const int kx = li < NH ? (P == 8 ? pair_spread(li, NH) : spread_kx<NH>(li)) : 0;
     fft_line<N, 1, P, 1>(tile + kx, NH, lane, s_tw, li < NH, &tc);
   }
   __syncthreads();
