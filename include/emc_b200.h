@@ -233,7 +233,7 @@ EMC_API emc_status emc_particle_spectrum(int n, const float* d_particle, const f
  * d_weights [count][(n/2+1)*n*n] or NULL, d_bandpass one shared half spectrum or NULL,
  * d_spectra_out [count][(n/2+1)*n*n] complex, d_energies [count].  The per-particle loop of
  * BH_alignRaw3d_v2.m:1089-1100 (particle weight, BH_bandLimitCenterNormalize) batched; each
- * particle's result equals emc_particle_spectrum's. */
+ * particle's result equals emc_particle_spectrum's.  At most 65535 particles per call. */
 EMC_API emc_status emc_particle_spectra(int n, int count, const float* d_particles,
                                 const float* d_weights, const float* d_bandpass,
                                 float* d_spectra_out, double* d_energies, void* stream);
