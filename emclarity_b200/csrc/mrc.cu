@@ -255,13 +255,37 @@ __global__ void __launch_bounds__(256) k_extract(const float* __restrict__ vol, 
   // the valid x range of every row of this window
   const long x_top = a.vx - sx;
   const int x_lo = sx < 0 ? -sx : 0, x_hi = x_top < a.w[0] ? (int)x_top : a.w[0];
-  for (long row = warp; row < nrows; row += nwarps) {
-    const int j = (int)(row % a.w[1]), k = (int)(row / a.w[1]);
-    const long gy = sy + j, gz = sz + k;
-    float* d = dst + row * a.w[0];
-    const bool in_yz = gy >= 0 && gz >= 0 && gy < a.vy && gz < a.vz;
-    const long base = (gz * a.vy + gy) * a.vx + sx;  // dereferenced only for in-volume voxels
-    for (int i = lane; i < a.w[0]; i += 32) d[i] = (in_yz && i >= x_lo && i < x_hi) ? __ldg(vol + base + i) : 0.f;
+  // RB rows per warp and step, every load of the step issued before its stores (a 64-voxel row is
+  // only two loads per lane: one row at a time left the copy latency-bound)
+  constexpr int RB = 8;
+  for (long row0 = warp * RB; row0 < nrows; row0 += nwarps * RB) {
+    for (int i0 = 0; i0 < a.w[0]; i0 += 64) {
+      float v[RB][2];
+#pragma unroll
+      for (int q = 0; q < RB; ++q) {
+        const long row = row0 + q;
+        const int j = (int)(row % a.w[1]), k = (int)(row / a.w[1]);
+        const long gy = sy + j, gz = sz + k;
+        const bool in_yz = row < nrows && gy >= 0 && gz >= 0 && gy < a.vy && gz < a.vz;
+        const long base = (gz * a.vy + gy) * a.vx + sx;  // dereferenced only for in-volume voxels
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int i = i0 + lane + 32 * h;
+          v[q][h] = (in_yz && i >= x_lo && i < x_hi) ? __ldg(vol + base + i) : 0.f;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < RB; ++q) {
+        const long row = row0 + q;
+        if (row >= nrows) break;
+        float* d = dst + row * a.w[0];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int i = i0 + lane + 32 * h;
+          if (i < a.w[0]) d[i] = v[q][h];
+        }
+      }
+    }
   }
 }
 
@@ -552,7 +576,7 @@ emc_status emc_extract_windows(const float* d_vol, int nx, int ny, int nz, const
     for (int d = 0; d < 3; ++d) a.w[d] = window_size[d];
     const long nw = (long)window_size[0] * window_size[1] * window_size[2];
     const long nrows = (long)window_size[1] * window_size[2];
-    const int gx = (int)std::max<long>(1, std::min<long>((nrows + 7) / 8, 64));  // 8 warps (rows) per block
+    const int gx = (int)std::max<long>(1, std::min<long>((nrows + 63) / 64, 64));  // 8 warps x 8 rows per block
     for (int p0 = 0; p0 < count && rs == EMC_OK; p0 += 65535) {
       const int cnt = std::min(65535, count - p0);
       emc::k_extract<<<dim3(gx, cnt), 256, 0, st>>>(d_vol, a, d_start + 3 * (size_t)p0, d_out + (size_t)p0 * nw);
