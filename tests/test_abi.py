@@ -84,6 +84,18 @@ def test_null_arguments_are_rejected_before_any_device_work(built_lib):
     assert built_lib.emc_search_destroy(None) == 0
 
 
+def test_batched_spectra_and_device_energy_search_reject_bad_arguments(built_lib):
+    from emclarity_b200 import _lib
+    fake = C.c_void_p(256)  # never dereferenced: every case below fails its argument checks first
+    assert built_lib.emc_search_run_energies(None, None, 0, fake, None, None, None, None) == _lib.EMC_E_ARG
+    assert built_lib.emc_particle_spectra(64, 0, fake, None, None, fake, fake, None) == _lib.EMC_E_ARG
+    assert built_lib.emc_particle_spectra(64, 4, None, None, None, fake, fake, None) == _lib.EMC_E_ARG
+    assert built_lib.emc_particle_spectra(100, 4, fake, None, None, fake, fake, None) == _lib.EMC_E_ARG
+    assert b"not supported" in built_lib.emc_last_error()
+    assert built_lib.emc_particle_spectra(64, 70000, fake, None, None, fake, fake, None) == _lib.EMC_E_ARG
+    assert b"65535" in built_lib.emc_last_error()
+
+
 def test_status_strings(built_lib):
     for s in (0, -1, -2, -3, -4, -5):
         assert built_lib.emc_status_string(s)
