@@ -246,11 +246,12 @@ struct SearchCfg {
   static constexpr int TEAMS_LC = 16;  // (2 r + 1 + 1) / 2 <= 16 row pairs for r <= 15
   static constexpr size_t SMEM_A = sizeof(float2) * ((size_t)G * PY * NH + (size_t)TEAMS_LA * LP + N) + 64;
   // resident pass-A CTAs per SM that shared memory allows (228 KB per SM, 1 KB reserved per CTA),
-  // and the target the register budget is capped for: 5 at 64^3 (48 registers, a 12-byte spill;
-  // 863.7 us per 602-evaluation chunk against 875.2 at the compiler's 64 registers and 4 CTAs), 2
-  // for the larger boxes, whose FFT codelets need more registers
+  // and the target the register budget is capped for: 5 at 64^3 with one plane per CTA (48
+  // registers, a 12-byte spill; 863.7 us per 602-evaluation chunk against 875.2 at the compiler's
+  // 64 registers and 4 CTAs), none for the multi-plane 64^3 tilings, 2 for the larger boxes, whose
+  // FFT codelets need more registers
   static constexpr int SMEM_CTAS_A = (int)((228 * 1024) / (SMEM_A + 1024));
-  static constexpr int MINB_A = N <= 64 ? 5 : (SMEM_CTAS_A < 2 ? SMEM_CTAS_A : 2);
+  static constexpr int MINB_A = N <= 64 ? (G == 1 ? 5 : 0) : (SMEM_CTAS_A < 2 ? SMEM_CTAS_A : 2);
   // Pass B: a CTA transforms the z lines of one ky and one of KS_B parts of the kx columns (NHB
   // columns at most, tile pitch TPB odd so the spread of lines over banks stays a permutation).
   // It prefetches its particle-spectrum and weight slabs into shared memory (64^3: four CTAs per
