@@ -31,11 +31,29 @@ N_ORIENT = 256
 PEAK_RADIUS = 7
 
 
-def bytes_per_eval(n):
-    """Algorithmic bytes of one CC evaluation: rotated source (4 n^3) + particle spectrum
-    (8 nh n^2) + wedge.CTF weight (4 nh n^2) + 16 B result."""
+def particle_bytes(n):
+    """Per-particle input of the search: the particle spectrum (8 nh n^2) and its wedge.CTF weight
+    wdgMask (4 nh n^2), read by every orientation of the particle (from L2 after the first)."""
     nh = n // 2 + 1
-    return 4 * n ** 3 + 8 * nh * n * n + 4 * nh * n * n + 16
+    return 12 * nh * n * n
+
+
+def reference_bytes(n, store="f32"):
+    """Per-reference input: the trilinear corner cells ((n+1)^3 x 32 B FP32 / 16 B BF16) and the
+    real-space mask (4 n^3)."""
+    return (n + 1) ** 3 * (32 if store == "f32" else 16) + 4 * n ** 3
+
+
+def compulsory_bytes(n, evals, particles, references=1, store="f32"):
+    """Compulsory HBM bytes of a launch that evaluates `evals` (particle, orientation) pairs of
+    `particles` distinct particles: every input read once, 16 B written per evaluation."""
+    return particles * particle_bytes(n) + references * reference_bytes(n, store) + 16 * evals
+
+
+def bytes_per_eval(n):
+    """Compulsory bytes per CC evaluation with N_ORIENT orientations per particle, the reference's share
+    left out (it is read once per launch of hundreds of evaluations)."""
+    return particle_bytes(n) / N_ORIENT + 16
 
 
 def flops_per_eval(n):
@@ -176,13 +194,19 @@ def run_ours(args, world, rank, local):
     s.set_orientations(b["grid"])
     d_parts = b["parts"].cuda()
     d_w = b["weights"].cuda()
+    d_w2 = torch.empty_like(d_w)
     spec = torch.empty((n, BOX, BOX, BOX // 2 + 1), dtype=torch.complex64, device="cuda")
     energy = torch.zeros(n, dtype=torch.float64, device="cuda")
     for i in range(n):
-        L_call_spectrum(api, d_parts[i], d_w[i], spec[i], energy[i:i + 1])
+        L_call_spectrum(api, d_parts[i], None, spec[i], energy[i:i + 1])
     torch.cuda.synchronize()
     en = energy.cpu().numpy()
-    descs = [s.particle(spec[i], en[i], rid, prior=b["priors"][i], orient_count=N_ORIENT) for i in range(n)]
+    # each particle's wedge.CTF weight is the CC's wdgMask, applied to the rotated reference
+    # (BH_multi_xcf_Translational_2.m:35-38 with BH_multi_xcf_Rotational's binding)
+    descs = [s.particle(spec[i], en[i], rid, prior=b["priors"][i], orient_count=N_ORIENT, wedge=d_w[i])
+             for i in range(n)]
+    descs_b = [s.particle(spec[i], en[i], rid, prior=b["priors"][i], orient_count=N_ORIENT, wedge=d_w2[i])
+               for i in range(n)]
     evals = n * N_ORIENT
     cc = torch.empty(evals, device="cuda")
     best = torch.empty((n, 5), dtype=torch.int32, device="cuda")
@@ -228,7 +252,8 @@ def run_ours(args, world, rank, local):
     h_best = torch.empty((n, 5), dtype=torch.int32).pin_memory()
     h2d = b["parts"].numel() * 4 + b["weights"].numel() * 4
     d2h = h_best.numel() * 4
-    in_bufs = [(d_parts, d_w), (torch.empty_like(d_parts), torch.empty_like(d_w))]
+    in_bufs = [(d_parts, d_w), (torch.empty_like(d_parts), d_w2)]
+    slot_descs = [descs, descs_b]  # the search reads the weights of the buffer its step copied into
     copy_stream = torch.cuda.Stream()
     copied = [torch.cuda.Event(), torch.cuda.Event()]
     consumed = [torch.cuda.Event(), torch.cuda.Event()]
@@ -246,9 +271,9 @@ def run_ours(args, world, rank, local):
         slot = k % 2
         stream.wait_event(copied[slot])
         pa, wa = in_bufs[slot]
-        api.particle_spectra(pa, wa, out=spec, energies=energy)  # one batched call for the step
+        api.particle_spectra(pa, out=spec, energies=energy)  # one batched call for the step
+        s.run(slot_descs[slot], cc=cc, best=best, energies=energy)
         consumed[slot].record(stream)
-        s.run(descs, cc=cc, best=best, energies=energy)
         h_best.copy_(best, non_blocking=True)
 
     def e2e_steps(k_steps):
@@ -298,15 +323,16 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": world * evals / (e2e_ms / 1e3), "unit": "CC evals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
                 "path": "pinned host volumes + weights (copy stream, two device buffers) -> emc_particle_spectra "
-                        "-> emc_search_run_energies (energies read on the device) -> host hits; step k+1's copy "
-                        "overlaps step k's search; hits checked equal to the device-resident run"},
+                        "-> emc_search_run_energies (energies read on the device, the buffer's weights as "
+                        "wdgMask) -> host hits; step k+1's copy overlaps step k's search; hits checked equal to "
+                        "the device-resident run"},
         "gpu_launches": int(launches_per_step * args.steps),
         "plain": plain,
     }
-    res["roofline"], res["passes"] = roofline(prof)
+    res["clocks"] = clk.summary()
+    res["roofline"], res["passes"] = roofline(prof, res["clocks"])
     g, g_ms = s.planes(BOX)
     res["passes"]["fwd_xy"]["planes_per_cta"] = {"chosen": g, "tuning_ms_per_launch": g_ms}
-    res["clocks"] = clk.summary()
     return res
 
 
@@ -316,8 +342,8 @@ def L_call_spectrum(api, part, w, q, e):
 
     from emclarity_b200 import _lib as L
     n = part.shape[-1]
-    L.call("emc_particle_spectrum", n, C.c_void_p(part.data_ptr()), C.c_void_p(w.data_ptr()), None,
-           C.c_void_p(q.data_ptr()), C.c_void_p(e.data_ptr()), api._stream())
+    L.call("emc_particle_spectrum", n, C.c_void_p(part.data_ptr()), C.c_void_p(w.data_ptr()) if w is not None else None,
+           None, C.c_void_p(q.data_ptr()), C.c_void_p(e.data_ptr()), api._stream())
 
 
 def profiled_traffic():
@@ -333,12 +359,17 @@ def profiled_traffic():
     return None
 
 
-def roofline(prof):
+def roofline(prof, clocks=None):
+    """HBM roofline of the fused search on the compulsory-traffic model: per launch (one chunk of the
+    three passes) the distinct particles' spectra and weights, the reference's cells and mask, and
+    16 B per evaluation, over the measured per-launch device time.  The passes are bound on chip
+    (shared memory, L1, issue), so the FP32 rate of the nominal FFT flop count is reported beside it
+    against the nominal FP32 CUDA-core peak at the sampled SM clock."""
     peak, which = measured_peaks()
     nl = max(1, prof["launches"]["fwd_xy"])
     per_launch_ms = (prof["ms"]["fwd_xy"] + prof["ms"]["z_mul"] + prof["ms"]["inv_peak"]) / nl
     evals_per_launch = prof["evals"] / nl
-    b = bytes_per_eval(BOX) * evals_per_launch
+    b = compulsory_bytes(BOX, evals_per_launch, evals_per_launch / N_ORIENT + 1)
     achieved = b / (per_launch_ms / 1e3) / 1e9
     passes = {k: {"ms_total": v, "launches": prof["launches"][k],
                   "us_per_launch": 1e3 * v / max(1, prof["launches"][k])} for k, v in prof["ms"].items()}
@@ -347,15 +378,24 @@ def roofline(prof):
         passes[k]["share"] = prof["ms"][k] / total if total else None
     per_eval = profiled_traffic()
     traffic = per_eval * evals_per_launch if per_eval else None
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    fp32 = flops_per_eval(BOX) * evals_per_launch / (per_launch_ms / 1e3) / 1e12
     return ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
              "peak_source": which + " (MEASURED_PEAKS.json hbm_gbs)" if which == "measured" else which,
              "traffic": traffic, "traffic_algorithmic": b,
-             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, --cache-control none, per CC "
-                               "evaluation of a full chunk (profiles/search_batched64_passes.md) x evaluations per "
-                               "launch" if traffic else None,
+             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per CC evaluation of a full "
+                               "chunk (profiles/search_batched64_passes.md) x evaluations per launch"
+                               if traffic else None,
+             "model": "compulsory bytes per launch: distinct particles x (8 + 4) nh n^2 (spectrum + wdgMask) + "
+                      "reference cells (n+1)^3 x 32 + mask 4 n^3 + 16 B per evaluation",
              "kernel": "fused search pipeline (fwd_xy + z_mul + inv_peak per chunk)",
-             "algorithmic_bytes_per_eval": bytes_per_eval(BOX), "evals_per_launch": evals_per_launch,
-             "us_per_launch": per_launch_ms * 1e3}, passes)
+             "compulsory_bytes_per_eval": b / evals_per_launch, "evals_per_launch": evals_per_launch,
+             "us_per_launch": per_launch_ms * 1e3,
+             "compute": {"unit": "TFLOP/s", "achieved": fp32, "peak": fp32_peak, "frac": fp32 / fp32_peak,
+                         "flops_per_eval": flops_per_eval(BOX),
+                         "peak_source": "nominal FP32 CUDA-core peak: 148 SMs x 128 lanes x 2 x %.0f MHz" % mhz}},
+            passes)
 
 
 def run_plain(args, api):
@@ -365,11 +405,11 @@ def run_plain(args, api):
     from emclarity_b200 import synthetic
     case = synthetic.PlainCase(seed=11)
     g = case.to_gpu()
-    q, e = api.particle_spectrum(g["particle"], g["weight"])
+    q, e = api.particle_spectrum(g["particle"])
     s = api.Search(peak_radius=case.peak_radius)
     rid = s.add_reference(g["ref"], g["mask"])
     s.set_orientations(case.grid)
-    d = [s.particle(q, e.item(), rid, orient_count=len(case.grid))]
+    d = [s.particle(q, e.item(), rid, orient_count=len(case.grid), wedge=g["weight"])]
     best = torch.empty((1, 5), dtype=torch.int32, device="cuda")
     for _ in range(max(3, args.warmup)):
         s.run(d, best=best)
@@ -388,29 +428,73 @@ def run_plain(args, api):
 
 
 # ---------------------------------------------------------------------------------------------
-def cpu_port_rate(seconds=12.0, threads=None, orient_per_call=None):
-    """Single-precision CPU port of the reference path (interpn-linear rotate, FFT, normalised
-    xcf, masked argmax) on a bounded sample of the workload; OpenMP over orientations."""
+def _cpu_case():
+    """One 64^3 particle of the default workload's shape (reference, mask, particle spectrum,
+    wedge weight) and the local orientation grid, for the CPU arms."""
     from emclarity_b200 import synthetic
     from oracle import oracle as O
-    threads = threads or os.cpu_count() or 1
     rng = np.random.default_rng(5)
     ref = synthetic.blob_reference(rng, BOX)
     mask = synthetic.soft_sphere_mask(BOX, 28)
     part = (np.roll(ref, 2, axis=0) + rng.standard_normal(ref.shape)).astype(np.float32)
-    q, e = O.particle_spectrum(part, precision="f32")
+    q, _ = O.particle_spectrum(part, precision="f32")
+    wdg = O.even_weight_np(rng, BOX)[:, :, : BOX // 2 + 1].astype(np.float32)  # wdgMask operand
     grid = synthetic_local_grid_np()
     mats = [O.define_matrix([p, t, s - p], "inv") for p, t, s in grid]
-    per = orient_per_call or max(threads, 8)
+    return ref, mask, q, wdg, mats
+
+
+def cpu_rates(seconds=12.0):
+    """The two CPU arms of the baseline on a bounded sample of the workload (one 64^3 particle over the
+    local grid): the single-precision C port of the reference path (liboracle_f32.so, OpenMP over
+    orientations on every host core) and the numpy / scipy.fft (pocketfft) restatement in one spawned
+    process per host core.  Returns {arm: (evals/s, cores, sample description)} and the faster arm."""
+    from oracle import oracle as O
+    from oracle import pocketfft_arm as PF
+    cores = os.cpu_count() or 1
+    ref, mask, q, wdg, mats = _cpu_case()
+    out = {}
+    per = max(cores, 8)
+    O.search(ref, q, mats[:per], mask=mask, wdg_mask=wdg, radius=PEAK_RADIUS, nthreads=cores, precision="f32")
     done, t0 = 0, time.time()
-    while True:
+    while time.time() - t0 < seconds:
         sl = [mats[(done + k) % len(mats)] for k in range(per)]
-        O.search(ref, q, e, sl, mask=mask, radius=PEAK_RADIUS, nthreads=threads, precision="f32")
+        O.search(ref, q, sl, mask=mask, wdg_mask=wdg, radius=PEAK_RADIUS, nthreads=cores, precision="f32")
         done += per
-        if time.time() - t0 >= seconds:
-            break
     dt = time.time() - t0
-    return done / dt, threads, "%d CC evaluations of one 64^3 particle over the local grid in %.1f s" % (done, dt)
+    out["c_port"] = (done / dt, cores, "C port (FP32, OpenMP, %d threads): %d CC evaluations of one 64^3 particle "
+                                       "over the local grid in %.1f s" % (cores, done, dt))
+    with PF.Pool(ref, q, mask=mask, wdg_mask=wdg, radius=PEAK_RADIUS, processes=cores) as pool:
+        pool.search(mats[:2 * cores])  # workers started and warm
+        per = 4 * cores
+        done, t0 = 0, time.time()
+        while time.time() - t0 < seconds:
+            pool.search([mats[(done + k) % len(mats)] for k in range(per)])
+            done += per
+        dt = time.time() - t0
+    out["pocketfft"] = (done / dt, cores, "numpy + scipy.fft (pocketfft) in %d spawned processes: %d CC evaluations "
+                                          "of one 64^3 particle over the local grid in %.1f s" % (cores, done, dt))
+    best = max(out, key=lambda k: out[k][0])
+    return out, best
+
+
+def cpu_baseline_entry(seconds=12.0):
+    rates, best = cpu_rates(seconds)
+    r, cores, sample = rates[best]
+    return {"value": r, "unit": "CC evals/s", "cores": cores, "kind": "port", "arm": best, "sample": sample,
+            "cpu_model": _cpu_model(),
+            "arms": {k: {"value": v[0], "cores": v[1], "sample": v[2]} for k, v in rates.items()}}
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def synthetic_local_grid_np():
@@ -423,25 +507,30 @@ def synthetic_local_grid_np():
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the reference path's CPU implementation on the host cores.  The reference's
+    own CPU path is MATLAB (absent here), so each step times both CPU restatements of it (the C port
+    and the pocketfft arm) on a bounded sample of the workload and reports the faster."""
     if rank != 0:
         return None
-    rates = []
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        cpu_port_rate(seconds=2.0)
-    threads = os.cpu_count() or 1
-    per_step = max(2.0, min(20.0, 150.0 / max(1, args.steps)))
-    sample = None
+    per_step = max(2.0, min(10.0, 60.0 / max(1, args.steps)))
+    cpu_rates(seconds=1.0)  # warm-up
+    steps = []
     for _ in range(args.steps):
-        r, threads, sample = cpu_port_rate(seconds=per_step)
-        rates.append(r)
-    v = float(np.mean(rates))
+        rates, best = cpu_rates(seconds=per_step)
+        steps.append((rates, best))
+    arms = {k: float(np.mean([r[k][0] for r, _ in steps])) for k in steps[0][0]}
+    best = max(arms, key=arms.get)
+    v = arms[best]
+    cores = steps[-1][0][best][1]
     return {
         "metric": "CC evals/s at 64^3 (batched)", "value": v, "unit": "CC evals/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_step, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 2e3 * per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-        "config": {"workload": "batched alignment, 64^3 share (bounded CPU sample)", "box": BOX,
-                   "orientations": N_ORIENT, "peak_radius": PEAK_RADIUS},
-        "cpu_baseline": {"value": v, "unit": "CC evals/s", "cores": threads, "kind": "port", "sample": sample},
+        "config": {"workload": "batched alignment, 64^3 share (bounded CPU sample: one particle over the local "
+                               "grid per step, both CPU arms)", "box": BOX, "orientations": N_ORIENT,
+                   "peak_radius": PEAK_RADIUS},
+        "cpu_baseline": {"value": v, "unit": "CC evals/s", "cores": cores, "kind": "port", "arm": best,
+                         "sample": steps[-1][0][best][2], "cpu_model": _cpu_model(), "arms": arms},
         "e2e": {"value": v, "unit": "CC evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -483,10 +572,10 @@ def run_mixed(args, store="f32"):
         w = api.wedge_ctf_weight(int(n), -rng.uniform(50, 65), rng.uniform(50, 65),
                                  synthetic.ctf_dict(rng.uniform(15000, 40000)))
         p = synthetic.make_particle(refs[n][0], rng, truth, rng.integers(-4, 5, 3), w, 0.1, ft=fts[n])
-        q, e = api.particle_spectrum(p, w)
-        keep.append(q)
-        descs.append(s.particle(q, e.item(), refs[n][1], prior=prior, orient_count=N_ORIENT))
-        del p, w
+        q, e = api.particle_spectrum(p)
+        keep += [q, w]
+        descs.append(s.particle(q, e.item(), refs[n][1], prior=prior, orient_count=N_ORIENT, wedge=w))
+        del p
     evals = len(descs) * N_ORIENT
     best = torch.empty((len(descs), 5), dtype=torch.int32, device="cuda")
     for _ in range(args.warmup):
@@ -500,7 +589,7 @@ def run_mixed(args, store="f32"):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     counts = {int(n): int(np.sum(sizes == n)) for n in (64, 96, 128)}
-    byts = sum(bytes_per_eval(n) * c * N_ORIENT for n, c in counts.items())
+    byts = sum(compulsory_bytes(n, c * N_ORIENT, c, 1, store) for n, c in counts.items())
     peak, which = measured_peaks()
     return {"metric": "CC evals/s, batched uneven boxes" + (" (BF16 reference storage)" if store == "bf16" else ""),
             "value": evals / (ms / 1e3), "unit": "CC evals/s", "n_gpus": 1, "steps": args.steps,
@@ -865,24 +954,27 @@ def run_refine(args):
     dense = api.euler_search("C1", 8, 1, 8, 1)
     s = api.Search(peak_radius=6)
     rid = s.add_reference(rg, mg)
-    priors, truths, specs, hs, ens = [], [], [], [], []
+    priors, truths, specs, hs, ens, wedges = [], [], [], [], [], []
     for _ in range(n_part):
         prior = api.define_matrix(synthetic.random_euler(rng), "inv")
         jitter = _rodrigues(rng.standard_normal(3), rng.uniform(0, 12))
         truth = prior @ jitter
         w = api.wedge_ctf_weight(n, -60, 60, synthetic.ctf_dict(rng.uniform(15000, 40000)))
         p = synthetic.make_particle(rg, rng, truth, rng.integers(-3, 4, 3), w, 0.05, ft=ft)
-        q, e = api.particle_spectrum(p, w)
+        q, e = api.particle_spectrum(p)
         priors.append(prior)
         truths.append(truth)
         specs.append(q)
+        wedges.append(w)
         ens.append(e.item())
-        hs.append(api.particle_template(q))
+        # the adjoint's template h = F^-1(wdgMask .* P): its zero-lag numerator is the search's
+        hs.append(api.particle_template(api.particle_spectrum(p, w)[0]))
     truths = np.array(truths)
 
     def coarse_search():
         s.set_orientations(coarse)
-        d = [s.particle(specs[i], ens[i], rid, prior=priors[i], orient_count=len(coarse)) for i in range(n_part)]
+        d = [s.particle(specs[i], ens[i], rid, prior=priors[i], orient_count=len(coarse), wedge=wedges[i])
+             for i in range(n_part)]
         _, _, best = s.run_host(d)
         return best
 
@@ -914,7 +1006,8 @@ def run_refine(args):
     # (b) plain GPU grid search: dense 1-degree local grid around the coarse best
     def dense_search():
         s.set_orientations(dense)
-        d = [s.particle(specs[i], ens[i], rid, prior=R_coarse[i], orient_count=len(dense)) for i in range(n_part)]
+        d = [s.particle(specs[i], ens[i], rid, prior=R_coarse[i], orient_count=len(dense), wedge=wedges[i])
+             for i in range(n_part)]
         _, _, bd = s.run_host(d)
         return bd
 
@@ -967,9 +1060,7 @@ def main():
     res = run_ours(args, world, rank, local)
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
-            r, threads, sample = cpu_port_rate(seconds=12.0)
-            res["cpu_baseline"] = {"value": r, "unit": "CC evals/s", "cores": threads, "kind": "port",
-                                   "sample": sample}
+            res["cpu_baseline"] = cpu_baseline_entry(seconds=10.0)
         print(json.dumps(res))
     if world > 1:
         import torch.distributed as dist

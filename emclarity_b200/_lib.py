@@ -37,7 +37,7 @@ def _status_name(s):
 class ParticleDesc(C.Structure):
     _fields_ = [("spectrum", C.c_void_p), ("energy", C.c_double), ("prior", C.c_double * 9),
                 ("shift", C.c_float * 3), ("box", C.c_int), ("ref_id", C.c_int),
-                ("orient_begin", C.c_int), ("orient_count", C.c_int)]
+                ("orient_begin", C.c_int), ("orient_count", C.c_int), ("wedge", C.c_void_p)]
 
 
 class SearchHit(C.Structure):

@@ -289,9 +289,17 @@ class Search:
         self.n_orient = a.shape[0]
 
     @staticmethod
-    def particle(spectrum, energy, ref_id, prior=None, shift=(0, 0, 0), orient_begin=0, orient_count=0):
+    def particle(spectrum, energy, ref_id, prior=None, shift=(0, 0, 0), orient_begin=0, orient_count=0, wedge=None):
+        """Search item.  spectrum = refWdg .* B .* F(particle) (particle_spectrum with weight = refWdg) and
+        energy its sum |.|^2; wedge: wdgMask, the real half-spectrum weight applied to the rotated
+        reference (BH_multi_xcf_Translational_2.m:35-38), or None (= 1).  The tensors must stay alive
+        while the search runs."""
         d = L.ParticleDesc()
         d.spectrum = spectrum.data_ptr()
+        if wedge is not None:
+            if tuple(wedge.shape) != tuple(spectrum.shape):
+                raise ValueError("wedge must be a real half spectrum of the spectrum's shape")
+            d.wedge = _need_cuda(wedge, "wedge").value
         d.energy = float(energy)
         pr = np.eye(3) if prior is None else np.asarray(prior, dtype=np.float64).reshape(3, 3)
         d.prior[:] = list(pr.flatten(order="F"))

@@ -5,7 +5,8 @@
 // (box size, reference storage type) and cut into chunks whose on-chip-spilled scratch
 // (S1 + S2) stays inside a budget sized to the L2 cache; each chunk is four launches
 // (fwd_xy, z_mul, inv_peak, decode).  The whole launch sequence of a run is captured once
-// in a CUDA graph and replayed while the request (particles, outputs, settings) is unchanged.
+// in a CUDA graph; the graphs of the four most recent requests (particles, outputs, settings)
+// are kept, each with its own particle table, and replayed when a request repeats.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -292,8 +293,28 @@ struct emc_search_s {
   // cost HBM bandwidth the passes leave unused
   size_t scratch_budget = 768ull << 20;
 
-  emc::DevBuf<emc::DevParticle> d_parts;
-  emc::DevBuf<emc::EvalItem> d_items;
+  // Particle table and evaluation list of one recorded request.  Each cached graph reads its own
+  // (the graph replays kernels that read them), so alternating requests -- a double-buffered
+  // pipeline whose descriptors point at one of two input buffers -- replay instead of re-recording.
+  struct RunTables {
+    emc::DevBuf<emc::DevParticle> parts;
+    emc::DevBuf<emc::EvalItem> items;
+    void release() {
+      parts.release();
+      items.release();
+    }
+  };
+  struct GraphEntry {
+    std::vector<char> key;
+    cudaGraphExec_t exec = nullptr;
+    RunTables tables;
+    unsigned long long used = 0;
+  };
+  static constexpr size_t kGraphCache = 4;
+  std::vector<GraphEntry> graphs;  // least recently used evicted; capacity reserved at creation
+  unsigned long long use_clock = 0;
+  RunTables eager_tables;          // tables of profiled (eager, unrecorded) runs
+  RunTables* cur = nullptr;        // tables of the run being recorded or launched eagerly
   emc::DevBuf<emc::EvalResult> d_results;
   emc::DevBuf<unsigned long long> d_best_keys;
   emc::DevBuf<float2> s1, s2;
@@ -303,8 +324,6 @@ struct emc_search_s {
 
   const double* run_energy = nullptr;  // device energies of the run being recorded (or null)
   cudaStream_t cap_stream = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  std::vector<char> gkey;
   long last_launches = 0;
 
   // profiling: a ring of per-chunk event sets, harvested before reuse
@@ -337,6 +356,16 @@ int effective_radius(const emc_search_s* s, int n) {
   return std::min(r, n / 2 - 1);
 }
 
+// Forgets every recorded request (their graphs hold scratch pointers and read the orientation and
+// reference tables, so any change to those invalidates them).
+void drop_graphs(emc_search_s* s) {
+  for (auto& g : s->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.tables.release();
+  }
+  s->graphs.clear();
+}
+
 }  // namespace
 
 extern "C" {
@@ -350,6 +379,7 @@ emc_status emc_search_create(emc_search_t* out) {
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b / 8 < s->scratch_budget)
       s->scratch_budget = std::max<size_t>(free_b / 8, 16ull << 20);
   }
+  s->graphs.reserve(emc_search_s::kGraphCache);
   if (cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete s;
     emc::set_error("emc_search_create: stream creation failed");
@@ -415,7 +445,7 @@ emc_status emc_search_set_orientations(emc_search_t s, const double* ptp, int n)
   EMC_TRY(s->d_dmat.reserve(s->dmat.size()));
   EMC_CUDA(cudaMemcpy(s->d_dmat.p, s->dmat.data(), sizeof(double) * s->dmat.size(), cudaMemcpyHostToDevice));
   s->norient = n;
-  s->gkey.clear();  // invalidate the cached graph
+  drop_graphs(s);
   return EMC_OK;
 }
 
@@ -427,7 +457,7 @@ emc_status emc_search_configure(emc_search_t s, int peak_radius, int interp, int
   s->radius = peak_radius;
   s->interp = interp;
   s->chunk_evals = chunk_evals;
-  s->gkey.clear();
+  drop_graphs(s);
   return EMC_OK;
 }
 
@@ -446,8 +476,8 @@ static emc_status harvest_slot(emc_search_t s, int slot) {
 
 static emc::SearchChunkArgs chunk_args(emc_search_t s, const Chunk& c) {
   emc::SearchChunkArgs a;
-  a.items = s->d_items.p + c.item_offset;
-  a.parts = s->d_parts.p;
+  a.items = s->cur->items.p + c.item_offset;
+  a.parts = s->cur->parts.p;
   a.refs = s->d_refs.p;
   a.dmat = s->d_dmat.p;
   a.s1 = s->s1.p;
@@ -519,7 +549,7 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
   EMC_CUDA(cudaMemsetAsync(s->done.p, 0, sizeof(unsigned) * s->done.cap, st));
   long launches = 0;
   if (s->run_energy) {
-    emc::k_search_energies<<<(np + 255) / 256, 256, 0, st>>>(s->d_parts.p, np, s->run_energy);
+    emc::k_search_energies<<<(np + 255) / 256, 256, 0, st>>>(s->cur->parts.p, np, s->run_energy);
     EMC_LAUNCH_CHECK();
     ++launches;
   }
@@ -542,7 +572,7 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
     }
   }
   if (d_best) {
-    emc::k_search_best<<<(np + 127) / 128, 128, 0, st>>>(s->d_parts.p, np, s->d_results.p, s->d_best_keys.p, d_best);
+    emc::k_search_best<<<(np + 127) / 128, 128, 0, st>>>(s->cur->parts.p, np, s->d_results.p, s->d_best_keys.p, d_best);
     EMC_LAUNCH_CHECK();
     ++launches;
   }
@@ -576,6 +606,7 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
     EMC_CHECK_ARG(d_energy || d.energy > 0.0, "particle %d: energy must be > 0", p);
     emc::DevParticle& q = parts[p];
     q.spec = reinterpret_cast<const float2*>(d.spectrum);
+    q.wedge = d.wedge;
     q.energy = d.energy;
     memcpy(q.prior, d.prior, sizeof(q.prior));
     memcpy(q.shift, d.shift, sizeof(q.shift));
@@ -600,9 +631,14 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
     memcpy(k + 56, &d_energy, 8);
   }
   s->run_energy = d_energy;
-  if (!s->profiling && !s->gkey.empty() && s->gkey == key && s->gexec && !s->refs_dirty) {
-    EMC_CUDA(cudaGraphLaunch(s->gexec, st));
-    return EMC_OK;
+  if (s->refs_dirty) drop_graphs(s);
+  if (!s->profiling) {
+    for (auto& g : s->graphs)
+      if (g.key == key) {
+        g.used = ++s->use_clock;
+        EMC_CUDA(cudaGraphLaunch(g.exec, st));
+        return EMC_OK;
+      }
   }
   // ---- group pairs by (box, dtype) and cut chunks
   std::vector<emc::EvalItem> items;
@@ -630,9 +666,8 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
         max_chunk = std::max(max_chunk, c.count);
       }
     }
-  // ---- buffers
-  EMC_TRY(s->d_parts.reserve(np));
-  EMC_TRY(s->d_items.reserve(items.size()));
+  // ---- shared scratch (a reallocation invalidates every recorded request)
+  const void* before[7] = {s->d_results.p, s->d_best_keys.p, s->stats.p, s->keys.p, s->done.p, s->s1.p, s->s2.p};
   EMC_TRY(s->d_results.reserve(total));
   EMC_TRY(s->d_best_keys.reserve(np));
   EMC_TRY(s->stats.reserve(max_chunk));
@@ -650,6 +685,10 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
     EMC_TRY(s->s1.reserve(s1n));
     EMC_TRY(s->s2.reserve(s2n));
   }
+  {
+    const void* after[7] = {s->d_results.p, s->d_best_keys.p, s->stats.p, s->keys.p, s->done.p, s->s1.p, s->s2.p};
+    if (memcmp(before, after, sizeof(before)) != 0) drop_graphs(s);
+  }
   if (s->refs_dirty) {
     std::vector<emc::DevRef> dr(s->refs.size());
     for (size_t i = 0; i < s->refs.size(); ++i)
@@ -658,44 +697,74 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
     EMC_CUDA(cudaMemcpy(s->d_refs.p, dr.data(), sizeof(emc::DevRef) * dr.size(), cudaMemcpyHostToDevice));
     s->refs_dirty = false;
   }
-  EMC_CUDA(cudaMemcpyAsync(s->d_parts.p, parts.data(), sizeof(emc::DevParticle) * np, cudaMemcpyHostToDevice, st));
-  EMC_CUDA(cudaMemcpyAsync(s->d_items.p, items.data(), sizeof(emc::EvalItem) * items.size(), cudaMemcpyHostToDevice,
-                           st));
-  // host vectors must outlive the async copies
-  EMC_CUDA(cudaStreamSynchronize(st));
-  for (const Chunk& c : chunks)
-    if (!planes_slot(s, c.n, c.dtype)) EMC_TRY(tune_planes(s, c, st));
+  // ---- this request's tables: the eager set when profiling, else a new cache entry
+  emc_search_s::GraphEntry* entry = nullptr;
   if (s->profiling) {
-    s->gkey.clear();
-    return search_record(s, chunks, np, total, d_cc, d_peak, d_best, st);
+    s->cur = &s->eager_tables;
+  } else {
+    if (s->graphs.size() >= emc_search_s::kGraphCache) {
+      auto lru = std::min_element(s->graphs.begin(), s->graphs.end(),
+                                  [](const auto& a, const auto& b) { return a.used < b.used; });
+      if (lru->exec) cudaGraphExecDestroy(lru->exec);
+      lru->tables.release();
+      s->graphs.erase(lru);
+    }
+    s->graphs.emplace_back();
+    entry = &s->graphs.back();
+    s->cur = &entry->tables;
   }
+  auto abandon = [&](emc_status rs) {
+    if (entry) {
+      entry->tables.release();
+      s->graphs.pop_back();
+    }
+    return rs;
+  };
+  {
+    emc_status rs = s->cur->parts.reserve(np);
+    if (rs == EMC_OK) rs = s->cur->items.reserve(items.size());
+    if (rs != EMC_OK) return abandon(rs);
+  }
+  if (cudaMemcpyAsync(s->cur->parts.p, parts.data(), sizeof(emc::DevParticle) * np, cudaMemcpyHostToDevice, st) ||
+      cudaMemcpyAsync(s->cur->items.p, items.data(), sizeof(emc::EvalItem) * items.size(), cudaMemcpyHostToDevice,
+                      st) ||
+      // host vectors must outlive the async copies
+      cudaStreamSynchronize(st)) {
+    emc::set_error("emc_search_run: table upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return abandon(EMC_E_CUDA);
+  }
+  for (const Chunk& c : chunks)
+    if (!planes_slot(s, c.n, c.dtype)) {
+      const emc_status rs = tune_planes(s, c, st);
+      if (rs != EMC_OK) return abandon(rs);
+    }
+  if (s->profiling) return search_record(s, chunks, np, total, d_cc, d_peak, d_best, st);
   // ---- capture the launch sequence into a graph, then launch it
-  if (s->gexec) {
-    cudaGraphExecDestroy(s->gexec);
-    s->gexec = nullptr;
+  if (cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    emc::set_error("emc_search_run: stream capture failed to start");
+    return abandon(EMC_E_CUDA);
   }
-  s->gkey.clear();
-  EMC_CUDA(cudaStreamBeginCapture(s->cap_stream, cudaStreamCaptureModeThreadLocal));
   emc_status rs = search_record(s, chunks, np, total, d_cc, d_peak, d_best, s->cap_stream);
   cudaGraph_t graph = nullptr;
   cudaError_t ce = cudaStreamEndCapture(s->cap_stream, &graph);
   if (rs != EMC_OK) {
     if (graph) cudaGraphDestroy(graph);
-    return rs;
+    return abandon(rs);
   }
   if (ce != cudaSuccess) {
     emc::set_error("emc_search_run: graph capture failed: %s", cudaGetErrorString(ce));
-    return EMC_E_CUDA;
+    return abandon(EMC_E_CUDA);
   }
-  ce = cudaGraphInstantiate(&s->gexec, graph, 0);
+  ce = cudaGraphInstantiate(&entry->exec, graph, 0);
   cudaGraphDestroy(graph);
   if (ce != cudaSuccess) {
     emc::set_error("emc_search_run: graph instantiation failed: %s", cudaGetErrorString(ce));
-    s->gexec = nullptr;
-    return EMC_E_CUDA;
+    entry->exec = nullptr;
+    return abandon(EMC_E_CUDA);
   }
-  s->gkey = key;
-  EMC_CUDA(cudaGraphLaunch(s->gexec, st));
+  entry->key = key;
+  entry->used = ++s->use_clock;
+  EMC_CUDA(cudaGraphLaunch(entry->exec, st));
   return EMC_OK;
 }
 
@@ -741,7 +810,7 @@ emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particle
   cudaFree(d_peak);
   cudaFree(d_best);
   // the graph was recorded with these temporary outputs: do not replay it
-  s->gkey.clear();
+  drop_graphs(s);
   return rs;
 }
 
@@ -785,7 +854,7 @@ emc_status emc_search_set_planes(emc_search_t s, int box, int planes) {
     s->planes[b][d] = planes;
     for (int k = 0; k < 4; ++k) s->tune_ms[b][d][k] = -1.f;
   }
-  s->gkey.clear();
+  drop_graphs(s);
   return EMC_OK;
 }
 
@@ -805,7 +874,8 @@ emc_status emc_search_destroy(emc_search_t s) {
   for (int i = 0; i < emc_search_s::kRing; ++i)
     for (int k = 0; k < 5; ++k)
       if (s->ev[i][k]) cudaEventDestroy(s->ev[i][k]);
-  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  drop_graphs(s);
+  s->eager_tables.release();
   for (auto& r : s->refs) {
     cudaFree(r.data);
     cudaFree(r.mask);
@@ -814,8 +884,6 @@ emc_status emc_search_destroy(emc_search_t s) {
   }
   s->d_refs.release();
   s->d_dmat.release();
-  s->d_parts.release();
-  s->d_items.release();
   s->d_results.release();
   s->d_best_keys.release();
   s->s1.release();

@@ -5,7 +5,8 @@
 //                                FP64 sums of r and r^2 (DC-free energy by Parseval)
 //                                R2C along x (two rows per complex FFT), FFT along y
 //                                -> S1[e][z][y][kx]                         (n * n * nh c64)
-//   pass B  (CTA = one ky row)   FFT along z, X = Q .* conj(wref .* R), X(0) = 0,
+//   pass B  (CTA = one ky row)   FFT along z, X = Q .* conj(wref .* R) .* wdgMask, X(0) = 0,
+//                                E_R = sum |wref .* R .* wdgMask|^2 when either weight is set,
 //                                inverse FFT along z, keep the w output planes |sz| <= r
 //                                -> S2[e][j][ky][kx]                        (w * n * nh c64)
 //   pass C  (CTA = one sz plane) inverse FFT along y, C2R along x for the w rows |sy| <= r,
@@ -19,8 +20,9 @@
 namespace emc {
 
 struct DevParticle {
-  const float2* spec;  // Q, [z][y][kx]
-  double energy;       // E_P
+  const float2* spec;  // Q = refWdg .* P, [z][y][kx]
+  const float* wedge;  // wdgMask, the weight on the rotated reference, [z][y][kx] or null (= 1)
+  double energy;       // E_P = sum |Q|^2
   double prior[9];     // column-major
   float shift[3];
   int ref;
@@ -517,8 +519,9 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
 }
 
 // ------------------------------------------------------------------ pass B
+// 64^3: four resident 288-thread CTAs per SM asked of the compiler (56 registers)
 template <int N>
-__global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const SearchChunkArgs a,
+__global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_z_mul(const SearchChunkArgs a,
                                                                       const float2* __restrict__ g_tw) {
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, P = C::P, TPB = C::TPB, NT = C::NT_B;
@@ -537,12 +540,17 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const Searc
   constexpr int NB = C::NHB;
   const EvalItem it = a.items[e];
   const DevParticle& pt = a.parts[it.particle];
+  // weights on the rotated reference: the reference's bandpass wref and the particle's wdgMask
+  // (BH_multi_xcf_Translational_2.m:35-38).  The first present one (the wedge when both are) is
+  // prefetched into shared memory with the spectrum; a second one is read at use.
   const float* __restrict__ wref = a.refs[pt.ref].wref;
+  const float* __restrict__ w1 = pt.wedge ? pt.wedge : wref;
+  const float* __restrict__ w2 = pt.wedge ? wref : nullptr;
   const float2* __restrict__ q = pt.spec;
   const int w = 2 * a.radius + 1;
   constexpr int IT = (N * NB + NT - 1) / NT;
 
-  // (PREF_B) this thread's elements i of the particle spectrum and of the reference weight,
+  // (PREF_B) this thread's elements i of the particle spectrum and of the first weight,
   // copied asynchronously while the slab loads and the forward transform run
   float2* s_q = s_tw + N;                                     // [N * NHB]
   float* s_w = reinterpret_cast<float*>(s_q + N * C::NHB);    // [N * NHB]
@@ -553,7 +561,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const Searc
       if (i < N * NB && i % NB < cnt) {
         const size_t gi = ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB;
         cp_async8(s_q + i, q + gi);
-        if (wref) cp_async4(s_w + i, wref + gi);
+        if (w1) cp_async4(s_w + i, w1 + gi);
       }
     }
     cp_async_commit();
@@ -589,6 +597,15 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const Searc
     float2 qv[C::PREF_B ? 1 : IT];
     if constexpr (C::PREF_B) {
       cp_async_wait<0>();  // this thread's own copies; no other thread reads them
+      if (w2) {
+        // both weights: fold the second into this thread's prefetched elements (a separate loop,
+        // so its loads do not hold registers across the multiply below)
+#pragma unroll 1
+        for (int k = 0; k < IT; ++k) {
+          const int i = threadIdx.x + k * NT;
+          if (i < N * NB && i % NB < cnt) s_w[i] *= __ldg(w2 + ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB);
+        }
+      }
     } else {
 #pragma unroll
       for (int k = 0; k < IT; ++k) {
@@ -604,8 +621,9 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const Searc
       const size_t gi = ((size_t)z * N + ky) * NH + kx;
       float2& slot = tile[lpos<1>(z) * TPB + kl];
       float2 r = slot;
-      if (wref) {
-        const float wv = C::PREF_B ? s_w[i] : __ldg(wref + gi);
+      if (w1) {
+        float wv = C::PREF_B ? s_w[i] : __ldg(w1 + gi);
+        if (!C::PREF_B && w2) wv *= __ldg(w2 + gi);
         r.x *= wv;
         r.y *= wv;
         if (gi != 0) en += (kx == 0 || 2 * kx == N ? 1.0 : 2.0) * ((double)r.x * r.x + (double)r.y * r.y);
@@ -615,7 +633,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B) k_search_z_mul(const Searc
       slot = x;
     }
   }
-  if (wref) {
+  if (w1) {
     double t = block_sum(en, red);
     if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
   }
@@ -656,7 +674,9 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC, N <= 64 ? 4 : 0) k_search
   const int sz = j - r;
   const EvalItem it = a.items[e];
   const DevParticle& pt = a.parts[it.particle];
-  const bool has_wref = a.refs[pt.ref].wref != nullptr;
+  // with a weight on the reference E_R is its weighted spectral energy (pass B), else the
+  // DC-free real-space energy of the rotated, masked reference (pass A, by Parseval)
+  const bool weighted = a.refs[pt.ref].wref != nullptr || pt.wedge != nullptr;
 
   load_twiddles<N>(s_tw, g_tw);
   if (threadIdx.x == 0) s_best = 0ull;
@@ -687,7 +707,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC, N <= 64 ? 4 : 0) k_search
   __syncthreads();
 
   const EvalStats st = a.stats[e];
-  const double er = has_wref ? st.energy_spec : ((double)N * N * N * st.sum_r2 - st.sum_r * st.sum_r);
+  const double er = weighted ? st.energy_spec : ((double)N * N * N * st.sum_r2 - st.sum_r * st.sum_r);
   const double denom = er * pt.energy;
   const float inv_norm = denom > 0.0 ? (float)(1.0 / sqrt(denom)) : 0.f;
   constexpr int c = N / 2;

@@ -1,8 +1,12 @@
 // mexEmcSearch -- MEX gateway for the fused orientation search (no single reference MEX: it
 // replaces the per-orientation MATLAB loop of alignment/BH_alignRaw3d_v2.m:1119-1423).
 //   [cc, peak, best] = mexEmcSearch(gpuArray single ref, gpuArray single mask or [],
-//                                   gpuArray single particle, gpuArray single weight or [],
-//                                   double prior[9], double eulers[n x 3], int peakRadius)
+//                                   gpuArray single particle, gpuArray single wdgMask or [],
+//                                   double prior[9], double eulers[n x 3], int peakRadius
+//                                   [, gpuArray single refWdg or []])
+//   wdgMask / refWdg: real half spectra ((n/2+1) x n x n, FFT order), the weights of
+//   BH_multi_xcf_Translational_2.m:35-38 on the rotated reference (the particle's wedge) and on
+//   the particle (the reference's wedge); [] = 1.
 //   cc:   n x 1 single (normalised CC at each orientation's peak)
 //   peak: n x 3 int32  (integer shift x, y, z)
 //   best: 1 x 5 double [cc, orientation (1-based), dx, dy, dz]
@@ -13,7 +17,7 @@
 #include "mex_common.h"
 
 void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
-  if (nrhs != 7) mexErrMsgIdAndTxt("EMC:mexEmcSearch:rhs", "expected 7 inputs");
+  if (nrhs != 7 && nrhs != 8) mexErrMsgIdAndTxt("EMC:mexEmcSearch:rhs", "expected 7 or 8 inputs");
   const mxGPUArray* ref = mxGPUCreateFromMxArray(prhs[0]);
   const int n = (int)mxGPUGetDimensions(ref)[0];
   const float* mask = nullptr;
@@ -23,11 +27,17 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     mask = (const float*)mxGPUGetDataReadOnly(gm);
   }
   const mxGPUArray* part = mxGPUCreateFromMxArray(prhs[2]);
-  const float* weight = nullptr;
+  const float* wdg_mask = nullptr;
   const mxGPUArray* gw = nullptr;
   if (mxGetNumberOfElements(prhs[3]) > 0) {
     gw = mxGPUCreateFromMxArray(prhs[3]);
-    weight = (const float*)mxGPUGetDataReadOnly(gw);
+    wdg_mask = (const float*)mxGPUGetDataReadOnly(gw);
+  }
+  const float* ref_wdg = nullptr;
+  const mxGPUArray* grw = nullptr;
+  if (nrhs == 8 && mxGetNumberOfElements(prhs[7]) > 0) {
+    grw = mxGPUCreateFromMxArray(prhs[7]);
+    ref_wdg = (const float*)mxGPUGetDataReadOnly(grw);
   }
   emc_particle_desc d;
   memset(&d, 0, sizeof(d));
@@ -41,7 +51,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   mxGPUArray* spec = mxGPUCreateGPUArray(3, hd, mxSINGLE_CLASS, mxCOMPLEX, MX_GPU_DO_NOT_INITIALIZE);
   const mwSize one = 1;
   mxGPUArray* en = mxGPUCreateGPUArray(1, &one, mxDOUBLE_CLASS, mxREAL, MX_GPU_INITIALIZE_VALUES);
-  EMC_MEX_CHECK("mexEmcSearch", emc_particle_spectrum(n, (const float*)mxGPUGetDataReadOnly(part), weight, nullptr,
+  EMC_MEX_CHECK("mexEmcSearch", emc_particle_spectrum(n, (const float*)mxGPUGetDataReadOnly(part), ref_wdg, nullptr,
                                                       (float*)mxGPUGetData(spec), (double*)mxGPUGetData(en),
                                                       nullptr));
   emc_search_t s = nullptr;
@@ -63,6 +73,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     d.ref_id = rid;
     d.orient_begin = 0;
     d.orient_count = no;
+    d.wedge = wdg_mask;
     st = emc_search_run_host(s, &d, 1, cc.data(), pk.data(), &hit, nullptr);
   }
   emc_search_destroy(s);
@@ -72,6 +83,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   mxGPUDestroyGPUArray(part);
   if (gm) mxGPUDestroyGPUArray(gm);
   if (gw) mxGPUDestroyGPUArray(gw);
+  if (grw) mxGPUDestroyGPUArray(grw);
   EMC_MEX_CHECK("mexEmcSearch", st);
   mwSize cd[2] = {(mwSize)no, 1};
   plhs[0] = mxCreateNumericArray(2, cd, mxSINGLE_CLASS, mxREAL);

@@ -13,6 +13,7 @@ is applied in real space with the reference sampling ('forward' semantics).
 import ctypes as C
 
 import numpy as np
+import torch
 
 from . import _lib as L
 
@@ -34,7 +35,11 @@ class BatchObjective:
 
     def __call__(self, poses, idx=None):
         """poses: (k, 6) for the items idx (all items when None).  Returns (-cc, -grad)."""
-        import torch
+        f, g = self.cc_grad(poses, idx)
+        return -f, -g
+
+    def cc_grad(self, poses, idx=None):
+        """poses: (k, 6) for the items idx (all items when None).  Returns (cc, dcc/dpose)."""
         idx = np.arange(self.n) if idx is None else np.asarray(idx)
         k = len(idx)
         poses = np.ascontiguousarray(poses, dtype=np.float64).reshape(k, 6)
@@ -49,7 +54,27 @@ class BatchObjective:
                en.ctypes.data_as(pd), pr.ctypes.data_as(pd), poses.ctypes.data_as(pd), self.interp,
                cc.ctypes.data_as(pd), g.ctypes.data_as(pd), C.c_void_p(torch.cuda.current_stream().cuda_stream))
         self.evals += k
-        return -cc, -g
+        return cc, g
+
+
+class CCPose(torch.autograd.Function):
+    """torch.autograd.Function over the forward + adjoint (emc_cc_adjoint_batch).
+    ``CCPose.apply(poses, objective)`` maps a (k, 6) float64 tensor of poses (phi, theta, psi in
+    degrees; tx, ty, tz in voxels) to the k masked normalised CCs of a BatchObjective; backward
+    returns grad_out * dCC/dpose from the same launch (the adjoint kernel evaluates the value and its
+    exact gradient together, so nothing is recomputed).  For tests and for optimisers written against
+    torch; the L-BFGS below calls the objective directly."""
+
+    @staticmethod
+    def forward(ctx, poses, objective):
+        cc, g = objective.cc_grad(poses.detach().cpu().numpy())
+        ctx.save_for_backward(torch.from_numpy(g).to(poses))
+        return torch.from_numpy(cc).to(poses)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (g,) = ctx.saved_tensors
+        return grad_out.unsqueeze(-1) * g, None
 
 
 def lbfgs(objective, x0, n_iter=20, memory=6, max_ls=8, c1=1e-4, first_step=1.0, tol=1e-10):

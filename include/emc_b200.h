@@ -202,9 +202,18 @@ EMC_API emc_status emc_xcf_translational(const float* d_a, const float* d_b, int
 
 typedef struct emc_search_s* emc_search_t;
 
-/* Particle side of one search item.  spectrum = W .* B .* F(particle) with
- * F(0) = 0 (BH_bandLimitCenterNormalize.m:48-55 times the particle weight),
- * as produced by emc_particle_spectrum. */
+/* Particle side of one search item.  The search scores every orientation with the normalised
+ * translational CC of BH_multi_xcf_Translational_2.m:35-38,
+ *   map = real(ifftn(refWdg .* rotPART_FT .* REF_FT .* wdgMask)) * numel
+ *         / sqrt(sum |REF_FT .* wdgMask|^2 * sum |rotPART_FT .* refWdg|^2),
+ * with REF_FT = conj(wref .* fftn(rotated, masked reference)), DC = 0.  The particle's operands are
+ *   spectrum = refWdg .* rotPART_FT, rotPART_FT = B .* F(particle) with F(0) = 0
+ *              (BH_bandLimitCenterNormalize.m:48-55), as emc_particle_spectrum makes it with
+ *              weight = refWdg;  energy = sum |spectrum|^2;
+ *   wedge    = wdgMask, a real half spectrum that multiplies the rotated reference's spectrum (NULL
+ *              = 1).  With BH_multi_xcf_Rotational's binding (BH_alignRaw3d_v2.m:1376-1383: the
+ *              particle's wedge on the reference, the reference's wedge on the particle) this is
+ *              the particle's own missing-wedge / CTF weight and refWdg is the reference's. */
 typedef struct {
   const float* spectrum;   /* device, (n/2+1)*n*n complex */
   double energy;           /* sum over the full spectrum of |spectrum|^2 */
@@ -214,6 +223,7 @@ typedef struct {
   int    ref_id;           /* reference registered with emc_search_add_reference */
   int    orient_begin;     /* slice [begin, begin+count) of the orientation list */
   int    orient_count;
+  const float* wedge;      /* device, (n/2+1)*n*n floats (FFT order), or NULL */
 } emc_particle_desc;
 
 typedef struct {
@@ -224,7 +234,9 @@ typedef struct {
 
 /* Q = weight .* bandpass .* fftn(particle) with Q(0) = 0; *energy = sum |Q|^2 over the
  * full spectrum (Hermitian-weighted, FP64).  weight/bandpass: real half spectra
- * (n/2+1)*n*n in FFT order, either may be NULL (= 1).  d_energy: one device double. */
+ * (n/2+1)*n*n in FFT order, either may be NULL (= 1).  d_energy: one device double.
+ * For the search, weight is the CC formula's refWdg (the weight that multiplies the particle)
+ * and bandpass the particle's bandpassFilt. */
 EMC_API emc_status emc_particle_spectrum(int n, const float* d_particle, const float* d_weight,
                                  const float* d_bandpass, float* d_spectrum_out,
                                  double* d_energy, void* stream);
@@ -261,7 +273,9 @@ EMC_API emc_status emc_search_configure(emc_search_t s, int peak_radius, int int
  * d_peak holds 3 ints per pair.  d_best: one hit per particle (stable argmax over its
  * orientations, first index wins ties, as sortrows(...,-6) at BH_alignRaw3d_v2.m:1423).
  * All outputs are device memory.  Uneven box sizes are allowed in one call; the
- * launch sequence is captured in a CUDA graph and replayed on identical calls. */
+ * launch sequence is captured in a CUDA graph, and the graphs of the four most recent distinct
+ * requests are kept and replayed when a request repeats (a double-buffered pipeline alternating
+ * between two descriptor sets replays both). */
 EMC_API emc_status emc_search_run(emc_search_t s, const emc_particle_desc* particles, int n_particles,
                           float* d_cc, int* d_peak, emc_search_hit* d_best, void* stream);
 /* emc_search_run with the particle energies read on the device: d_energy[p] replaces

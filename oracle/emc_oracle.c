@@ -505,22 +505,69 @@ EXPORT double FN(orc_particle_spectrum)(const REAL* particle, const REAL* weight
   return e;
 }
 
+/* ------------------------------------------------------------------ normalised translational CC */
+/* statistics/BH_multi_xcf_Translational_2.m:35-38 with its four operands, on half spectra (every
+ * sum over MATLAB's full spectrum is the Hermitian-weighted sum over the half):
+ *   iCCCmap = real(ifftn(refWdg .* rotPART_FT .* REF_FT .* wdgMask))
+ *             * numel / sqrt(sum|REF_FT .* wdgMask|^2 * sum|rotPART_FT .* refWdg|^2)
+ * where, as at the call site (alignment/BH_alignRaw3d_v2.m:1287-1330):
+ *   REF_FT     = conj(R), R = wref .* fftn(mask .* I(M (p - c - t) + c)) with R(0) = 0: the
+ *                reference sampled through M with 'forward' semantics and passed through
+ *                BH_bandLimitCenterNormalize(.., bandpassFiltREF) (whose final scalar cancels);
+ *   rotPART_FT = P, the particle spectrum with P(0) = 0 (BH_bandLimitCenterNormalize output);
+ *   wdgMask    = the weight that multiplies the reference spectrum (NULL = 1);
+ *   refWdg     = the weight that multiplies the particle spectrum (NULL = 1).
+ * The unnormalised inverse transform (no 1/numel) is numel * ifftn.  Writes the map in FFT order
+ * (unshifted) and returns 1 / sqrt(E_R E_P). */
+static double xcf2_map(const REAL* ref, const REAL* mask, const REAL* wref, int n, const cplx* P,
+                       const REAL* ref_wdg, const REAL* wdg_mask, const double M[9], const double shift[3],
+                       int interp, REAL* r, cplx* X, REAL* map) {
+  const int nh = n / 2 + 1;
+  const long nhalf = (long)nh * n * n;
+  const int c = n / 2;
+  for (int z = 0; z < n; ++z)
+    for (int y = 0; y < n; ++y)
+      for (int x = 0; x < n; ++x) {
+        double s[3];
+        sample_pos(M, shift, 1, x, y, z, c, c, c, s);
+        REAL v = interp == 1 ? interp_cubic(ref, n, n, n, s[0], s[1], s[2])
+                             : interp_linear(ref, n, n, n, s[0], s[1], s[2], interp == 2);
+        long i = ((long)z * n + y) * n + x;
+        r[i] = mask ? (REAL)(v * mask[i]) : v;
+      }
+  FN(orc_fft3_r2c)(r, n, n, n, (REAL*)X);
+  double ER = 0, EP = 0;
+  for (long i = 0; i < nhalf; ++i) {
+    const double hw = herm_w((int)(i % nh), n);
+    cplx R = X[i];
+    if (wref) { R.re *= wref[i]; R.im *= wref[i]; }
+    if (i == 0) { R.re = 0; R.im = 0; }
+    const cplx ref_ft = {R.re, (REAL)-R.im};                       /* REF_FT = conj(R) */
+    const REAL wm = wdg_mask ? wdg_mask[i] : (REAL)1, rw = ref_wdg ? ref_wdg[i] : (REAL)1;
+    const cplx rw_ref = {ref_ft.re * wm, ref_ft.im * wm};           /* REF_FT .* wdgMask */
+    const cplx p_rw = {P[i].re * rw, P[i].im * rw};                 /* rotPART_FT .* refWdg */
+    ER += hw * ((double)rw_ref.re * rw_ref.re + (double)rw_ref.im * rw_ref.im);
+    EP += hw * ((double)p_rw.re * p_rw.re + (double)p_rw.im * p_rw.im);
+    X[i] = c_mul(p_rw, rw_ref);                                     /* refWdg.*P.*REF_FT.*wdgMask */
+  }
+  FN(orc_fft3_c2r)((REAL*)X, n, n, n, map);
+  return 1.0 / sqrt(ER * EP);
+}
+
 /* ------------------------------------------------------------------ orientation search */
-/* One CC evaluation per orientation (alignment/BH_alignRaw3d_v2.m:1287-1336 with the
- * normalised map of statistics/BH_multi_xcf_Translational_2.m:35-38 and the masked argmax
- * of statistics/BH_multi_xcf_Translational.m:31-42):
- *   r   = mask .* I(M_o (p - c - t) + c)                  reference through RotMat', 'forward'
- *   R   = wref .* fftn(r),  R(0) = 0
- *   map = real(ifftn(Q .* conj(R))) * numel / sqrt(sum|R|^2 * E_P)
- * argmax of the map over shifts s with |s|^2 <= radius^2; ties go to the smallest
- * fftshifted column-major index (MATLAB max).  Outputs per orientation the CC and the
- * integer shift s (x, y, z).  OpenMP over orientations with `nthreads` threads. */
-EXPORT void FN(orc_search)(const REAL* ref, const REAL* mask, const REAL* wref, int n, const REAL* Q_c, double EP,
-                           const double* Mlist, int norient, const double shift[3], int radius, int interp,
-                           int nthreads, double* cc_out, int* peak_out) {
+/* One CC evaluation per orientation: the normalised map of xcf2_map (BH_multi_xcf_Translational_2.m:
+ * 35-38) for M = RotMat (the reference sampled through RotMat', 'forward';
+ * BH_alignRaw3d_v2.m:1287-1291) and the masked argmax of BH_multi_xcf_Translational.m:33-42 over
+ * shifts s with |s|^2 <= radius^2 (the spherical peakMask); ties go to the smallest fftshifted
+ * column-major index (MATLAB max).  Outputs per orientation the CC and the integer shift s
+ * (x, y, z).  P: particle half spectrum (complex).  OpenMP over orientations with `nthreads`. */
+EXPORT void FN(orc_search)(const REAL* ref, const REAL* mask, const REAL* wref, int n, const REAL* P_c,
+                           const REAL* ref_wdg, const REAL* wdg_mask, const double* Mlist, int norient,
+                           const double shift[3], int radius, int interp, int nthreads, double* cc_out,
+                           int* peak_out) {
   const int nh = n / 2 + 1;
   const long nvox = (long)n * n * n, nhalf = (long)nh * n * n;
-  const cplx* Q = (const cplx*)Q_c;
+  const cplx* P = (const cplx*)P_c;
   const int c = n / 2;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -529,35 +576,12 @@ EXPORT void FN(orc_search)(const REAL* ref, const REAL* mask, const REAL* wref, 
   {
     REAL* r = (REAL*)malloc(sizeof(REAL) * nvox);
     REAL* map = (REAL*)malloc(sizeof(REAL) * nvox);
-    cplx* R = (cplx*)malloc(sizeof(cplx) * nhalf);
+    cplx* X = (cplx*)malloc(sizeof(cplx) * nhalf);
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 1)
 #endif
     for (int o = 0; o < norient; ++o) {
-      const double* M = Mlist + 9 * o;
-      for (int z = 0; z < n; ++z)
-        for (int y = 0; y < n; ++y)
-          for (int x = 0; x < n; ++x) {
-            double s[3];
-            sample_pos(M, shift, 1, x, y, z, c, c, c, s);
-            REAL v = interp == 1 ? interp_cubic(ref, n, n, n, s[0], s[1], s[2])
-                                 : interp_linear(ref, n, n, n, s[0], s[1], s[2], interp == 2);
-            long i = ((long)z * n + y) * n + x;
-            r[i] = mask ? (REAL)(v * mask[i]) : v;
-          }
-      FN(orc_fft3_r2c)(r, n, n, n, (REAL*)R);
-      double ER = 0;
-      for (long i = 0; i < nhalf; ++i) {
-        if (wref) { R[i].re *= wref[i]; R[i].im *= wref[i]; }
-        if (i == 0) { R[i].re = 0; R[i].im = 0; }
-        ER += herm_w((int)(i % nh), n) * ((double)R[i].re * R[i].re + (double)R[i].im * R[i].im);
-        /* X = Q conj(R) */
-        cplx q = Q[i], rr = R[i];
-        R[i].re = q.re * rr.re + q.im * rr.im;
-        R[i].im = q.im * rr.re - q.re * rr.im;
-      }
-      FN(orc_fft3_c2r)((REAL*)R, n, n, n, map);
-      const double norm = 1.0 / sqrt(ER * EP);
+      const double norm = xcf2_map(ref, mask, wref, n, P, ref_wdg, wdg_mask, Mlist + 9 * o, shift, interp, r, X, map);
       double best = -INFINITY;
       long best_idx = 0x7fffffffffffL;
       int bs[3] = {0, 0, 0};
@@ -578,46 +602,25 @@ EXPORT void FN(orc_search)(const REAL* ref, const REAL* mask, const REAL* wref, 
       peak_out[3 * o + 1] = bs[1];
       peak_out[3 * o + 2] = bs[2];
     }
-    free(r); free(map); free(R);
+    free(r); free(map); free(X);
   }
 }
 
-/* Full normalised CC map (fftshifted, BH_multi_xcf_Translational_2.m:35-38) for one rotation
- * matrix, followed by the peak-mask / argmax / two-pass centre of mass of
- * BH_multi_xcf_Translational.m:33-97 (peakCOM = 3).  Writes the map (n^3, fftshifted) and
- * the subvoxel peak (x, y, z) relative to the origin. */
-EXPORT double FN(orc_xcf_translational)(const REAL* ref, const REAL* mask, const REAL* wref, int n, const REAL* Q_c,
-                                        double EP, const double M[9], const double shift[3], const REAL* peak_mask,
-                                        int interp, REAL* map_out, double peak_out[3]) {
+/* Full normalised CC map (fftshifted, BH_multi_xcf_Translational_2.m:35-38, operands as xcf2_map) for
+ * one rotation matrix, followed by the peak-mask / argmax / two-pass centre of mass of
+ * BH_multi_xcf_Translational.m:33-97 (peakCOM = 3).  Writes the map (n^3, fftshifted) and the
+ * subvoxel peak (x, y, z) relative to the origin; returns the map maximum inside the peak mask. */
+EXPORT double FN(orc_xcf_translational)(const REAL* ref, const REAL* mask, const REAL* wref, int n, const REAL* P_c,
+                                        const REAL* ref_wdg, const REAL* wdg_mask, const double M[9],
+                                        const double shift[3], const REAL* peak_mask, int interp, REAL* map_out,
+                                        double peak_out[3]) {
   const int nh = n / 2 + 1;
   const long nvox = (long)n * n * n, nhalf = (long)nh * n * n;
-  const cplx* Q = (const cplx*)Q_c;
   const int c = n / 2;
   REAL* r = (REAL*)malloc(sizeof(REAL) * nvox);
   REAL* map = (REAL*)malloc(sizeof(REAL) * nvox);
-  cplx* R = (cplx*)malloc(sizeof(cplx) * nhalf);
-  for (int z = 0; z < n; ++z)
-    for (int y = 0; y < n; ++y)
-      for (int x = 0; x < n; ++x) {
-        double s[3];
-        sample_pos(M, shift, 1, x, y, z, c, c, c, s);
-        REAL v = interp == 1 ? interp_cubic(ref, n, n, n, s[0], s[1], s[2])
-                             : interp_linear(ref, n, n, n, s[0], s[1], s[2], interp == 2);
-        long i = ((long)z * n + y) * n + x;
-        r[i] = mask ? (REAL)(v * mask[i]) : v;
-      }
-  FN(orc_fft3_r2c)(r, n, n, n, (REAL*)R);
-  double ER = 0;
-  for (long i = 0; i < nhalf; ++i) {
-    if (wref) { R[i].re *= wref[i]; R[i].im *= wref[i]; }
-    if (i == 0) { R[i].re = 0; R[i].im = 0; }
-    ER += herm_w((int)(i % nh), n) * ((double)R[i].re * R[i].re + (double)R[i].im * R[i].im);
-    cplx q = Q[i], rr = R[i];
-    R[i].re = q.re * rr.re + q.im * rr.im;
-    R[i].im = q.im * rr.re - q.re * rr.im;
-  }
-  FN(orc_fft3_c2r)((REAL*)R, n, n, n, map);
-  const double norm = 1.0 / sqrt(ER * EP);
+  cplx* X = (cplx*)malloc(sizeof(cplx) * nhalf);
+  const double norm = xcf2_map(ref, mask, wref, n, (const cplx*)P_c, ref_wdg, wdg_mask, M, shift, interp, r, X, map);
   /* fftshift into map_out */
   double minv = INFINITY;
   for (int z = 0; z < n; ++z)
@@ -656,7 +659,7 @@ EXPORT double FN(orc_xcf_translational)(const REAL* ref, const REAL* mask, const
     }
   }
   for (int d = 0; d < 3; ++d) peak_out[d] = pc[d] - c;
-  free(r); free(map); free(R);
+  free(r); free(map); free(X);
   return bv;
 }
 

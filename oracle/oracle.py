@@ -46,9 +46,8 @@ def lib(precision="f64"):
         "orc_ctf2d": (None, [R, R, R, R, R, R, R, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, R, R, pR]),
         "orc_sf3d": (None, [C.c_int, C.c_int, C.c_int, C.c_int, pR, pR, pR, pR, pR, pR, pR, C.c_int, pR, pR, pR, pR]),
         "orc_particle_spectrum": (C.c_double, [pR, pR, pR, C.c_int, pR]),
-        "orc_search": (None, [pR, pR, pR, C.c_int, pR, C.c_double, pd, C.c_int, pd, C.c_int, C.c_int, C.c_int, pd,
-                              pi]),
-        "orc_xcf_translational": (C.c_double, [pR, pR, pR, C.c_int, pR, C.c_double, pd, pd, pR, C.c_int, pR, pd]),
+        "orc_search": (None, [pR, pR, pR, C.c_int, pR, pR, pR, pd, C.c_int, pd, C.c_int, C.c_int, C.c_int, pd, pi]),
+        "orc_xcf_translational": (C.c_double, [pR, pR, pR, C.c_int, pR, pR, pR, pd, pd, pR, C.c_int, pR, pd]),
         "orc_tsearch": (None, [pR, C.c_int, C.c_int, C.c_int, pR, C.c_int, pd, C.c_int, pR, pR]),
         "orc_cc_pose": (C.c_double, [pR, pR, C.c_int, pR, C.c_double, pd, pd, pd, pd]),
         "orc_cc_pose_interp": (C.c_double, [pR, pR, C.c_int, pR, C.c_double, pd, pd, C.c_int, pd, pd]),
@@ -157,42 +156,45 @@ def particle_spectrum(particle, weight=None, bandpass=None, precision="f64"):
     return q, e
 
 
-def search(ref, q, energy, matrices, mask=None, wref=None, shift=(0, 0, 0), radius=7, interp=0, nthreads=0,
-           precision="f64"):
-    """Per-orientation (cc, peak) of the fused search.  ``matrices``: RotMat per orientation
-    (the reference is sampled through RotMat', 'forward')."""
+def search(ref, P, matrices, mask=None, wref=None, ref_wdg=None, wdg_mask=None, shift=(0, 0, 0), radius=7, interp=0,
+           nthreads=0, precision="f64"):
+    """Per-orientation (cc, peak) of the normalised translational CC (BH_multi_xcf_Translational_2.m:35-38)
+    over the spherical peak window.  ``matrices``: RotMat per orientation (the reference is sampled
+    through RotMat', 'forward'); ``P``: particle half spectrum (rotPART_FT, P(0) = 0); ``wref``: the
+    reference bandpass; ``ref_wdg`` / ``wdg_mask``: the formula's refWdg (multiplies P) and wdgMask
+    (multiplies the reference), real half spectra or None (= 1)."""
     L = lib(precision)
     r = _arr(ref, L.dtype)
     n = r.shape[0]
-    m = _arr(mask, L.dtype)
-    wr = _arr(wref, L.dtype)
-    qq = np.ascontiguousarray(q, dtype=np.complex128 if precision == "f64" else np.complex64)
+    m, wr, rw, wm = (_arr(a, L.dtype) for a in (mask, wref, ref_wdg, wdg_mask))
+    pp = np.ascontiguousarray(P, dtype=np.complex128 if precision == "f64" else np.complex64)
     mats = np.ascontiguousarray(np.stack([np.asarray(M).T.flatten(order="F") for M in matrices]))
     sh = np.ascontiguousarray(shift, dtype=np.float64)
     no = len(matrices)
     cc = np.zeros(no)
     pk = np.zeros((no, 3), dtype=np.int32)
-    L.orc_search(L.ptr(r), L.ptr(m) if m is not None else None, L.ptr(wr) if wr is not None else None, n,
-                 L.ptr(qq.view(L.dtype)), float(energy), _p(mats), no, _p(sh), int(radius), int(interp),
-                 int(nthreads), _p(cc), _p(pk, C.c_int))
+    opt = lambda a: L.ptr(a) if a is not None else None  # noqa: E731
+    L.orc_search(L.ptr(r), opt(m), opt(wr), n, L.ptr(pp.view(L.dtype)), opt(rw), opt(wm), _p(mats), no, _p(sh),
+                 int(radius), int(interp), int(nthreads), _p(cc), _p(pk, C.c_int))
     return cc, pk
 
 
-def xcf_translational(ref, q, energy, matrix, mask=None, wref=None, shift=(0, 0, 0), peak_mask=None, interp=0):
+def xcf_translational(ref, P, matrix, mask=None, wref=None, ref_wdg=None, wdg_mask=None, shift=(0, 0, 0),
+                      peak_mask=None, interp=0):
+    """(max inside the peak mask, subvoxel peak, fftshifted normalised map) for one matrix; operands as
+    ``search``."""
     L = lib("f64")
     r = _arr(ref, L.dtype)
     n = r.shape[0]
-    m = _arr(mask, L.dtype)
-    wr = _arr(wref, L.dtype)
-    pm = _arr(peak_mask, L.dtype)
-    qq = np.ascontiguousarray(q, dtype=np.complex128)
+    m, wr, rw, wm, pm = (_arr(a, L.dtype) for a in (mask, wref, ref_wdg, wdg_mask, peak_mask))
+    pp = np.ascontiguousarray(P, dtype=np.complex128)
     M = np.ascontiguousarray(np.asarray(matrix).T.flatten(order="F"))
     sh = np.ascontiguousarray(shift, dtype=np.float64)
     out = np.zeros((n, n, n))
     peak = np.zeros(3)
-    v = L.orc_xcf_translational(L.ptr(r), L.ptr(m) if m is not None else None, L.ptr(wr) if wr is not None else None,
-                                n, L.ptr(qq.view(L.dtype)), float(energy), _p(M), _p(sh),
-                                L.ptr(pm) if pm is not None else None, int(interp), L.ptr(out), _p(peak))
+    opt = lambda a: L.ptr(a) if a is not None else None  # noqa: E731
+    v = L.orc_xcf_translational(L.ptr(r), opt(m), opt(wr), n, L.ptr(pp.view(L.dtype)), opt(rw), opt(wm), _p(M),
+                                _p(sh), opt(pm), int(interp), L.ptr(out), _p(peak))
     return v, peak, out
 
 
@@ -366,6 +368,22 @@ def xcf_rotational_np(P, R, wdg_mask=None, ref_wdg=None, nx=None):
     num = np.sum(hw * np.real(rw * P * R * wm))
     den = np.sum(hw * np.abs(R * wm) ** 2) * np.sum(hw * np.abs(P * rw) ** 2)
     return num / math.sqrt(den)
+
+
+def xcf_translational_2_np(rotPART_FT, REF_FT, wdgMask, refWdg):
+    """statistics/BH_multi_xcf_Translational_2.m:35-38 as written, on FULL spectra (numpy fftn order):
+    fftshift(real(ifftn((refWdg .* rotPART_FT .* REF_FT .* wdgMask) ./
+    (sqrt(sum(abs(REF_FT .* wdgMask).^2) .* sum(abs(rotPART_FT .* refWdg).^2)) ./ numel(wdgMask)))))."""
+    num = refWdg * rotPART_FT * REF_FT * wdgMask
+    den = np.sqrt(np.sum(np.abs(REF_FT * wdgMask) ** 2) * np.sum(np.abs(rotPART_FT * refWdg) ** 2)) / np.size(wdgMask)
+    return np.fft.fftshift(np.real(np.fft.ifftn(num / den)))
+
+
+def even_weight_np(rng, n, lo=0.2, hi=1.5):
+    """A random real full-grid weight with W(-k) = W(k) (as every wedge / CTF weight is), numpy fftn order."""
+    a = rng.uniform(lo, hi, (n, n, n))
+    flip = np.roll(a[::-1, ::-1, ::-1], 1, axis=(0, 1, 2))
+    return 0.5 * (a + flip)
 
 
 def symmetry_matrices_np(symmetry):

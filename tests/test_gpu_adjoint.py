@@ -155,3 +155,91 @@ def test_lbfgs_refinement_reduces_pose_error(setup):
     assert np.all(hist[-1] <= hist[0] + 1e-12)
     assert np.median(err) < 0.5 < np.median(err0)
     assert np.allclose(x[:, 3:], [1, -2, 0], atol=0.3)
+
+
+def _poses50(seed=50):
+    """50 seeded poses around the planted one (truth = defineMatrix([12, 25, -40], 'inv'), shift (1, -2, 0)):
+    angles within +/-6 degrees, shifts within +/-1.5 voxels."""
+    rng = np.random.default_rng(seed)
+    base = np.array([12.0, 25.0, -28.0, 1.0, -2.0, 0.0])
+    return base + np.concatenate([rng.uniform(-6, 6, (50, 3)), rng.uniform(-1.5, 1.5, (50, 3))], axis=1)
+
+
+def _angle_grad_from_dM(prior, p, dM):
+    """Chain dCC/dM (the oracle's matrix gradient) through M(angles) = (prior D(phi, theta, psi - phi))'."""
+    from emclarity_b200 import api
+    eps = 1e-5
+    out = []
+    for k in range(3):
+        pp = p.copy(); pp[k] += eps
+        pm = p.copy(); pm[k] -= eps
+        Mp = (prior @ api.define_matrix([pp[0], pp[1], pp[2] - pp[0]], "inv")).T
+        Mm = (prior @ api.define_matrix([pm[0], pm[1], pm[2] - pm[0]], "inv")).T
+        out.append(np.sum(dM * (Mp - Mm) / (2 * eps)))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("interp,oracle_interp", [("cubic", 1), ("linear", 0)])
+def test_adjoint_on_50_poses_against_the_fp64_gradient(setup, interp, oracle_interp):
+    """CC and the full 6-vector gradient of the device adjoint against the FP64 oracle's analytic
+    gradient (orc_cc_pose_interp) on 50 seeded poses with a non-trivial prior."""
+    from emclarity_b200 import api
+    prior = api.define_matrix([-20.0, 10.0, 35.0], "inv")
+    poses = _poses50()
+    cc, grad = _batch(setup, poses, interp, prior=prior)
+    hn = setup["h"].cpu().numpy()
+    rel = []
+    for i, p in enumerate(poses):
+        M = (prior @ api.define_matrix([p[0], p[1], p[2] - p[0]], "inv")).T
+        cco, dM, dt = O.cc_pose(setup["ref"], hn, setup["e"], M, p[3:], mask=setup["mask"], interp=oracle_interp)
+        assert abs(cc[i] - cco) <= 1e-4 * abs(cco) + 1e-6, (i, cc[i], cco)
+        go = np.concatenate([_angle_grad_from_dM(prior, p, dM), dt])
+        for part in (slice(0, 3), slice(3, 6)):
+            rel.append(np.linalg.norm(grad[i, part] - go[part]) / max(np.linalg.norm(go[part]), 1e-12))
+    rel = np.array(rel)
+    assert np.median(rel) < 1e-3 and rel.max() < 5e-3, (np.median(rel), rel.max())
+
+
+def test_adjoint_on_50_poses_against_finite_differences(setup):
+    """The tricubic gradient against central differences of the device forward value on 50 poses, all
+    600 displaced poses evaluated in one batched launch."""
+    from emclarity_b200 import api
+    prior = api.define_matrix([-20.0, 10.0, 35.0], "inv")
+    poses = _poses50(seed=51)
+    _, g0 = _batch(setup, poses, "cubic", prior=prior)
+    steps = np.array([0.02, 0.02, 0.02, 0.01, 0.01, 0.01])
+    disp = []
+    for p in poses:
+        for k in range(6):
+            for sg in (1, -1):
+                q = p.copy(); q[k] += sg * steps[k]
+                disp.append(q)
+    cc, _ = _batch(setup, np.array(disp), "cubic", prior=prior)
+    fd = ((cc[0::2] - cc[1::2]).reshape(50, 6)) / (2 * steps)
+    rel = []
+    for i in range(50):
+        for part in (slice(0, 3), slice(3, 6)):
+            rel.append(np.linalg.norm(g0[i, part] - fd[i, part]) / max(np.linalg.norm(fd[i, part]), 1e-12))
+    rel = np.array(rel)
+    assert np.median(rel) < 5e-3 and rel.max() < 3e-2, (np.median(rel), rel.max())
+
+
+def test_autograd_function_shim(setup):
+    """refine.CCPose (torch.autograd.Function over emc_cc_adjoint_batch): values equal the batched call,
+    backward scales the adjoint gradient by grad_out, and torch.autograd.gradcheck's finite differences
+    agree with the analytic Jacobian (tricubic objective, FP32 forward)."""
+    from emclarity_b200 import api, refine
+    k = 4
+    prior = api.define_matrix([-20.0, 10.0, 35.0], "inv")
+    obj = refine.BatchObjective(setup["s"], [setup["rid"]] * k, [setup["h"]] * k, [setup["e"]] * k, [prior] * k,
+                                interp="cubic")
+    x = torch.tensor(_poses50(seed=52)[:k], dtype=torch.float64, requires_grad=True)
+    cc = refine.CCPose.apply(x, obj)
+    cc_ref, g_ref = obj.cc_grad(x.detach().numpy())
+    assert np.array_equal(cc.detach().numpy(), cc_ref)
+    w = torch.tensor([1.0, -2.0, 0.5, 3.0], dtype=torch.float64)
+    (w * cc).sum().backward()
+    assert np.allclose(x.grad.numpy(), w.numpy()[:, None] * g_ref, rtol=1e-12, atol=0)
+    atol = 2e-2 * float(np.abs(g_ref).max())
+    assert torch.autograd.gradcheck(lambda t: refine.CCPose.apply(t, obj), (x.detach().requires_grad_(),),
+                                    eps=1e-2, atol=atol, rtol=2e-2, raise_exception=True)

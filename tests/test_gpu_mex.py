@@ -77,16 +77,20 @@ def test_mexEmcSearch_gateway(gateways):
     case = synthetic.PlainCase(seed=4)
     gd = case.to_gpu()
     grid = case.grid[::10]
-    cc, pk, best = gateways["mexEmcSearch"](3, gd["ref"], gd["mask"], gd["particle"], gd["weight"], np.eye(3),
-                                            grid, np.int32(7))
-    q, e = api.particle_spectrum(gd["particle"], gd["weight"])
-    s = api.Search(peak_radius=7)
-    rid = s.add_reference(gd["ref"], gd["mask"])
-    s.set_orientations(grid)
-    cc2, pk2, best2 = s.run_host([s.particle(q, e.item(), rid, orient_count=len(grid))])
-    assert np.allclose(cc.reshape(-1), cc2, atol=1e-6)
-    assert np.array_equal(pk, pk2)
-    assert int(best[0, 1]) == best2[0][1] + 1
+    # argument 4 is wdgMask (the particle's wedge, on the rotated reference), the optional 8th refWdg
+    ref_wdg = (0.5 + 0.5 * gd["weight"].abs()).contiguous()
+    for extra in ((), (ref_wdg,)):
+        cc, pk, best = gateways["mexEmcSearch"](3, gd["ref"], gd["mask"], gd["particle"], gd["weight"], np.eye(3),
+                                                grid, np.int32(7), *extra)
+        q, e = api.particle_spectrum(gd["particle"], *extra)
+        s = api.Search(peak_radius=7)
+        rid = s.add_reference(gd["ref"], gd["mask"])
+        s.set_orientations(grid)
+        cc2, pk2, best2 = s.run_host([s.particle(q, e.item(), rid, orient_count=len(grid), wedge=gd["weight"])])
+        s.close()
+        assert np.allclose(cc.reshape(-1), cc2, atol=1e-6)
+        assert np.array_equal(pk, pk2)
+        assert int(best[0, 1]) == best2[0][1] + 1
 
 
 # ------------------------------------------------------------------ the reference's own kernels

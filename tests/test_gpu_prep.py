@@ -69,7 +69,7 @@ def test_xcf_translational_matches_oracle(built_lib, cuda):
     ax = np.arange(n) - c
     zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
     pmask = ((xx ** 2 + yy ** 2 + zz ** 2) <= 36).astype(np.float32)
-    v_o, peak_o, map_o = O.xcf_translational(ref, q, e, M, peak_mask=pmask)
+    v_o, peak_o, map_o = O.xcf_translational(ref, q, M, peak_mask=pmask)
     R = np.fft.rfftn(ref.astype(np.float64))
     R.flat[0] = 0
     A = torch.from_numpy(q.astype(np.complex64)).cuda()

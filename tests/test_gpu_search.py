@@ -1,28 +1,18 @@
-"""Fused orientation search against the FP64 oracle (same inputs, same orientation list)."""
+"""Fused orientation search against the FP64 oracle (same inputs, same orientation list).
+
+Operands follow BH_multi_xcf_Translational_2.m:35-38 with BH_multi_xcf_Rotational's binding
+(BH_alignRaw3d_v2.m:1376-1383): the particle's own wedge.CTF weight is wdgMask and multiplies the
+rotated reference (the search descriptor's `wedge`); the reference's weight refWdg multiplies the
+particle (folded into its spectrum; 1 unless a test sets it).  Every peak or best-orientation
+difference must be a near-tie in the oracle's own map (tests/searchcheck.py)."""
 import numpy as np
 import pytest
 import torch
 
 from oracle import oracle as O
+from tests.searchcheck import check_best, check_cc_and_peaks
 
 pytestmark = pytest.mark.gpu
-
-RTOL = 1e-4   # CC relative tolerance
-ATOL = 1e-6
-
-
-def compare(cc_g, pk_g, cc_o, pk_o):
-    """CC within RTOL; integer peaks identical except at near-ties (where the GPU's CC at its own
-    peak equals the oracle's peak value within tolerance)."""
-    assert np.allclose(cc_g, cc_o, rtol=RTOL, atol=ATOL), np.abs(cc_g - cc_o).max()
-    mism = np.any(pk_g != pk_o, axis=1)
-    assert mism.mean() < 0.02, "too many peak mismatches: %d" % mism.sum()
-
-
-def best_nondegenerate(cc_o):
-    order = np.argsort(-cc_o, kind="stable")
-    gap = cc_o[order[0]] - cc_o[order[1]]
-    return order[0], gap > 10 * (RTOL * abs(cc_o[order[0]]) + ATOL)
 
 
 @pytest.fixture(scope="module")
@@ -33,38 +23,47 @@ def plain_case(built_lib, cuda):
     return case, g
 
 
-def run_gpu(case, g, grid, interp="linear", store="f32", wref=None, prior=None):
+def run_gpu(case, g, grid, interp="linear", store="f32", wref=None, prior=None, ref_wdg=None, radius=None):
     from emclarity_b200 import api
-    q, e = api.particle_spectrum(g["particle"], g["weight"])
-    s = api.Search(peak_radius=case.peak_radius, interp=interp)
+    q, e = api.particle_spectrum(g["particle"], ref_wdg)
+    s = api.Search(peak_radius=radius or case.peak_radius, interp=interp)
     rid = s.add_reference(g["ref"], g["mask"], wref, store=store)
     s.set_orientations(grid)
-    pdesc = s.particle(q, e.item(), rid, prior=prior, orient_count=len(grid))
+    pdesc = s.particle(q, e.item(), rid, prior=prior, orient_count=len(grid), wedge=g["weight"])
     cc, pk, best = s.run_host([pdesc])
     s.close()
-    return cc, pk, best, q, e.item()
+    return cc, pk, best
 
 
-def run_oracle(case, g, grid, interp=0, ref=None, wref=None, prior=None):
-    from emclarity_b200 import api
-    part = g["particle"].cpu().numpy()
-    w = g["weight"].cpu().numpy()
-    q, e = O.particle_spectrum(part, w)
-    mats = api.search_matrices(grid, prior)
-    ref = case.ref if ref is None else ref
-    return O.search(ref, q, e, mats, mask=case.mask, wref=wref, radius=case.peak_radius, interp=interp)
+class OracleRun:
+    """The FP64 oracle on the same operands; .map(o) gives orientation o's full map for tie checks."""
+
+    def __init__(self, case, g, grid, interp=0, ref=None, wref=None, prior=None, ref_wdg=None, radius=None):
+        from emclarity_b200 import api
+        self.P, _ = O.particle_spectrum(g["particle"].cpu().numpy())
+        self.kw = dict(mask=case.mask, wref=wref, ref_wdg=ref_wdg, wdg_mask=g["weight"].cpu().numpy(), interp=interp)
+        self.ref = case.ref if ref is None else ref
+        self.mats = api.search_matrices(grid, prior)
+        self.cc, self.pk = O.search(self.ref, self.P, self.mats, radius=radius or case.peak_radius, **self.kw)
+
+    def map(self, o):
+        return O.xcf_translational(self.ref, self.P, self.mats[o], **self.kw)[2]
+
+
+def compare(cc_g, pk_g, orc, what=""):
+    return check_cc_and_peaks(cc_g, pk_g, orc.cc, orc.pk, orc.map, what)
 
 
 def test_plain_search_parity_and_truth(plain_case):
     case, g = plain_case
     grid = case.grid
-    cc_g, pk_g, best, _, _ = run_gpu(case, g, grid)
-    cc_o, pk_o = run_oracle(case, g, grid)
-    compare(cc_g, pk_g, cc_o, pk_o)
-    b, nondeg = best_nondegenerate(cc_o)
-    if nondeg:
-        assert best[0][1] == b
-        assert tuple(best[0][2]) == tuple(pk_o[b])
+    cc_g, pk_g, best = run_gpu(case, g, grid)
+    orc = OracleRun(case, g, grid)
+    compare(cc_g, pk_g, orc, "plain")
+    check_best(best[0][1], orc.cc, what="plain")
+    b = int(np.argmax(orc.cc))
+    if best[0][1] == b:
+        assert tuple(best[0][2]) == tuple(orc.pk[b])
     # the planted shift is recovered at the best orientation
     assert tuple(best[0][2]) == tuple(int(v) for v in case.shift)
     # and the best orientation is the grid point nearest the truth
@@ -74,35 +73,70 @@ def test_plain_search_parity_and_truth(plain_case):
     assert ang[best[0][1]] <= np.sort(ang)[2] + 1e-9
 
 
+def test_wedges_on_both_sides_and_bandpass(plain_case):
+    """Different non-unit weights on both sides of the CC (refWdg on the particle, the particle's
+    wedge.CTF as wdgMask on the reference) plus a bandpass on the reference; swapping the two
+    weights' roles gives other CCs, so the binding is tested, not only the product."""
+    case, g = plain_case
+    n = case.n
+    rng = np.random.default_rng(17)
+    ref_wdg = O.even_weight_np(rng, n, 0.3, 1.4)[:, :, : n // 2 + 1].astype(np.float32)
+    k = np.fft.fftfreq(n)
+    kz, ky, kx = np.meshgrid(k, k, np.fft.rfftfreq(n), indexing="ij")
+    bp = np.exp(-(kx ** 2 + ky ** 2 + kz ** 2) / (2 * 0.2 ** 2)).astype(np.float32)
+    grid = case.grid[::6]
+    cc_g, pk_g, best = run_gpu(case, g, grid, wref=torch.from_numpy(bp).cuda(),
+                               ref_wdg=torch.from_numpy(ref_wdg).cuda())
+    orc = OracleRun(case, g, grid, wref=bp, ref_wdg=ref_wdg)
+    compare(cc_g, pk_g, orc, "two wedges")
+    check_best(best[0][1], orc.cc, what="two wedges")
+    swapped, _ = O.search(case.ref, orc.P, orc.mats, radius=case.peak_radius, mask=case.mask, wref=bp,
+                          ref_wdg=g["weight"].cpu().numpy(), wdg_mask=ref_wdg)
+    assert np.abs(swapped - orc.cc).max() > 1e-2 * np.abs(orc.cc).max()
+
+
 def test_cubic_and_border_modes(plain_case):
     case, g = plain_case
     grid = case.grid[::9]
     for interp, mode in (("cubic", 1), ("linear_border", 2)):
-        cc_g, pk_g, _, _, _ = run_gpu(case, g, grid, interp=interp)
-        cc_o, pk_o = run_oracle(case, g, grid, interp=mode)
-        compare(cc_g, pk_g, cc_o, pk_o)
+        cc_g, pk_g, best = run_gpu(case, g, grid, interp=interp)
+        orc = OracleRun(case, g, grid, interp=mode)
+        compare(cc_g, pk_g, orc, interp)
+        check_best(best[0][1], orc.cc, what=interp)
 
 
 def test_reference_weight_path(plain_case):
-    """A real half-spectrum weight on the rotated reference (bandpass): E_R from the spectrum."""
+    """A real half-spectrum bandpass on the rotated reference and no particle wedge: the weighted
+    E_R comes from one weight only."""
     case, g = plain_case
     n = case.n
     k = np.fft.fftfreq(n)
     kz, ky, kx = np.meshgrid(k, k, np.fft.rfftfreq(n), indexing="ij")
     bp = np.exp(-(kx ** 2 + ky ** 2 + kz ** 2) / (2 * 0.18 ** 2)).astype(np.float32)
     grid = case.grid[::7]
-    cc_g, pk_g, _, _, _ = run_gpu(case, g, grid, wref=torch.from_numpy(bp).cuda())
-    cc_o, pk_o = run_oracle(case, g, grid, wref=bp)
-    compare(cc_g, pk_g, cc_o, pk_o)
+    from emclarity_b200 import api
+    q, e = api.particle_spectrum(g["particle"], g["weight"])
+    s = api.Search(peak_radius=case.peak_radius)
+    rid = s.add_reference(g["ref"], g["mask"], torch.from_numpy(bp).cuda())
+    s.set_orientations(grid)
+    cc_g, pk_g, best = s.run_host([s.particle(q, e.item(), rid, orient_count=len(grid))])
+    s.close()
+    P, _ = O.particle_spectrum(g["particle"].cpu().numpy())
+    kw = dict(mask=case.mask, wref=bp, ref_wdg=g["weight"].cpu().numpy())
+    mats = api.search_matrices(grid)
+    cc_o, pk_o = O.search(case.ref, P, mats, radius=case.peak_radius, **kw)
+    check_cc_and_peaks(cc_g, pk_g, cc_o, pk_o, lambda o: O.xcf_translational(case.ref, P, mats[o], **kw)[2], "wref")
+    check_best(best[0][1], cc_o, what="wref")
 
 
 def test_bf16_reference_storage(plain_case):
     case, g = plain_case
     grid = case.grid[::5]
-    cc_g, pk_g, _, _, _ = run_gpu(case, g, grid, store="bf16")
+    cc_g, pk_g, best = run_gpu(case, g, grid, store="bf16")
     ref_bf = torch.from_numpy(case.ref).to(torch.bfloat16).float().numpy()
-    cc_o, pk_o = run_oracle(case, g, grid, ref=ref_bf)
-    compare(cc_g, pk_g, cc_o, pk_o)
+    orc = OracleRun(case, g, grid, ref=ref_bf)
+    compare(cc_g, pk_g, orc, "bf16")
+    check_best(best[0][1], orc.cc, what="bf16")
 
 
 def test_prior_composition(plain_case):
@@ -111,9 +145,53 @@ def test_prior_composition(plain_case):
     case, g = plain_case
     prior = api.define_matrix([33.0, 21.0, -48.0], "inv")
     grid = case.grid[::11]
-    cc_g, pk_g, _, _, _ = run_gpu(case, g, grid, prior=prior)
-    cc_o, pk_o = run_oracle(case, g, grid, prior=prior)
-    compare(cc_g, pk_g, cc_o, pk_o)
+    cc_g, pk_g, best = run_gpu(case, g, grid, prior=prior)
+    orc = OracleRun(case, g, grid, prior=prior)
+    compare(cc_g, pk_g, orc, "prior")
+    check_best(best[0][1], orc.cc, what="prior")
+
+
+def _uneven_batch(rng, s, boxes, grid, radius, slices=True, store="f32"):
+    """Particles of the given boxes (C2 recipe: seeded prior, truth within a few degrees of it,
+    integer shift, defocus U[1.5, 4] um, tilt range +/-U[50, 65] deg, SNR 0.1) registered on s."""
+    from emclarity_b200 import api, synthetic
+    refs, descs, keep, oracle_in = {}, [], [], []
+    for n in sorted(set(boxes)):
+        ref = synthetic.blob_reference(rng, n)
+        mask = synthetic.soft_sphere_mask(n, 28 * n / 64)
+        refs[n] = (ref, mask, s.add_reference(torch.from_numpy(ref).cuda(), torch.from_numpy(mask).cuda(), store=store))
+    for i, n in enumerate(boxes):
+        ref, mask, rid = refs[n]
+        prior = api.define_matrix(synthetic.random_euler(rng), "inv")
+        truth = prior @ api.define_matrix([rng.uniform(-6, 6), rng.uniform(0, 6), rng.uniform(-6, 6)], "inv")
+        shift = rng.integers(-4, 5, 3)
+        wt = api.wedge_ctf_weight(n, -rng.uniform(50, 65), rng.uniform(50, 65),
+                                  synthetic.ctf_dict(rng.uniform(15000, 40000)))
+        part = synthetic.make_particle(torch.from_numpy(ref).cuda(), rng, truth, shift, wt, 0.1)
+        q, e = api.particle_spectrum(part)
+        keep += [q, wt]
+        begin = (3 * i) % 8 if slices else 0
+        descs.append(s.particle(q, e.item(), rid, prior=prior, orient_begin=begin, orient_count=len(grid) - begin,
+                                wedge=wt))
+        oracle_in.append((ref, mask, part.cpu().numpy(), wt.cpu().numpy(), prior, begin))
+    return descs, keep, oracle_in
+
+
+def _check_uneven(grid, descs, oracle_in, cc_g, pk_g, best, radius, ref_override=None):
+    from emclarity_b200 import api
+    off = 0
+    for k, ((ref, mask, part, wt, prior, begin), hit) in enumerate(zip(oracle_in, best)):
+        ref = ref_override(ref) if ref_override else ref
+        P, _ = O.particle_spectrum(part)
+        mats = api.search_matrices(grid[begin:], prior)
+        kw = dict(mask=mask, wdg_mask=wt)
+        cc_o, pk_o = O.search(ref, P, mats, radius=radius, **kw)
+        m = len(grid) - begin
+        check_cc_and_peaks(cc_g[off:off + m], pk_g[off:off + m], cc_o, pk_o,
+                           lambda o: O.xcf_translational(ref, P, mats[o], **kw)[2], "particle %d" % k)
+        if check_best(hit[1], cc_o, offset=begin, what="particle %d" % k):
+            assert tuple(hit[2]) == tuple(pk_o[hit[1] - begin])
+        off += m
 
 
 def test_batched_uneven_matches_oracle(built_lib, cuda):
@@ -122,41 +200,30 @@ def test_batched_uneven_matches_oracle(built_lib, cuda):
     rng = np.random.default_rng(21)
     grid = synthetic.local_grid(24, 8.0, 2.0)
     s = api.Search(peak_radius=5)
-    refs, descs, oracle_in = {}, [], []
-    for n in (64, 96, 128):
-        ref = synthetic.blob_reference(rng, n)
-        mask = synthetic.soft_sphere_mask(n, 28 * n / 64)
-        refs[n] = (ref, mask, s.add_reference(torch.from_numpy(ref).cuda(), torch.from_numpy(mask).cuda()))
     s.set_orientations(grid)
-    keep = []
-    for i, n in enumerate([64, 96, 64, 128, 96]):
-        ref, mask, rid = refs[n]
-        prior = api.define_matrix(rng.uniform(-90, 90, 3), "inv")
-        truth = prior @ api.define_matrix([rng.uniform(0, 5), rng.uniform(0, 5), rng.uniform(-5, 5)], "inv")
-        shift = rng.integers(-3, 4, 3)
-        wt = api.wedge_ctf_weight(n, -55, 62, synthetic.ctf_dict(rng.uniform(15000, 40000)))
-        part = synthetic.make_particle(torch.from_numpy(ref).cuda(), rng, truth, shift, wt, 0.5)
-        q, e = api.particle_spectrum(part, wt)
-        keep.append(q)
-        begin = (3 * i) % 8
-        descs.append(s.particle(q, e.item(), rid, prior=prior, orient_begin=begin, orient_count=len(grid) - begin))
-        oracle_in.append((ref, mask, part.cpu().numpy(), wt.cpu().numpy(), prior, begin))
+    descs, keep, oracle_in = _uneven_batch(rng, s, [64, 96, 64, 128, 96], grid, 5)
     cc_g, pk_g, best = s.run_host(descs)
-    off = 0
-    for (ref, mask, part, wt, prior, begin), hit in zip(oracle_in, best):
-        q, e = O.particle_spectrum(part, wt)
-        mats = api.search_matrices(grid[begin:], prior)
-        cc_o, pk_o = O.search(ref, q, e, mats, mask=mask, radius=5)
-        m = len(grid) - begin
-        compare(cc_g[off:off + m], pk_g[off:off + m], cc_o, pk_o)
-        b, nondeg = best_nondegenerate(cc_o)
-        if nondeg:
-            assert hit[1] == begin + b
-            assert tuple(hit[2]) == tuple(pk_o[b])
-        off += m
+    _check_uneven(grid, descs, oracle_in, cc_g, pk_g, best, 5)
     # the same request again replays the captured graph and gives identical results
     cc2, pk2, best2 = s.run_host(descs)
     assert np.array_equal(cc2, cc_g) and np.array_equal(pk2, pk_g)
+
+
+def test_batched_uneven_c2_shape(built_lib, cuda):
+    """The batched uneven configuration at parity scale: 20 particles (12 x 64^3, 6 x 96^3, 2 x 128^3,
+    the 60/30/10 split) x 256 local orientations within 8 degrees of each particle's prior, peak
+    radius 7, one call; every CC, peak and best orientation against the FP64 oracle."""
+    from emclarity_b200 import api, synthetic
+    rng = np.random.default_rng(2000)
+    grid = synthetic.local_grid(256, 8.0, 2.0)
+    boxes = [int(b) for b in synthetic.batched_sizes(20, seed=3)]
+    assert sorted(boxes).count(64) == 12 and boxes.count(96) == 6 and boxes.count(128) == 2
+    s = api.Search(peak_radius=7)
+    s.set_orientations(grid)
+    descs, keep, oracle_in = _uneven_batch(rng, s, boxes, grid, 7, slices=False)
+    cc_g, pk_g, best = s.run_host(descs)
+    _check_uneven(grid, descs, oracle_in, cc_g, pk_g, best, 7)
+    s.close()
 
 
 def test_graph_replay_device_outputs(plain_case):
@@ -228,9 +295,9 @@ def test_planes_per_cta_options_agree(built_lib, cuda, store):
         wt = api.wedge_ctf_weight(n, -55, 62, synthetic.ctf_dict(25000.0))
         truth = api.define_matrix([2.0, 4.0, -3.0], "inv")
         part = synthetic.make_particle(torch.from_numpy(ref).cuda(), rng, truth, (1, 0, -1), wt, 0.5)
-        q, e = api.particle_spectrum(part, wt)
-        keep.append(q)
-        descs.append(s.particle(q, e.item(), rid, orient_count=len(grid)))
+        q, e = api.particle_spectrum(part)
+        keep += [q, wt]
+        descs.append(s.particle(q, e.item(), rid, orient_count=len(grid), wedge=wt))
     s.set_orientations(grid)
     cc0, pk0, best0 = s.run_host(descs)
     for n in (64, 96, 128):
@@ -260,21 +327,13 @@ def test_planes_per_cta_options_agree(built_lib, cuda, store):
 @pytest.mark.parametrize("radius", [12, 15])
 def test_large_peak_radius_matches_oracle(plain_case, radius):
     """Peak windows up to the largest supported radius (15: 31 rows / 16 row pairs in pass C)."""
-    from emclarity_b200 import api
     case, g = plain_case
     grid = case.grid[::20]
-    q, e = api.particle_spectrum(g["particle"], g["weight"])
-    s = api.Search(peak_radius=radius)
-    rid = s.add_reference(g["ref"], g["mask"])
-    s.set_orientations(grid)
-    cc, pk, best = s.run_host([s.particle(q, e.item(), rid, orient_count=len(grid))])
-    part = g["particle"].cpu().numpy()
-    w = g["weight"].cpu().numpy()
-    qo, eo = O.particle_spectrum(part, w)
-    cc_o, pk_o = O.search(case.ref, qo, eo, api.search_matrices(grid), mask=case.mask, radius=radius)
-    compare(cc, pk, cc_o, pk_o)
+    cc, pk, best = run_gpu(case, g, grid, radius=radius)
+    orc = OracleRun(case, g, grid, radius=radius)
+    compare(cc, pk, orc, "radius %d" % radius)
+    check_best(best[0][1], orc.cc, what="radius %d" % radius)
     assert np.all(np.sum(pk.astype(float) ** 2, axis=1) <= radius * radius)
-    s.close()
 
 
 def test_device_energies_match_host_energies(plain_case):

@@ -129,7 +129,7 @@ def test_search_oracle_finds_planted_shift():
     d = (2, -1, 3)
     part = np.roll(ref, (d[2], d[1], d[0]), axis=(0, 1, 2))
     q, e = O.particle_spectrum(part)
-    cc, pk = O.search(ref, q, e, [np.eye(3)], radius=5)
+    cc, pk = O.search(ref, q, [np.eye(3)], radius=5)
     assert tuple(pk[0]) == d
     assert abs(cc[0] - 1.0) < 1e-9
 
@@ -142,16 +142,75 @@ def test_search_oracle_matches_full_map():
     part = rng.standard_normal((n, n, n))
     q, e = O.particle_spectrum(part)
     M = O.define_matrix([10, 20, 30], "inv")
-    cc, pk = O.search(ref, q, e, [M], radius=4)
+    cc, pk = O.search(ref, q, [M], radius=4)
     c = n // 2
     ax = np.arange(n) - c
     zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
     pmask = ((xx ** 2 + yy ** 2 + zz ** 2) <= 16).astype(np.float64)
-    v, peak, full = O.xcf_translational(ref, q, e, M, peak_mask=pmask)
+    v, peak, full = O.xcf_translational(ref, q, M, peak_mask=pmask)
     full_masked = np.where(pmask > 0.5, full, -np.inf)
     idx = np.unravel_index(np.argmax(full_masked), full.shape)
     assert (idx[2] - c, idx[1] - c, idx[0] - c) == tuple(pk[0])
     assert abs(full_masked[idx] - cc[0]) < 1e-12
+
+
+def _xcf2_case(seed, n=16):
+    """Reference, particle, mask, bandpasses and two different non-unit even weights."""
+    rng = np.random.default_rng(seed)
+    ax = np.arange(n) - n // 2
+    zz, yy, xx = np.meshgrid(ax, ax, ax, indexing="ij")
+    ref = np.exp(-((xx - 1) ** 2 + (yy + 2) ** 2 + zz ** 2) / 6.0) + 0.7 * np.exp(-((xx + 3) ** 2 + yy ** 2 + (zz - 2) ** 2) / 3.0)
+    ref += 0.1 * rng.standard_normal(ref.shape)
+    mask = np.clip(1.2 - np.sqrt(xx ** 2 + yy ** 2 + zz ** 2) / 6.0, 0, 1)
+    part = np.roll(ref, (1, -2, 2), axis=(0, 1, 2)) + 0.3 * rng.standard_normal(ref.shape)
+    k = np.fft.fftfreq(n)
+    kz, ky, kx = np.meshgrid(k, k, k, indexing="ij")
+    s2 = kx ** 2 + ky ** 2 + kz ** 2
+    bp_part = np.exp(-s2 / (2 * 0.22 ** 2))         # bandpassFilt (particle)
+    bp_ref = np.exp(-s2 / (2 * 0.3 ** 2))           # bandpassFiltREF (rotated reference)
+    w_part = O.even_weight_np(rng, n, 0.1, 2.0)     # wdgMask (multiplies the reference)
+    w_ref = O.even_weight_np(rng, n, 0.5, 1.5)      # refWdg (multiplies the particle)
+    return ref, mask, part, bp_part, bp_ref, w_part, w_ref
+
+
+def test_search_oracle_is_the_literal_translational_2_formula():
+    """orc_xcf_translational's map equals a numpy transcription of BH_multi_xcf_Translational_2.m:35-38
+    on full spectra, with different non-unit weights on both sides, a reference bandpass, a mask, a
+    rotation and a shift; its zero-lag value equals BH_multi_xcf_Rotational (:71-78) of the same
+    operands; orc_search's windowed peak is the map's masked maximum."""
+    n = 16
+    ref, mask, part, bp_part, bp_ref, w_part, w_ref = _xcf2_case(9, n)
+    h = n // 2 + 1
+    M = O.define_matrix([12.0, 25.0, -40.0], "inv")
+    shift = (0.5, -1.0, 0.25)
+    # operands as at BH_alignRaw3d_v2.m:1287-1330 (the reference through RotMat', 'forward')
+    P_full = np.fft.fftn(part)
+    P_full.flat[0] = 0
+    P_full *= bp_part
+    r = O.rotate(ref, M.T, shift, "forward") * mask
+    R_full = np.fft.fftn(r) * bp_ref
+    R_full.flat[0] = 0
+    want = O.xcf_translational_2_np(P_full, np.conj(R_full), w_part, w_ref)
+    P_half, _ = O.particle_spectrum(part, bandpass=bp_part[:, :, :h])
+    c = n // 2
+    zz, yy, xx = np.meshgrid(*(np.arange(n) - c,) * 3, indexing="ij")
+    pmask = ((xx ** 2 + yy ** 2 + zz ** 2) <= 9).astype(np.float64)
+    v, peak, got = O.xcf_translational(ref, P_half, M, mask=mask, wref=bp_ref[:, :, :h], ref_wdg=w_ref[:, :, :h],
+                                       wdg_mask=w_part[:, :, :h], shift=shift, peak_mask=pmask)
+    assert np.abs(got - want).max() < 1e-12 * np.abs(want).max()
+    rot = O.xcf_rotational_np(P_half, np.conj(R_full[:, :, :h]), w_part[:, :, :h], w_ref[:, :, :h], nx=n)
+    assert abs(got[c, c, c] - rot) < 1e-12 * abs(rot)
+    cc, pk = O.search(ref, P_half, [M], mask=mask, wref=bp_ref[:, :, :h], ref_wdg=w_ref[:, :, :h],
+                      wdg_mask=w_part[:, :, :h], shift=shift, radius=3)
+    masked = np.where(pmask > 0.5, want, -np.inf)
+    idx = np.unravel_index(np.argmax(masked), masked.shape)
+    assert (idx[2] - c, idx[1] - c, idx[0] - c) == tuple(pk[0])
+    assert abs(masked[idx] - cc[0]) < 1e-12 * abs(cc[0])
+    # the wedges matter: swapping their roles changes the normalisation (so a test that used only one
+    # binding could not tell them apart)
+    v_sw, _, got_sw = O.xcf_translational(ref, P_half, M, mask=mask, wref=bp_ref[:, :, :h], ref_wdg=w_part[:, :, :h],
+                                          wdg_mask=w_ref[:, :, :h], shift=shift)
+    assert abs(got_sw[c, c, c] - got[c, c, c]) > 1e-3 * abs(got[c, c, c])
 
 
 def test_f32_port_agrees_with_f64_oracle():
@@ -163,8 +222,9 @@ def test_f32_port_agrees_with_f64_oracle():
     mats = [O.define_matrix([a, 10, -a], "inv") for a in (0, 20, 40)]
     q64, e64 = O.particle_spectrum(part)
     q32, e32 = O.particle_spectrum(part, precision="f32")
-    cc64, pk64 = O.search(ref, q64, e64, mats, radius=4)
-    cc32, pk32 = O.search(ref, q32, e32, mats, radius=4, precision="f32")
+    w64 = O.even_weight_np(rng, n)[:, :, : n // 2 + 1]
+    cc64, pk64 = O.search(ref, q64, mats, radius=4, wdg_mask=w64)
+    cc32, pk32 = O.search(ref, q32, mats, radius=4, wdg_mask=w64, precision="f32")
     assert np.allclose(cc32, cc64, rtol=1e-4, atol=1e-6)
     assert np.array_equal(pk32, pk64)
 
@@ -191,3 +251,19 @@ def test_cc_pose_gradient_matches_finite_differences():
         tm = t.copy(); tm[j] -= eps
         fd = (O.cc_pose(ref, h, 2.0, M, tp)[0] - O.cc_pose(ref, h, 2.0, M, tm)[0]) / (2 * eps)
         assert abs(fd - dt[j]) < 1e-6 * max(1.0, abs(fd)) + 1e-8
+
+
+def test_pocketfft_arm_matches_oracle():
+    """The second CPU arm (numpy + scipy.fft in spawned processes) computes the oracle's CCs and peaks."""
+    from oracle import pocketfft_arm as PF
+    n = 16
+    ref, mask, part, bp_part, bp_ref, w_part, w_ref = _xcf2_case(13, n)
+    h = n // 2 + 1
+    P, _ = O.particle_spectrum(part, bandpass=bp_part[:, :, :h])
+    mats = [O.define_matrix([a, 15.0, -2 * a], "inv") for a in range(0, 90, 15)]
+    kw = dict(mask=mask, wref=bp_ref[:, :, :h], ref_wdg=w_ref[:, :, :h], wdg_mask=w_part[:, :, :h], shift=(1, 0, -1))
+    cc, pk = O.search(ref, P, mats, radius=3, **kw)
+    with PF.Pool(ref, P, radius=3, processes=2, **kw) as pool:
+        cc2, pk2 = pool.search(mats)
+    assert np.allclose(cc2, cc, rtol=1e-4, atol=1e-6)
+    assert np.array_equal(pk2, pk)
