@@ -546,58 +546,148 @@ def _timed(fn, reps=1):
     return (time.time() - t0) / reps, out
 
 
-def run_mixed(args, store="f32"):
-    """Batched uneven alignment: 60% 64^3, 30% 96^3, 10% 128^3, 256 local orientations each, seeded
-    defocus in [1.5, 4] um and tilt range in [+-50, +-65] deg, one emc_search_run per step."""
+def mixed_batch(n_part, seed=2024):
+    """The batched uneven configuration: n_part particles split 60/30/10 over 64^3 / 96^3 / 128^3 in a
+    seeded order, each made like the plain case with a seeded defocus in [1.5, 4] um, tilt range
+    +/-U[50, 65] deg, SNR 0.1, and a truth within 8 degrees of a seeded prior.  Returns host-side
+    records (box, prior, truth, shift) and device particles / wedges / references."""
     import torch
 
     from emclarity_b200 import api, synthetic
-    n_part = args.particles if args.particles != 1200 else 2000
     sizes = synthetic.batched_sizes(n_part, seed=3)
-    rng = np.random.default_rng(2024)
-    grid = synthetic.local_grid(N_ORIENT, 8.0, 2.0)
-    s = api.Search(peak_radius=PEAK_RADIUS)
+    rng = np.random.default_rng(seed)
     refs, fts = {}, {}
     for n in (64, 96, 128):
         ref = synthetic.blob_reference(rng, n)
         mask = synthetic.soft_sphere_mask(n, 28 * n / 64)
-        rg = torch.from_numpy(ref).cuda()
-        refs[n] = (rg, s.add_reference(rg, torch.from_numpy(mask).cuda(), store=store))
+        refs[n] = (ref, mask, torch.from_numpy(ref).cuda(), torch.from_numpy(mask).cuda())
         fts[n] = api.FourierTransformer((n, n, n))
-    s.set_orientations(grid)
-    descs, keep = [], []
+    parts = []
     for n in sizes:
+        n = int(n)
         prior = api.define_matrix(synthetic.random_euler(rng), "inv")
         truth = prior @ api.define_matrix([rng.uniform(-6, 6), rng.uniform(0, 6), rng.uniform(-6, 6)], "inv")
-        w = api.wedge_ctf_weight(int(n), -rng.uniform(50, 65), rng.uniform(50, 65),
+        shift = rng.integers(-4, 5, 3)
+        w = api.wedge_ctf_weight(n, -rng.uniform(50, 65), rng.uniform(50, 65),
                                  synthetic.ctf_dict(rng.uniform(15000, 40000)))
-        p = synthetic.make_particle(refs[n][0], rng, truth, rng.integers(-4, 5, 3), w, 0.1, ft=fts[n])
+        p = synthetic.make_particle(refs[n][2], rng, truth, shift, w, 0.1, ft=fts[n])
         q, e = api.particle_spectrum(p)
-        keep += [q, w]
-        descs.append(s.particle(q, e.item(), refs[n][1], prior=prior, orient_count=N_ORIENT, wedge=w))
-        del p
-    evals = len(descs) * N_ORIENT
+        parts.append(dict(n=n, prior=prior, truth=truth, shift=shift, wedge=w, spec=q, energy=e.item(),
+                          particle=p))
+    return sizes, refs, parts
+
+
+def time_mixed(parts, refs, store, steps, warmup, grid):
+    """One emc_search_run over every particle of the batch with the reference stored as `store`."""
+    import torch
+
+    from emclarity_b200 import api
+    s = api.Search(peak_radius=PEAK_RADIUS)
+    rids = {n: s.add_reference(refs[n][2], refs[n][3], store=store) for n in (64, 96, 128)}
+    s.set_orientations(grid)
+    descs = [s.particle(p["spec"], p["energy"], rids[p["n"]], prior=p["prior"], orient_count=len(grid),
+                        wedge=p["wedge"]) for p in parts]
     best = torch.empty((len(descs), 5), dtype=torch.int32, device="cuda")
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         s.run(descs, best=best)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         s.run(descs, best=best)
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    counts = {int(n): int(np.sum(sizes == n)) for n in (64, 96, 128)}
-    byts = sum(compulsory_bytes(n, c * N_ORIENT, c, 1, store) for n, c in counts.items())
+    ms = e0.elapsed_time(e1) / steps
+    launches = s.timings()["launches_last_run"]
+    s.close()
+    return ms, launches, best.cpu().numpy()
+
+
+def mixed_entry(sizes, parts, refs, store, steps, warmup, grid):
+    ms, launches, _ = time_mixed(parts, refs, store, steps, warmup, grid)
+    evals = len(parts) * len(grid)
+    counts = {n: int(np.sum(sizes == n)) for n in (64, 96, 128)}
+    byts = sum(compulsory_bytes(n, c * len(grid), c, 1, store) for n, c in counts.items())
     peak, which = measured_peaks()
     return {"metric": "CC evals/s, batched uneven boxes" + (" (BF16 reference storage)" if store == "bf16" else ""),
-            "value": evals / (ms / 1e3), "unit": "CC evals/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "dtype": store,
-            "data": "synthetic", "config": {"workload": "%d particles (%s) x %d local orientations, one call" %
-                                            (len(descs), counts, N_ORIENT), "store": store},
+            "value": evals / (ms / 1e3), "unit": "CC evals/s", "steps": steps, "warmup": warmup, "ms_per_step": ms,
+            "dtype": store, "gpu_launches_per_step": launches,
+            "config": {"workload": "%d particles (%s) x %d local orientations (8 deg of a seeded prior), peak radius "
+                                   "%d, one emc_search_run (CUDA graph) per step" % (len(parts), counts, len(grid),
+                                                                                      PEAK_RADIUS), "store": store},
             "roofline": {"bound": "hbm", "achieved": byts / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": byts / (ms / 1e3) / 1e9 / peak, "peak_source": which}}
+                         "frac": byts / (ms / 1e3) / 1e9 / peak, "peak_source": which,
+                         "model": "compulsory bytes: particles x (8 + 4) nh n^2 + references' cells and masks + 16 B "
+                                  "per evaluation"}}
+
+
+def bf16_report(sizes, refs, parts, grid, n_sub=200, orient_stride=16):
+    """Mixed precision against the FP64 oracle: over a seeded subset of n_sub particles (every box size
+    in its share) and every orient_stride-th orientation of the local grid, the CCs and best
+    orientations of the search with BF16 reference storage (and with FP32 storage, as the control)
+    against the FP64 oracle on the unrounded reference."""
+    import torch
+
+    from emclarity_b200 import api
+    from oracle import oracle as O
+    rng = np.random.default_rng(200)
+    sub = np.sort(rng.choice(len(parts), size=min(n_sub, len(parts)), replace=False))
+    g = grid[::orient_stride]
+    out = {}
+    orc = []
+    for i in sub:
+        p = parts[i]
+        ref, mask = refs[p["n"]][0], refs[p["n"]][1]
+        P, _ = O.particle_spectrum(p["particle"].cpu().numpy())
+        cc, pk = O.search(ref, P, api.search_matrices(g, p["prior"]), mask=mask, wdg_mask=p["wedge"].cpu().numpy(),
+                          radius=PEAK_RADIUS)
+        orc.append((cc, pk))
+    for store in ("bf16", "f32"):
+        s = api.Search(peak_radius=PEAK_RADIUS)
+        rids = {n: s.add_reference(refs[n][2], refs[n][3], store=store) for n in (64, 96, 128)}
+        s.set_orientations(g)
+        descs = [s.particle(parts[i]["spec"], parts[i]["energy"], rids[parts[i]["n"]], prior=parts[i]["prior"],
+                            orient_count=len(g), wedge=parts[i]["wedge"]) for i in sub]
+        cc_g, pk_g, best = s.run_host(descs)
+        s.close()
+        cc_g = cc_g.reshape(len(sub), len(g))
+        rel = np.concatenate([np.abs(cc_g[k] - orc[k][0]) / np.abs(orc[k][0]) for k in range(len(sub))])
+        agree, near, ang = 0, 0, []
+        for k in range(len(sub)):
+            b_o = int(np.argmax(orc[k][0]))
+            b_g = best[k][1]
+            if b_g == b_o:
+                agree += 1
+            else:
+                gap = abs(orc[k][0][b_g] - orc[k][0][b_o]) / abs(orc[k][0][b_o])
+                near += gap <= 1e-3
+                Ra = api.search_matrices([g[b_g]], parts[sub[k]]["prior"])[0]
+                Rb = api.search_matrices([g[b_o]], parts[sub[k]]["prior"])[0]
+                ang.append(float(np.degrees(np.arccos(np.clip((np.trace(Ra.T @ Rb) - 1) / 2, -1, 1)))))
+        pk_agree = float(np.mean([np.array_equal(pk_g[k * len(g) + int(np.argmax(orc[k][0]))],
+                                                 orc[k][1][int(np.argmax(orc[k][0]))]) for k in range(len(sub))]))
+        out[store] = {"cc_rel_err_median": float(np.median(rel)), "cc_rel_err_p99": float(np.percentile(rel, 99)),
+                      "cc_rel_err_max": float(rel.max()), "best_orientation_agreement": agree / len(sub),
+                      "disagreements_within_1e-3_of_the_oracle_best": int(near),
+                      "disagreement_angles_deg": ang, "peak_agreement_at_oracle_best": pk_agree}
+    counts = {n: int(np.sum(np.array([parts[i]["n"] for i in sub]) == n)) for n in (64, 96, 128)}
+    return {"particles": len(sub), "boxes": counts, "orientations_per_particle": len(g),
+            "oracle": "FP64 CPU oracle on the unrounded (FP32) reference", **out}
+
+
+def run_mixed(args, store="f32"):
+    """Batched uneven alignment: 60% 64^3, 30% 96^3, 10% 128^3, 256 local orientations each, seeded
+    defocus in [1.5, 4] um and tilt range in [+-50, +-65] deg, one emc_search_run per step.  With BF16
+    storage, the report against the FP64 oracle on a 200-particle subset is added."""
+    from emclarity_b200 import synthetic
+    n_part = args.particles if args.particles != 1200 else 2000
+    grid = synthetic.local_grid(N_ORIENT, 8.0, 2.0)
+    sizes, refs, parts = mixed_batch(n_part)
+    res = mixed_entry(sizes, parts, refs, store, args.steps, args.warmup, grid)
+    res.update({"n_gpus": 1, "higher_is_better": True, "data": "synthetic"})
+    if store == "bf16":
+        res["vs_fp64_oracle"] = bf16_report(sizes, refs, parts, grid)
+    return res
 
 
 def run_tsearch(args):
@@ -935,7 +1025,7 @@ def _rodrigues(axis, deg):
     return np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
 
 
-def run_refine(args):
+def run_refine(args, n_part=None):
     """Gradient pose refinement: 96^3 particles at SNR 0.05, coarse 15-degree local search (95
     orientations around a seeded prior within 12 degrees of the truth), then either 20 L-BFGS steps on
     the forward + adjoint CC or a dense 1-degree local grid (3,859 orientations) around the coarse best;
@@ -944,7 +1034,7 @@ def run_refine(args):
 
     from emclarity_b200 import api, refine, synthetic
     n = 96
-    n_part = args.particles if args.particles != 1200 else 1000
+    n_part = n_part or (args.particles if args.particles != 1200 else 1000)
     rng = np.random.default_rng(96)
     ref = synthetic.blob_reference(rng, n)
     mask = synthetic.soft_sphere_mask(n, 28 * n / 64)
@@ -1029,6 +1119,23 @@ def run_refine(args):
             "speedup_total": (t_coarse + t_dense) / (t_coarse + lin["seconds"])}
 
 
+def run_extras(args):
+    """Keys of the default line beside the headline: the batched uneven configuration (2,000 particles,
+    60/30/10 over 64^3 / 96^3 / 128^3, 256 local orientations each) with FP32 and with BF16 reference
+    storage (one warm-up and two timed runs each), and a bounded pose refinement (200 x 96^3)."""
+    import torch
+
+    from emclarity_b200 import synthetic
+    grid = synthetic.local_grid(N_ORIENT, 8.0, 2.0)
+    sizes, refs, parts = mixed_batch(2000)
+    out = {"mixed": mixed_entry(sizes, parts, refs, "f32", 2, 1, grid),
+           "mixed_bf16": mixed_entry(sizes, parts, refs, "bf16", 2, 1, grid)}
+    del parts, refs
+    torch.cuda.empty_cache()
+    out["refine"] = run_refine(args, n_part=200)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1037,6 +1144,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--particles", type=int, default=1200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched-uneven (FP32, BF16) and refinement keys of the default line")
     ap.add_argument("--planes", type=int, default=0, help="pass-A z-planes per CTA (0: timed choice)")
     ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine", "average", "formats",
                                                                     "tsearch_post"])
@@ -1059,6 +1168,8 @@ def main():
     world, rank, local = dist_setup()
     res = run_ours(args, world, rank, local)
     if rank == 0:
+        if not args.no_extras and world == 1:
+            res.update(run_extras(args))
         if not args.no_cpu_baseline and world == 1:
             res["cpu_baseline"] = cpu_baseline_entry(seconds=10.0)
         print(json.dumps(res))

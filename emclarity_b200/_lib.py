@@ -76,6 +76,9 @@ SIGNATURES = {
     "emc_fft_c2r": (_i, [_vp, _vp, _vp, _vp]),
     "emc_fft_destroy": (_i, [_vp]),
     "emc_ctf2d": (_i, [C.POINTER(CtfParams), _i, _i, _i, _i, _i, _vp, _vp]),
+    "emc_binary_wedge": (_i, [_i, _f, _f, _i, _i, _vp, _vp]),
+    "emc_mask_sphere": (_i, [_pi, _pd, _pd, _d, _vp, _vp]),
+    "emc_cref_filter": (_i, [_pd, _pd, _i, _pd, _pd, _i, _d, _pi, _f, _vp, _vp]),
     "emc_ctf2d_exposure": (_i, [C.POINTER(CtfParams), _i, _i, _i, _i, _i, _f, _f, _vp, _vp]),
     "emc_sf3d": (_i, [_i, _i, C.POINTER(C.c_uint), _pf, _pf, _pf, _pf, _pf, _pf, _pf, C.c_uint, _pf, _pf, _pf,
                       _vp, _vp]),

@@ -218,6 +218,46 @@ def wedge_ctf_weight(n, tilt_min=-60.0, tilt_max=60.0, ctf=None, squared=False):
 
 
 # --------------------------------------------------------------------------- particle prep
+def binary_wedge(n, tilt_min=-60.0, tilt_max=60.0, smooth=True, half=True):
+    """BH_weightMask3d 'binaryWedgeGPU' for a Y tilt axis (smoothed, Nyquist-windowed, normalised to
+    [0, 1]): the half spectrum in FFT order ((n, n, n/2+1), the search's wdgMask form) or the centred
+    n^3 volume the reference returns (half=False)."""
+    shape = (n, n, n // 2 + 1) if half else (n, n, n)
+    out = torch.empty(shape, dtype=torch.float32, device="cuda")
+    L.call("emc_binary_wedge", int(n), float(tilt_min), float(tilt_max), int(bool(smooth)), int(bool(half)),
+           _need_cuda(out, "out"), _stream())
+    return out
+
+
+def mask_sphere(shape_zyx, radius, shift=(0.0, 0.0, 0.0), kernel=0.04):
+    """EMC_maskShape('sphere', SIZE, RADIUS, 'gpu', {'shift', shift; 'kernel', kernel}): shape and the
+    returned tensor are (z, y, x); radius and shift are (x, y, z) like the reference's vectors (a
+    scalar radius is isotropic)."""
+    nz, ny, nx = shape_zyx
+    r = np.broadcast_to(np.asarray(radius, dtype=np.float64), (3,)).copy()
+    size = (C.c_int * 3)(int(nx), int(ny), int(nz))
+    ra, rp = _dptr(r)
+    sa, sp = _dptr(np.asarray(shift, dtype=np.float64).reshape(3))
+    out = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda")
+    L.call("emc_mask_sphere", size, rp, sp, float(kernel), _need_cuda(out, "out"), _stream())
+    return out
+
+
+def cref_filter(shell_freq, shell_fsc, os_freq, shape_zyx, pixel_size, force_mask=None, mtf=0.0):
+    """BH_multi_cRef's isotropic filter sqrt(2 FSC / (1 + FSC)) . MTF . forceMask as a half spectrum
+    (z, y, x/2+1) in FFT order; frequencies in 1/Angstrom."""
+    nz, ny, nx = shape_zyx
+    sf, sfp = _dptr(shell_freq)
+    fs, fsp = _dptr(shell_fsc)
+    ox, oxp = _dptr(os_freq)
+    fm, fmp = _dptr(force_mask) if force_mask is not None else (None, None)
+    size = (C.c_int * 3)(int(nx), int(ny), int(nz))
+    out = torch.empty((nz, ny, nx // 2 + 1), dtype=torch.float32, device="cuda")
+    L.call("emc_cref_filter", sfp, fsp, len(sf), oxp, fmp, len(ox), float(mtf), size, float(pixel_size),
+           _need_cuda(out, "out"), _stream())
+    return out
+
+
 def particle_spectrum(particle, weight=None, bandpass=None):
     """Q = weight .* bandpass .* fftn(particle), Q(0) = 0, and E_P = sum |Q|^2 (full spectrum)."""
     n = particle.shape[-1]

@@ -139,7 +139,8 @@ __global__ void k_sf3d_accum(const float* __restrict__ imgs, const float2* __res
 }
 
 // Binary Y-tilt-axis missing wedge of masking/BH_weightMask3d.m:103-120 on the half spectrum
-// (FFT order), without the Gaussian smoothing: theta = atan2d(kx, kz) is excluded inside the
+// (FFT order, the ifftshift of the reference's centred grid), without the Gaussian smoothing
+// (emc_binary_wedge applies it): theta = atan2d(kx, kz) is excluded inside the
 // +/-(90 - tilt) cones around kz; the |kx|,|kz| <= 2 slab through the origin is kept; times the
 // 'nyquist' radial window of BH_bandpass3d (:124-131 of BH_weightMask3d.m).  Optionally times the 3-D CTF of |k|
 // (ctf.cu:45-62 with the radius taken in 3-D).
@@ -148,10 +149,12 @@ __global__ void k_wedge_ctf(int n, float max_cone, float min_cone, int use_ctf, 
   const int nh = n / 2 + 1;
   const long total = (long)nh * n * n;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const int kx = (int)(i % nh);
+    // signed frequencies of the ifftshifted centred grid: for even n the Nyquist index is -n/2
+    const int kx0 = (int)(i % nh);
     const int ky0 = (int)((i / nh) % n), kz0 = (int)(i / ((long)nh * n));
-    const int ky = ky0 <= n / 2 ? ky0 : ky0 - n;
-    const int kz = kz0 <= n / 2 ? kz0 : kz0 - n;
+    const int kx = 2 * kx0 < n ? kx0 : kx0 - n;
+    const int ky = 2 * ky0 < n ? ky0 : ky0 - n;
+    const int kz = 2 * kz0 < n ? kz0 : kz0 - n;
     const float theta = atan2f((float)kx, (float)kz) * (180.0f / 3.14159265358979323f);
     const bool excluded = (180.0f - min_cone <= theta || theta <= max_cone - 180.0f) ||
                           (-min_cone <= theta && theta <= max_cone);

@@ -47,26 +47,34 @@ def blob_reference(rng, n=64, n_blobs=40, radius=None, sigma=(2.0, 4.0)):
     return vol.astype(np.float32)
 
 
-def soft_sphere_mask(n, radius, kernel=None):
-    """Soft spherical mask after EMC_maskShape('sphere') (masking/EMC_maskShape.m:124-143,218-224):
-    binary ball of radius + ceil(k/2), blurred by a normalised Gaussian of size k
-    (k = max(9, 4% of the box), sigma = k/5), rescaled to max 1, values <= 0.001 set to 0."""
-    k = kernel if kernel is not None else max(9, int(round(0.04 * n)))
-    r = radius + math.ceil(k / 2)
-    c = n // 2
-    ax = np.arange(n) - c
-    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
-    ball = ((x * x + y * y + z * z) <= r * r).astype(np.float64)
-    sigma = k / 5.0
-    t = np.arange(k) - (k - 1) / 2.0
-    g = np.exp(-t * t / (2 * sigma * sigma))
+def soft_sphere_mask(n, radius, kernel=0.04):
+    """Soft spherical mask of EMC_maskShape('sphere', [n n n], radius, ..) (masking/EMC_maskShape.m:
+    95-224), the input generator's host copy of emc_mask_sphere: a ball of radius + ceil(k/2) about
+    floor(n/2) (single-precision test), the outer ceil(k/2) voxels of every face zeroed, a separable
+    Gaussian of k = max(9, round((0.04 n - 1)/2)*2+1) taps and sigma = sqrt(-(ceil(k/2)/2)^2/(2 ln 0.5)),
+    rescaled to max 1, values <= 0.001 set to 0."""
+    v = (n * kernel - 1) / 2
+    k = max(9, int(math.floor(abs(v) + 0.5) * (1 if v >= 0 else -1)) * 2 + 1)
+    m = math.ceil(k / 2)
+    r = np.float32(radius + m)
+    ax = (np.arange(n) - n // 2).astype(np.float32) / r
+    q = (ax[None, None, :] * ax[None, None, :] + ax[None, :, None] * ax[None, :, None]) + ax[:, None, None] * ax[:, None, None]
+    ball = (q <= np.float32(1)).astype(np.float64)
+    ball[:m] = 0
+    ball[n - m:] = 0
+    ball[:, :m] = 0
+    ball[:, n - m:] = 0
+    ball[:, :, :m] = 0
+    ball[:, :, n - m:] = 0
+    sigma = math.sqrt(-(m / 2) ** 2 / (2 * math.log(0.5)))
+    g = np.exp(-0.5 * ((np.arange(k) - (k - 1) / 2) / sigma) ** 2)
     g /= g.sum()
-    m = ball
+    out = ball
     for axis in range(3):
-        m = np.apply_along_axis(lambda v: np.convolve(v, g, mode="same"), axis, m)
-    m /= m.max()
-    m[m <= 0.001] = 0.0
-    return m.astype(np.float32)
+        out = np.apply_along_axis(lambda v_: np.convolve(v_, g, mode="same"), axis, out)
+    out /= out.max()
+    out[out <= 0.001] = 0.0
+    return out.astype(np.float32)
 
 
 def random_euler(rng, theta_max=180.0):

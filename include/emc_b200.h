@@ -158,6 +158,35 @@ EMC_API emc_status emc_sf3d(int half, int squared, const unsigned size[3], const
 EMC_API emc_status emc_wedge_ctf_weight(int n, float tilt_min_deg, float tilt_max_deg, const emc_ctf_params* ctf,
                                         int squared, float* d_out, void* stream);
 
+/* BH_weightMask3d(SIZE, tilts, 'binaryWedgeGPU', ..) (masking/BH_weightMask3d.m:99-143) for a Y tilt
+ * axis: the binary wedge on the centred n^3 grid (theta = atan2d(X, Z); the cones of
+ * +/-(90 - |tilt|) removed; the |X|, |Z| <= 2 slab kept), smoothed (smooth != 0) by convn with
+ * BH_multi_gaussian3d(9, 1.5) ('same', zero outside), times the 'nyquist' window of BH_bandpass3d,
+ * then (W - min) / max(W - min).  layout 0: the centred n^3 volume the reference returns; layout 1:
+ * its ifftshifted half spectrum ((n/2+1)*n*n, FFT order), the form the search takes as wdgMask.
+ * Scratch (two n^3 volumes) comes from the stream-ordered allocator. */
+EMC_API emc_status emc_binary_wedge(int n, float tilt_min_deg, float tilt_max_deg, int smooth, int layout,
+                                    float* d_out, void* stream);
+/* EMC_maskShape('sphere', SIZE, RADIUS, 'gpu', {'shift', shift; 'kernel', kernel_frac})
+ * (masking/EMC_maskShape.m:95-224): the ellipsoid of radius RADIUS + ceil(k/2) centred at
+ * floor(SIZE/2) + shift (single-precision test, as MATLAB), the outer ceil(k/2) voxels of every
+ * face zeroed, blurred by the separable Gaussian of k = max(9, round((min(SIZE) kernel_frac - 1)/2)*2+1)
+ * taps and sigma = sqrt(-(ceil(k/2)/2)^2 / (2 ln 0.5)), divided by its maximum, values <= 0.001 set
+ * to 0.  kernel_frac = 0.04 is the reference's default; 0 gives the binary ellipsoid.  size[2] == 1
+ * makes a 2-D mask.  shift may be NULL.  d_out: size[0]*size[1]*size[2] floats, x fastest. */
+EMC_API emc_status emc_mask_sphere(const int size[3], const double radius[3], const double shift[3],
+                                   double kernel_frac, float* d_out, void* stream);
+/* BH_multi_cRef(fscINFO, radialGrid, bFactor, flgAlignRef) (statistics/BH_multi_cRef.m:1-166; the
+ * isotropic filter, cones being off there): F = the not-a-knot cubic spline through (shell_freq,
+ * max(shell_fsc, 0)); cRef = the not-a-knot spline through (os_freq, sqrt(|2F/(1+F)|) .* MTF .*
+ * force_mask) with the ad hoc MTF of fscINFO{3}{3} (0: none; 1, 2 and other values as the
+ * reference); the filter is cRef(|k| / pixel_size) on the half spectrum (FFT order) of a
+ * size[0] x size[1] x size[2] volume, the particle bandpass of BH_alignRaw3d_v2.m:524-531.
+ * Frequencies in 1/Angstrom; force_mask may be NULL (= 1).  Synchronises the stream. */
+EMC_API emc_status emc_cref_filter(const double* shell_freq, const double* shell_fsc, int n_shells,
+                                   const double* os_freq, const double* force_mask, int n_os, double mtf,
+                                   const int size[3], float pixel_size, float* d_out, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Volume and spectrum operators around the search                          */
 /* ------------------------------------------------------------------------ */

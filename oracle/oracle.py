@@ -386,6 +386,106 @@ def even_weight_np(rng, n, lo=0.2, hi=1.5):
     return 0.5 * (a + flip)
 
 
+def _conv_same_np(v, taps):
+    """convn(v, taps along each axis, 'same') with zero padding (a symmetric, odd-length kernel)."""
+    out = np.asarray(v, dtype=np.float64)
+    for axis in range(out.ndim):
+        if out.shape[axis] > 1:
+            out = np.apply_along_axis(lambda r: np.convolve(r, taps, mode="same"), axis, out)
+    return out
+
+
+def binary_wedge_np(n, tilt_min, tilt_max, smooth=True, half=True):
+    """BH_weightMask3d(.., 'binaryWedgeGPU') (masking/BH_weightMask3d.m:99-143), Y tilt axis, FP64:
+    theta = atan2d(X, Z) on the centred grid, cones of +/-(90 - |tilt|) removed, |X|, |Z| <= 2 kept,
+    convn with BH_multi_gaussian3d(9, 1.5), times fftshift(BH_bandpass3d(.., 'nyquist')), then
+    (W - min) / max(W - min).  half: the ifftshifted half spectrum (z, y, x <= n/2)."""
+    c = n // 2
+    ax = np.arange(n) - c
+    Z, Y, X = np.meshgrid(ax, ax, ax, indexing="ij")
+    max_cone, min_cone = 90.0 - abs(tilt_min), 90.0 - abs(tilt_max)
+    th = np.degrees(np.arctan2(X, Z))
+    excl = ((180 - min_cone <= th) | (th <= max_cone - 180)) | ((-min_cone <= th) & (th <= max_cone))
+    w = np.where(excl, 0.0, 1.0)
+    w[(np.abs(X) <= 2) & (np.abs(Z) <= 2)] = 1.0
+    if smooth:
+        t = np.exp(-0.5 * ((np.arange(9) - 4) / 1.5) ** 2)
+        w = _conv_same_np(w, t / t.sum())
+    rn = np.sqrt(X ** 2 + Y ** 2 + Z ** 2) / n
+    w = w * np.where(rn < 0.485, 1.0, np.exp(-(rn - 0.485) ** 2 / (2 * (1.5 / n) ** 2)))
+    w = w - w.min()
+    w = w / w.max()
+    return np.fft.ifftshift(w)[:, :, : n // 2 + 1] if half else w
+
+
+def mask_sphere_np(shape_zyx, radius_xyz, shift_xyz=(0.0, 0.0, 0.0), kernel=0.04):
+    """EMC_maskShape('sphere', SIZE, RADIUS, .., {'shift', shift; 'kernel', kernel})
+    (masking/EMC_maskShape.m:95-224): coordinates i - floor(n/2) - shift (EMC_coordVectors, origin 1),
+    the ellipsoid test in single precision, the outer ceil(k/2) voxels of every face zeroed
+    (EMC_resize 'force_taper' with a zero taper), EMC_convn with the separable EMC_gaussianKernel
+    ([1, k], sigma), / max, <= 0.001 -> 0."""
+    nz, ny, nx = shape_zyx
+    r = np.broadcast_to(np.asarray(radius_xyz, np.float64), (3,)).copy()
+    sh = np.asarray(shift_xyz, np.float64)
+    k = 0
+    if kernel > 0:
+        mn = min(nx, ny, nz) if nz > 1 else min(nx, ny)
+        v = (mn * kernel - 1) / 2
+        k = int(np.floor(abs(v) + 0.5) * np.sign(v)) * 2 + 1  # MATLAB round: half away from zero
+        k = max(k, 9)
+        r = r + math.ceil(k / 2)
+    f32 = np.float32
+    vx = ((np.arange(nx) - nx // 2).astype(f32) - f32(sh[0])) / f32(r[0])
+    vy = ((np.arange(ny) - ny // 2).astype(f32) - f32(sh[1])) / f32(r[1])
+    if nz > 1:
+        vz = ((np.arange(nz) - nz // 2).astype(f32) - f32(sh[2])) / f32(r[2])
+    else:
+        vz = np.zeros(1, f32)
+    q = (vx[None, None, :] * vx[None, None, :] + vy[None, :, None] * vy[None, :, None]) + vz[:, None, None] * vz[:, None, None]
+    m = (q <= f32(1)).astype(np.float64)
+    if not k:
+        return m
+    t = math.ceil(k / 2)
+    m[:, :, :t] = 0
+    m[:, :, nx - t:] = 0
+    m[:, :t, :] = 0
+    m[:, ny - t:, :] = 0
+    if nz > 1:
+        m[:t] = 0
+        m[nz - t:] = 0
+    sigma = math.sqrt(-(math.ceil(k / 2) / 2) ** 2 / (2 * math.log(0.5)))
+    g = np.exp(-0.5 * ((np.arange(k) - (k - 1) / 2) / sigma) ** 2)
+    m = _conv_same_np(m, g / g.sum())
+    m = m / m.max()
+    m[m <= 0.001] = 0
+    return m
+
+
+def cref_filter_np(shell_freq, shell_fsc, os_freq, shape_zyx, pixel_size, force_mask=None, mtf=0.0):
+    """BH_multi_cRef (statistics/BH_multi_cRef.m:55-145, the isotropic filter) with scipy's not-a-knot
+    CubicSpline for MATLAB's fit(.., 'cubicSpline'): cRef(|k| / pixel) on the half spectrum (FFT order),
+    the radius formed in single precision as the reference's single radialGrid."""
+    from scipy.interpolate import CubicSpline
+    fsc = CubicSpline(np.asarray(shell_freq, float), np.maximum(np.asarray(shell_fsc, float), 0.0), bc_type="not-a-knot")
+    ox = np.asarray(os_freq, float)
+    if mtf == 0:
+        m = np.ones_like(ox)
+    else:
+        det, cap = {1.0: (-100.0, 0.05), 2.0: (-25.0, 0.06)}.get(float(mtf), (-np.round(mtf), mtf - np.round(mtf)))
+        m = 1.0 / ((np.exp(det * ox ** 1.25) + cap) / cap)
+    F = fsc(ox)
+    vals = np.sqrt(np.abs(2 * F / (1 + F))) * m * (1.0 if force_mask is None else np.asarray(force_mask, float))
+    cref = CubicSpline(ox, vals, bc_type="not-a-knot")
+    nz, ny, nx = shape_zyx
+    f32 = np.float32
+    kx = np.arange(nx // 2 + 1).astype(f32) / f32(nx)
+    ky = (np.fft.fftfreq(ny) * ny).astype(f32) / f32(ny)
+    kz = (np.fft.fftfreq(nz) * nz).astype(f32) / f32(nz)
+    r2 = (kx[None, None, :] * kx[None, None, :] + ky[None, :, None] * ky[None, :, None]) + kz[:, None, None] * kz[:, None, None]
+    rad = np.sqrt(r2.astype(f32)) / f32(pixel_size)
+    return cref(rad.astype(np.float64))
+
+
 def symmetry_matrices_np(symmetry):
     """interpolator.check_symmetry operators as applied by interp3d (testScripts/interpolator.m:172-214):
     C<n> / D<n>: defineMatrix([0, 0, k 360/n], 'Bah', 'forward') for k < n (for D<n> nSymMats = n, so the

@@ -235,11 +235,12 @@ def test_autograd_function_shim(setup):
                                 interp="cubic")
     x = torch.tensor(_poses50(seed=52)[:k], dtype=torch.float64, requires_grad=True)
     cc = refine.CCPose.apply(x, obj)
+    # a second launch: the FP64 reductions' atomic order may differ in the last bits
     cc_ref, g_ref = obj.cc_grad(x.detach().numpy())
-    assert np.array_equal(cc.detach().numpy(), cc_ref)
+    assert np.allclose(cc.detach().numpy(), cc_ref, rtol=1e-12, atol=0)
     w = torch.tensor([1.0, -2.0, 0.5, 3.0], dtype=torch.float64)
     (w * cc).sum().backward()
-    assert np.allclose(x.grad.numpy(), w.numpy()[:, None] * g_ref, rtol=1e-12, atol=0)
+    assert np.allclose(x.grad.numpy(), w.numpy()[:, None] * g_ref, rtol=1e-9, atol=1e-12 * np.abs(g_ref).max())
     atol = 2e-2 * float(np.abs(g_ref).max())
     assert torch.autograd.gradcheck(lambda t: refine.CCPose.apply(t, obj), (x.detach().requires_grad_(),),
                                     eps=1e-2, atol=atol, rtol=2e-2, raise_exception=True)

@@ -52,11 +52,14 @@ def test_sf3d(built_lib, cuda):
 def test_wedge_ctf_weight(built_lib, cuda):
     from emclarity_b200 import api
     n = 64
-    w = api.wedge_ctf_weight(n, -60, 60, None).cpu().numpy()
+    # an asymmetric range (-55, 62): the cones are 35 and 28 degrees; the half spectrum is the
+    # ifftshifted centred grid, so the Nyquist index of every axis is the frequency -n/2
+    w = api.wedge_ctf_weight(n, -55, 62, None).cpu().numpy()
     k = np.fft.fftfreq(n) * n
-    kz, ky, kx = np.meshgrid(k, k, np.arange(n // 2 + 1), indexing="ij")
+    kxs = np.where(np.arange(n // 2 + 1) == n // 2, -n // 2, np.arange(n // 2 + 1))
+    kz, ky, kx = np.meshgrid(k, k, kxs, indexing="ij")
     th = np.degrees(np.arctan2(kx, kz))
-    excl = (150 <= th) | (th <= -150) | ((-30 <= th) & (th <= 30))
+    excl = (180 - 28 <= th) | (th <= 35 - 180) | ((-28 <= th) & (th <= 35))
     ref = np.where(excl, 0.0, 1.0)
     ref[(np.abs(kx) <= 2) & (np.abs(kz) <= 2)] = 1.0
     # BH_bandpass3d 'nyquist' window: 1 below 0.485 cycles/px, Gaussian roll-off of width 1.5/n
@@ -64,7 +67,7 @@ def test_wedge_ctf_weight(built_lib, cuda):
     ref = ref * np.where(rn < 0.485, 1.0, np.exp(-(rn - 0.485) ** 2 / (2 * (1.5 / n) ** 2)))
     assert np.abs(w - ref).max() < 5e-6
     ctf = dict(pixel_size=2.5, wavelength=0.019687, cs_mm=2.7, defocus=25000.0, amp_contrast=0.07)
-    wc = api.wedge_ctf_weight(n, -60, 60, ctf).cpu().numpy()
+    wc = api.wedge_ctf_weight(n, -55, 62, ctf).cpu().numpy()
     s2 = (kx ** 2 + ky ** 2 + kz ** 2) / (n * 2.5) ** 2
     amp = np.arctan(0.07 / np.sqrt(1 - 0.07 ** 2))
     c = np.sin(np.pi * 0.5 * 2.7e7 * 0.019687 ** 3 * s2 * s2 - np.pi * 0.019687 * s2 * 25000.0 - amp)

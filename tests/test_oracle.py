@@ -267,3 +267,22 @@ def test_pocketfft_arm_matches_oracle():
         cc2, pk2 = pool.search(mats)
     assert np.allclose(cc2, cc, rtol=1e-4, atol=1e-6)
     assert np.array_equal(pk2, pk)
+
+
+def test_synthetic_mask_matches_the_emc_maskshape_restatement():
+    """The input generator's soft sphere is EMC_maskShape('sphere') (kernel 4 %, single-precision test)."""
+    from emclarity_b200 import synthetic
+    for n, r in ((64, 28.0), (32, 10.5)):
+        assert np.abs(synthetic.soft_sphere_mask(n, r) - O.mask_sphere_np((n, n, n), r)).max() < 1e-6
+
+
+def test_unsmoothed_wedge_restatement_is_the_binary_wedge():
+    """Without smoothing, BH_weightMask3d's wedge is the binary cone test times the Nyquist window (its
+    min / max normalisation is the identity); the half layout is the ifftshifted centred grid."""
+    n = 24
+    w = O.binary_wedge_np(n, -50.0, 65.0, smooth=False, half=False)
+    assert w.min() == 0.0 and abs(w.max() - 1.0) < 1e-15
+    h = O.binary_wedge_np(n, -50.0, 65.0, smooth=False, half=True)
+    assert np.array_equal(h, np.fft.ifftshift(w)[:, :, : n // 2 + 1])
+    c = n // 2
+    assert w[c, c, c] == 1.0  # the origin slab is kept
