@@ -190,6 +190,8 @@ def run_ours(args, world, rank, local):
     s = api.Search(peak_radius=PEAK_RADIUS)
     if args.planes:
         s.set_planes(BOX, args.planes)
+    if args.overlap:
+        s.set_overlap(args.overlap)
     rid = s.add_reference(b["ref"], b["mask"])
     s.set_orientations(b["grid"])
     d_parts = b["parts"].cuda()
@@ -319,6 +321,7 @@ def run_ours(args, world, rank, local):
                                (n, N_ORIENT, PEAK_RADIUS),
                    "box": BOX, "particles_per_gpu": n, "orientations": N_ORIENT, "evals_per_step_per_gpu": evals,
                    "l2": "inputs larger than L2 (%.2f GB of particle spectra per GPU)" % (spec.numel() * 8 / 1e9),
+                   "chunk_overlap_slots": args.overlap or 2,
                    "parallelism": "replicas%d" % world},
         "e2e": {"value": world * evals / (e2e_ms / 1e3), "unit": "CC evals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -577,12 +580,14 @@ def mixed_batch(n_part, seed=2024):
     return sizes, refs, parts
 
 
-def time_mixed(parts, refs, store, steps, warmup, grid):
+def time_mixed(parts, refs, store, steps, warmup, grid, overlap=0):
     """One emc_search_run over every particle of the batch with the reference stored as `store`."""
     import torch
 
     from emclarity_b200 import api
     s = api.Search(peak_radius=PEAK_RADIUS)
+    if overlap:
+        s.set_overlap(overlap)
     rids = {n: s.add_reference(refs[n][2], refs[n][3], store=store) for n in (64, 96, 128)}
     s.set_orientations(grid)
     descs = [s.particle(p["spec"], p["energy"], rids[p["n"]], prior=p["prior"], orient_count=len(grid),
@@ -603,8 +608,8 @@ def time_mixed(parts, refs, store, steps, warmup, grid):
     return ms, launches, best.cpu().numpy()
 
 
-def mixed_entry(sizes, parts, refs, store, steps, warmup, grid):
-    ms, launches, _ = time_mixed(parts, refs, store, steps, warmup, grid)
+def mixed_entry(sizes, parts, refs, store, steps, warmup, grid, overlap=0):
+    ms, launches, _ = time_mixed(parts, refs, store, steps, warmup, grid, overlap)
     evals = len(parts) * len(grid)
     counts = {n: int(np.sum(sizes == n)) for n in (64, 96, 128)}
     byts = sum(compulsory_bytes(n, c * len(grid), c, 1, store) for n, c in counts.items())
@@ -683,7 +688,7 @@ def run_mixed(args, store="f32"):
     n_part = args.particles if args.particles != 1200 else 2000
     grid = synthetic.local_grid(N_ORIENT, 8.0, 2.0)
     sizes, refs, parts = mixed_batch(n_part)
-    res = mixed_entry(sizes, parts, refs, store, args.steps, args.warmup, grid)
+    res = mixed_entry(sizes, parts, refs, store, args.steps, args.warmup, grid, args.overlap)
     res.update({"n_gpus": 1, "higher_is_better": True, "data": "synthetic"})
     if store == "bf16":
         res["vs_fp64_oracle"] = bf16_report(sizes, refs, parts, grid)
@@ -908,14 +913,16 @@ def run_formats(args):
     t[:, 10] = np.linspace(0, 120, nt)
     t[:, 11], t[:, 12], t[:, 13] = 4.1e-8, -1.05, 1.0
     t[:, 14], t[:, 15], t[:, 16], t[:, 17], t[:, 18] = -3e-6, 2.17e-10, 2.7e-3, 1.968697e-12, 0.085
-    xyz = np.stack([rng.uniform(1, 512, 64), rng.uniform(1, 512, 64), rng.uniform(1, 256, 64)], axis=1)
+    n_sf = 2000
+    xyz = np.stack([rng.uniform(1, 512, n_sf), rng.uniform(1, 512, n_sf), rng.uniform(1, 256, n_sf)], axis=1)
     rg = np.array([[512, 512, 256], [0.0, 0.0, 0.0]])
     api.sf3d_particles((64, 64, 64), 1.0, t, xyz[:2], rg)
     torch.cuda.synchronize()
     t0 = time.time()
-    api.sf3d_particles((64, 64, 64), 1.0, t, xyz, rg)
+    sf = api.sf3d_particles((64, 64, 64), 1.0, t, xyz, rg)
     torch.cuda.synchronize()
     sf_s = time.time() - t0
+    del sf
     t0 = time.time()
     O.sf3d_particles_np((64, 64, 64), 1.0, t, xyz[:2], rg)
     sf_cpu = 2 / (time.time() - t0)
@@ -926,13 +933,14 @@ def run_formats(args):
     return {"metric": "windows/s extracted (64^3 from a 512x512x256 tomogram in HBM)", "value": k / (ext_ms / 1e3),
             "unit": "windows/s", "n_gpus": 1, "steps": reps, "ms_per_step": ext_ms, "higher_is_better": True,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "MRC read 512x512x256 float32 to HBM, 2,000 64^3 windows, 64 SF3D weights"},
+            "config": {"workload": "MRC read 512x512x256 float32 to HBM, 2,000 64^3 windows, 2,000 SF3D weights"},
             "roofline": {"bound": "hbm", "achieved": ext_bytes / (ext_ms / 1e3) / 1e9, "peak": pk, "unit": "GB/s",
                          "frac": ext_bytes / (ext_ms / 1e3) / 1e9 / pk, "peak_source": which},
             "mrc_read_device": {"gb_per_s": tomo_h.nbytes / read_s / 1e9, "ms": read_s * 1e3,
                                 "cpu_numpy_gb_per_s": tomo_h.nbytes / read_cpu_s / 1e9,
                                 "note": "file in the page cache; bound by the host read + PCIe"},
-            "sf3d_particles": {"value": 64 / sf_s, "unit": "particles/s", "cpu_restatement": sf_cpu},
+            "sf3d_particles": {"value": n_sf / sf_s, "unit": "particles/s", "particles": n_sf, "tilts": nt,
+                               "cpu_restatement": sf_cpu},
             "cpu_baseline": {"value": ext_cpu, "unit": "windows/s", "cores": 1, "kind": "port",
                              "sample": "20 windows through the numpy restatement"}}
 
@@ -1128,8 +1136,8 @@ def run_extras(args):
     from emclarity_b200 import synthetic
     grid = synthetic.local_grid(N_ORIENT, 8.0, 2.0)
     sizes, refs, parts = mixed_batch(2000)
-    out = {"mixed": mixed_entry(sizes, parts, refs, "f32", 2, 1, grid),
-           "mixed_bf16": mixed_entry(sizes, parts, refs, "bf16", 2, 1, grid)}
+    out = {"mixed": mixed_entry(sizes, parts, refs, "f32", 2, 1, grid, args.overlap),
+           "mixed_bf16": mixed_entry(sizes, parts, refs, "bf16", 2, 1, grid, args.overlap)}
     del parts, refs
     torch.cuda.empty_cache()
     out["refine"] = run_refine(args, n_part=200)
@@ -1147,6 +1155,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-uneven (FP32, BF16) and refinement keys of the default line")
     ap.add_argument("--planes", type=int, default=0, help="pass-A z-planes per CTA (0: timed choice)")
+    ap.add_argument("--overlap", type=int, default=0, help="chunk scratch slots (0: the library default, 2)")
     ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine", "average", "formats",
                                                                     "tsearch_post"])
     args = ap.parse_args()

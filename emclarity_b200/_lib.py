@@ -77,6 +77,7 @@ SIGNATURES = {
     "emc_fft_destroy": (_i, [_vp]),
     "emc_ctf2d": (_i, [C.POINTER(CtfParams), _i, _i, _i, _i, _i, _vp, _vp]),
     "emc_binary_wedge": (_i, [_i, _f, _f, _i, _i, _vp, _vp]),
+    "emc_centred_to_half": (_i, [_vp, _i, _i, _i, _i, _vp, _vp]),
     "emc_mask_sphere": (_i, [_pi, _pd, _pd, _d, _vp, _vp]),
     "emc_cref_filter": (_i, [_pd, _pd, _i, _pd, _pd, _i, _d, _pi, _f, _vp, _vp]),
     "emc_ctf2d_exposure": (_i, [C.POINTER(CtfParams), _i, _i, _i, _i, _i, _f, _f, _vp, _vp]),
@@ -103,6 +104,7 @@ SIGNATURES = {
     "emc_search_timings": (_i, [_vp, _pd, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_long), _i]),
     "emc_search_set_planes": (_i, [_vp, _i, _i]),
     "emc_search_get_planes": (_i, [_vp, _i, _i, _pi, _pf]),
+    "emc_search_set_overlap": (_i, [_vp, _i]),
     "emc_search_plain_noalloc": (_i, [_vp, _vp, _i, _vp, _d, _pd, _pf, _pd, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "emc_cc_adjoint_batch": (_i, [_vp, _i, _pi, C.POINTER(_vp), _pd, _pd, _pd, _i, _pd, _pd, _vp]),
     "emc_cc_adjoint": (_i, [_vp, _i, _vp, _d, _pd, _pd, _i, _pd, _pd, _vp]),

@@ -229,6 +229,16 @@ def binary_wedge(n, tilt_min=-60.0, tilt_max=60.0, smooth=True, half=True):
     return out
 
 
+def centred_to_half(vol):
+    """ifftshift of centred weight volumes ((count,) nz, ny, nx) cropped to half spectra ((count,) nz, ny,
+    nx/2+1) in FFT order: the reference's centred SF3D / wedge volumes in the form the search's wedge takes."""
+    v = vol if vol.dim() == 4 else vol.unsqueeze(0)
+    count, nz, ny, nx = v.shape
+    out = torch.empty((count, nz, ny, nx // 2 + 1), dtype=torch.float32, device="cuda")
+    L.call("emc_centred_to_half", _need_cuda(v, "vol"), nx, ny, nz, count, _need_cuda(out, "out"), _stream())
+    return out if vol.dim() == 4 else out[0]
+
+
 def mask_sphere(shape_zyx, radius, shift=(0.0, 0.0, 0.0), kernel=0.04):
     """EMC_maskShape('sphere', SIZE, RADIUS, 'gpu', {'shift', shift; 'kernel', kernel}): shape and the
     returned tensor are (z, y, x); radius and shift are (x, y, z) like the reference's vectors (a
@@ -398,6 +408,10 @@ class Search:
     def set_planes(self, box, planes):
         """Fixes pass A's z-planes per CTA for `box` (1, 2, 4 or 8); 0 returns it to timing-based tuning."""
         L.call("emc_search_set_planes", self._h, int(box), int(planes))
+
+    def set_overlap(self, slots):
+        """Chunk scratch slots of recorded runs: 2 (default) runs consecutive chunks concurrently, 1 in order."""
+        L.call("emc_search_set_overlap", self._h, int(slots))
 
     def planes(self, box, dtype="f32"):
         """(planes in use, {planes option: pass-A ms per launch at tuning}) for (box, dtype); 0 = not tuned yet."""

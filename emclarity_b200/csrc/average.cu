@@ -505,36 +505,46 @@ emc_status emc_average_add(emc_average_t a, const float* d_particles, int count,
       pr.pad = 0;
       widx[i] = pr.wedge;
     }
-    emc::k_avg_stage_in<<<64, 256, 0, st>>>(d_mats_h, d_parts_h, d_widx_h, nb, a->nsym, a->mats, a->parts,
-                                             a->widx);
-    EMC_LAUNCH_CHECK();
-    EMC_CUDA(cudaMemsetAsync(a->stats, 0, sizeof(emc::AvgStats) * nb, st));
-    const int bricks = ((a->n + emc::kBrick - 1) / emc::kBrick) * ((a->n + emc::kBrick - 1) / emc::kBrick) *
-                       ((a->n + emc::kBrick - 1) / emc::kBrick);
-    emc::k_avg_rotate<<<dim3(bricks, nb), 256, 0, st>>>(d_particles + (size_t)b0 * a->nv, a->nv, nullptr, a->n,
-                                                              a->mats, a->parts, 1, a->mask, a->bin_thr, a->rot,
-                                                              a->stats);
-    EMC_LAUNCH_CHECK();
-    if (a->nw) {
-      const int wb = ((a->nw + emc::kBrick - 1) / emc::kBrick) * ((a->nw + emc::kBrick - 1) / emc::kBrick) *
-                     ((a->nw + emc::kBrick - 1) / emc::kBrick);
-      emc::k_avg_rotate<<<dim3(wb, nb), 256, 0, st>>>(d_wedges, a->nvw, a->widx, a->nw, a->mats, a->parts, 0,
-                                                            nullptr, 0.f, a->wrot, nullptr);
+    // the batch's launches; on a failure the stream is drained before returning, since kernels
+    // already queued may still read the mapped staging that the next call overwrites
+    auto launch_batch = [&]() -> emc_status {
+      emc::k_avg_stage_in<<<64, 256, 0, st>>>(d_mats_h, d_parts_h, d_widx_h, nb, a->nsym, a->mats, a->parts,
+                                               a->widx);
       EMC_LAUNCH_CHECK();
-    }
-    emc::k_avg_coef<<<(nb + 127) / 128, 128, 0, st>>>(a->stats, a->parts, nb, a->n_bin, a->mask_sum, (double)a->nv,
-                                                     a->coef, a->counts, a->kept);
-    EMC_LAUNCH_CHECK();
-    const size_t smem = sizeof(float4) * nb;
-    if (smem > 48 * 1024) EMC_CUDA(cudaFuncSetAttribute(emc::k_avg_accumulate,
-                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    emc::k_avg_accumulate<<<grid_for(a->nv), 256, smem, st>>>(a->rot, a->nv, nb, a->coef, a->parts, a->mask, 1,
-                                                              a->sum[0], a->sum[1]);
-    EMC_LAUNCH_CHECK();
-    if (a->nw) {
-      emc::k_avg_accumulate<<<grid_for(a->nvw), 256, smem, st>>>(a->wrot, a->nvw, nb, a->coef, a->parts, nullptr, 0,
-                                                                 a->wsum[0], a->wsum[1]);
+      EMC_CUDA(cudaMemsetAsync(a->stats, 0, sizeof(emc::AvgStats) * nb, st));
+      const int bricks = ((a->n + emc::kBrick - 1) / emc::kBrick) * ((a->n + emc::kBrick - 1) / emc::kBrick) *
+                         ((a->n + emc::kBrick - 1) / emc::kBrick);
+      emc::k_avg_rotate<<<dim3(bricks, nb), 256, 0, st>>>(d_particles + (size_t)b0 * a->nv, a->nv, nullptr, a->n,
+                                                                a->mats, a->parts, 1, a->mask, a->bin_thr, a->rot,
+                                                                a->stats);
       EMC_LAUNCH_CHECK();
+      if (a->nw) {
+        const int wb = ((a->nw + emc::kBrick - 1) / emc::kBrick) * ((a->nw + emc::kBrick - 1) / emc::kBrick) *
+                       ((a->nw + emc::kBrick - 1) / emc::kBrick);
+        emc::k_avg_rotate<<<dim3(wb, nb), 256, 0, st>>>(d_wedges, a->nvw, a->widx, a->nw, a->mats, a->parts, 0,
+                                                              nullptr, 0.f, a->wrot, nullptr);
+        EMC_LAUNCH_CHECK();
+      }
+      emc::k_avg_coef<<<(nb + 127) / 128, 128, 0, st>>>(a->stats, a->parts, nb, a->n_bin, a->mask_sum, (double)a->nv,
+                                                       a->coef, a->counts, a->kept);
+      EMC_LAUNCH_CHECK();
+      const size_t smem = sizeof(float4) * nb;
+      if (smem > 48 * 1024) EMC_CUDA(cudaFuncSetAttribute(emc::k_avg_accumulate,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      emc::k_avg_accumulate<<<grid_for(a->nv), 256, smem, st>>>(a->rot, a->nv, nb, a->coef, a->parts, a->mask, 1,
+                                                                a->sum[0], a->sum[1]);
+      EMC_LAUNCH_CHECK();
+      if (a->nw) {
+        emc::k_avg_accumulate<<<grid_for(a->nvw), 256, smem, st>>>(a->wrot, a->nvw, nb, a->coef, a->parts, nullptr, 0,
+                                                                   a->wsum[0], a->wsum[1]);
+        EMC_LAUNCH_CHECK();
+      }
+      return EMC_OK;
+    };
+    const emc_status rs = launch_batch();
+    if (rs != EMC_OK) {
+      cudaStreamSynchronize(st);
+      return rs;
     }
     if (kept) {
       EMC_CUDA(cudaMemcpyAsync(kept_h.data(), a->kept, sizeof(int) * nb, cudaMemcpyDeviceToHost, st));

@@ -78,32 +78,37 @@ __global__ void k_ctf2d(const CtfDev c, const CtfGrid g, int use_exposure, float
   out[(long)y * g.dx + x] = v;
 }
 
-// All tilt images of the SF3D weight (full grid, centred, squared, exposure-filtered).
+// All tilt images of the SF3D weight (full grid, centred, squared, exposure-filtered) of a batch of
+// volumes: image blockIdx.z = p * ntilts + t uses the CTF c[blockIdx.z] (volume p, tilt t) and tilt
+// t's grid, occupancy and exposure.
 __global__ void k_sf3d_ctfs(const CtfDev* __restrict__ c, const CtfGrid* __restrict__ g, const float* __restrict__ occ,
-                            const float* __restrict__ expo, int nx, int ny, float* __restrict__ imgs) {
+                            const float* __restrict__ expo, int nx, int ny, int ntilts, float* __restrict__ imgs) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int t = blockIdx.z;
+  const int t = blockIdx.z % ntilts;
   if (x >= nx || y >= ny) return;
   int xs;
   const CtfGrid gg = g[t];
-  float v = ctf_eval(c[t], gg, x, y, &xs);
+  float v = ctf_eval(c[blockIdx.z], gg, x, y, &xs);
   const float rw = occ[t] * (xs == 0 ? 0.2f : fabsf((float)xs));
   const int ys = y - gg.oy;
   const float fx = (float)xs * gg.fvx, fy = (float)ys * gg.fvy;
   const float r2 = fx * fx + fy * fy;
   v *= rw * expf((-0.5f * expo[t]) / (0.24499f * powf(r2, -0.8325f) + 2.81410f));
-  imgs[((long)t * ny + y) * nx + x] = v;
+  imgs[((long)blockIdx.z * ny + y) * nx + x] = v;
 }
 
 // sf3dKernel (mexSF3D.cu:24-78) summed over tilts: for every (x, y) column and tilt, the voxels
 // within 4 px of the tilted central plane receive the bilinearly sampled CTF^2 image (zero
-// border) times the cosine edge weight.
+// border) times the cosine edge weight.  Volume blockIdx.z of a batch: its images follow those of
+// the previous volumes, its output volume too.
 __global__ void k_sf3d_accum(const float* __restrict__ imgs, const float2* __restrict__ sincos, int ntilts, int nx,
                              int ny, int nz, float* __restrict__ out) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= nx || y >= ny) return;
+  imgs += (long)blockIdx.z * ntilts * nx * ny;
+  out += (long)blockIdx.z * nx * ny * nz;
   const float PI = 3.14159265358979323f;
   const float ssx = (nx % 2 == 0) ? 0.5f : 0.f, ssy = (ny % 2 == 0) ? 0.5f : 0.f, ssz = (nz % 2 == 0) ? 0.5f : 0.f;
   const float u = (float)x - (float)nx / 2.0f;
@@ -325,7 +330,7 @@ emc_status emc_sf3d(int half, int squared, const unsigned size[3], const float* 
   }
   if (rs == EMC_OK) {
     dim3 block(32, 8), grid((nx + 31) / 32, (ny + 7) / 8, n_tilts);
-    emc::k_sf3d_ctfs<<<grid, block, 0, st>>>(d_c, d_g, d_occ, d_exp, nx, ny, imgs);
+    emc::k_sf3d_ctfs<<<grid, block, 0, st>>>(d_c, d_g, d_occ, d_exp, nx, ny, (int)n_tilts, imgs);
     dim3 grid2((nx + 31) / 32, (ny + 7) / 8);
     emc::k_sf3d_accum<<<grid2, block, 0, st>>>(imgs, d_sc, (int)n_tilts, nx, ny, nz, d_out);
     if (cudaGetLastError() != cudaSuccess) {
@@ -383,8 +388,11 @@ emc_status emc_sf3d_particles(const unsigned size[3], double sampling, const dou
     rshift[d] = recon_geometry[3 + d];
   }
   const long nv = (long)size[0] * size[1] * size[2];
+  const int nx = (int)size[0], ny = (int)size[1], nz = (int)size[2];
+  EMC_CHECK_ARG(nx > 0 && ny > 0 && nz > 0 && n < 65536, "emc_sf3d_particles: bad size or tilt count");
   cudaStream_t st = emc::as_stream(stream);
-  std::vector<float> df1(n), df2(n);
+  // every (particle, tilt) CTF, with the particle's defocus offset by its height along the beam
+  std::vector<emc::CtfDev> cs_all((size_t)count * n);
   for (int p = 0; p < count; ++p) {
     const double v[3] = {xyz[3 * (size_t)p] - origin[0] + rshift[0], xyz[3 * (size_t)p + 1] - origin[1] + rshift[1],
                          xyz[3 * (size_t)p + 2] - origin[2] + rshift[2]};
@@ -393,12 +401,60 @@ emc_status emc_sf3d_particles(const unsigned size[3], double sampling, const dou
       const float a = tilt[r] * (3.14159265358979323846f / 180.0f);
       const float z = -sinf(a) * (float)v[0] + cosf(a) * (float)v[2];
       const float d = def0[r] - z * pix[r];
-      df1[r] = d + ddf[r];
-      df2[r] = d - ddf[r];
+      const emc_ctf_params cp{pix[r], lam[r], cs[r], ac[r], d + ddf[r], d - ddf[r], dphi[r]};
+      cs_all[(size_t)p * n + r] = emc::make_ctf(cp);
     }
-    EMC_TRY(emc_sf3d(0, 1, size, pix.data(), lam.data(), cs.data(), df1.data(), df2.data(), dphi.data(), ac.data(),
-                     (unsigned)n, tilt.data(), expo.data(), occ.data(), d_out + (size_t)p * nv, stream));
   }
+  std::vector<emc::CtfGrid> gs(n);
+  std::vector<float2> sc(n);
+  for (int r = 0; r < n; ++r) {
+    gs[r] = emc::make_grid(nx, ny, 0, 1, 1, pix[r]);
+    const float a = -tilt[r] * 3.14159265358979323f / 180.0f;  // sincosf(deg_2_rad(-tilt)) (mexSF3D.cu:131-135)
+    sc[r] = make_float2(sinf(a), cosf(a));
+  }
+  // particles per launch pair: the tilt images of a chunk stay under 1 GiB, and the image grid's z
+  // extent (particles x tilts) under 65536
+  const size_t img_per = sizeof(float) * (size_t)n * nx * ny;
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>({(size_t)count, (size_t)(65535 / n),
+                                                               (size_t)(1ull << 30) / img_per}));
+  const size_t c_bytes = sizeof(emc::CtfDev) * cs_all.size();
+  const size_t hdr = ((c_bytes + sizeof(emc::CtfGrid) * n + 15) / 16) * 16 + sizeof(float2) * n + 2 * sizeof(float) * n;
+  char* buf = nullptr;
+  EMC_CUDA(cudaMallocAsync(&buf, img_per * chunk + hdr + 256, st));
+  float* imgs = reinterpret_cast<float*>(buf);
+  char* q = buf + ((img_per * chunk + 15) / 16) * 16;
+  emc::CtfDev* d_c = reinterpret_cast<emc::CtfDev*>(q);
+  emc::CtfGrid* d_g = reinterpret_cast<emc::CtfGrid*>(q + c_bytes);
+  q += ((c_bytes + sizeof(emc::CtfGrid) * n + 15) / 16) * 16;
+  float2* d_sc = reinterpret_cast<float2*>(q);
+  float* d_occ = reinterpret_cast<float*>(d_sc + n);
+  float* d_exp = d_occ + n;
+  emc_status rs0 = EMC_OK;
+  if (cudaMemcpyAsync(d_c, cs_all.data(), c_bytes, cudaMemcpyHostToDevice, st) ||
+      cudaMemcpyAsync(d_g, gs.data(), sizeof(emc::CtfGrid) * n, cudaMemcpyHostToDevice, st) ||
+      cudaMemcpyAsync(d_sc, sc.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, st) ||
+      cudaMemcpyAsync(d_occ, occ.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st) ||
+      cudaMemcpyAsync(d_exp, expo.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st) ||
+      cudaMemsetAsync(d_out, 0, sizeof(float) * (size_t)nv * count, st)) {
+    emc::set_error("emc_sf3d_particles: upload failed");
+    rs0 = EMC_E_CUDA;
+  }
+  dim3 block(32, 8);
+  for (int p0 = 0; p0 < count && rs0 == EMC_OK; p0 += chunk) {
+    const int cnt = std::min(chunk, count - p0);
+    emc::k_sf3d_ctfs<<<dim3((nx + 31) / 32, (ny + 7) / 8, cnt * n), block, 0, st>>>(d_c + (size_t)p0 * n, d_g, d_occ,
+                                                                                     d_exp, nx, ny, n, imgs);
+    emc::k_sf3d_accum<<<dim3((nx + 31) / 32, (ny + 7) / 8, cnt), block, 0, st>>>(imgs, d_sc, n, nx, ny, nz,
+                                                                                 d_out + (size_t)p0 * nv);
+    if (cudaGetLastError() != cudaSuccess) {
+      emc::set_error("emc_sf3d_particles: launch failed");
+      rs0 = EMC_E_CUDA;
+    }
+  }
+  // the host tables must outlive their copies
+  if (cudaStreamSynchronize(st) != cudaSuccess && rs0 == EMC_OK) rs0 = EMC_E_CUDA;
+  cudaFreeAsync(buf, st);
+  EMC_TRY(rs0);
   // SF3D - (min(SF3D(:)) - 1e-4) (:55)
   unsigned* keys = nullptr;
   EMC_CUDA(cudaMallocAsync((void**)&keys, sizeof(unsigned) * count, st));

@@ -1,5 +1,6 @@
 // fft_passes.cu -- launchers for the generic FFT passes and the mexFFT-style API.
 #include <algorithm>
+#include <atomic>
 #include <new>
 
 #include "fft_passes.cuh"
@@ -46,19 +47,23 @@ static emc_status cols_t(const float2* in, float2* out, long stride, long inner,
   const float2* tw = device_twiddles(L);
   if (!tw) return EMC_E_CUDA;
   auto kern = k_cols<L, SIGN, C::P, C::T>;
-  static int resident[64] = {0};  // CTAs per SM, per device
+  // CTAs per SM, per device: the first launch on a device queries it; threads that race there both
+  // store the same value
+  static std::atomic<int> resident[64];
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64) return EMC_E_CUDA;
-  if (!resident[dev]) {
+  int res = resident[dev].load(std::memory_order_acquire);
+  if (!res) {
     if (C::smem > 48 * 1024)
       EMC_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem));
     int nb = 0;
     EMC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, C::P * C::T, C::smem));
-    resident[dev] = std::max(nb, 1);
+    res = std::max(nb, 1);
+    resident[dev].store(res, std::memory_order_release);
   }
   const long units = (inner + C::T - 1) / C::T * outer;
-  const long ctas = std::min<long>(units, (long)resident[dev] * device_sm_count());
+  const long ctas = std::min<long>(units, (long)res * device_sm_count());
   kern<<<(unsigned)ctas, C::P * C::T, C::smem, st>>>(in, out, stride, inner, outer, outer_pitch, tw);
   EMC_LAUNCH_CHECK();
   return EMC_OK;

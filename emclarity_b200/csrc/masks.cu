@@ -278,10 +278,35 @@ __global__ void k_cref_eval(int nx, int ny, int nz, float pixel, const double* _
   }
 }
 
+// ifftshift of `count` centred volumes, keeping the half spectrum: out[v][r][q][p] (p <= nx/2) =
+// in[v][(r + cz) % nz][(q + cy) % ny][(p + cx) % nx] with c = floor(n/2) per axis.
+__global__ void k_centred_to_half(const float* __restrict__ in, int nx, int ny, int nz, long count,
+                                  float* __restrict__ out) {
+  const int nh = nx / 2 + 1;
+  const long per = (long)nh * ny * nz, nv = (long)nx * ny * nz;
+  const long total = per * count;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long v = i / per, j = i % per;
+    const int p = (int)(j % nh), q = (int)((j / nh) % ny), r = (int)(j / ((long)nh * ny));
+    out[i] = in[v * nv + ((long)((r + nz / 2) % nz) * ny + (q + ny / 2) % ny) * nx + (p + nx / 2) % nx];
+  }
+}
+
 }  // namespace
 }  // namespace emc
 
 extern "C" {
+
+emc_status emc_centred_to_half(const float* d_in, int nx, int ny, int nz, int count, float* d_out, void* stream) {
+  using namespace emc;
+  EMC_CHECK_ARG(d_in && d_out && nx > 0 && ny > 0 && nz > 0 && count >= 0, "emc_centred_to_half: bad argument");
+  EMC_CHECK_ARG(d_in != d_out, "emc_centred_to_half: in place is not supported");
+  if (count == 0) return EMC_OK;
+  const long total = (long)(nx / 2 + 1) * ny * nz * count;
+  k_centred_to_half<<<grid_blocks(total), 256, 0, as_stream(stream)>>>(d_in, nx, ny, nz, count, d_out);
+  EMC_LAUNCH_CHECK();
+  return EMC_OK;
+}
 
 emc_status emc_binary_wedge(int n, float tilt_min_deg, float tilt_max_deg, int smooth, int layout, float* d_out,
                             void* stream) {

@@ -37,6 +37,25 @@ __global__ void k_search_best(const DevParticle* __restrict__ parts, int np, con
   out[p] = h;
 }
 
+// x extent of the non-zero mask voxels of every (z, y) row (lo = n, hi = 0 for an empty row).
+__global__ void k_mask_rows(const float* __restrict__ mask, int n, unsigned* __restrict__ rows) {
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n * n) return;
+  const float* m = mask + (long)row * n;
+  int lo = n, hi = 0;
+  for (int x = lane; x < n; x += 32)
+    if (m[x] != 0.f) {
+      lo = min(lo, x);
+      hi = max(hi, x + 1);
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if (lane == 0) rows[row] = (unsigned)lo | ((unsigned)hi << 16);
+}
+
 // Particle energies taken from device memory (written there by emc_particle_spectrum) when the run
 // executes, for emc_search_run_energies.
 __global__ void k_search_energies(DevParticle* __restrict__ parts, int np, const double* __restrict__ energy) {
@@ -275,6 +294,7 @@ struct emc_search_s {
     float* mask = nullptr;
     float* wref = nullptr;
     void* cells = nullptr;
+    unsigned* mask_rows = nullptr;
     int n = 0;
     int dtype = 0;
   };
@@ -317,10 +337,27 @@ struct emc_search_s {
   RunTables* cur = nullptr;        // tables of the run being recorded or launched eagerly
   emc::DevBuf<emc::EvalResult> d_results;
   emc::DevBuf<unsigned long long> d_best_keys;
-  emc::DevBuf<float2> s1, s2;
-  emc::DevBuf<emc::EvalStats> stats;
-  emc::DevBuf<unsigned long long> keys;
-  emc::DevBuf<unsigned> done;
+  // Per-evaluation scratch of a chunk, one set per overlap slot: chunk i of a recorded run uses slot
+  // i % overlap and its own branch of the graph, so consecutive chunks run concurrently (pass A of one
+  // beside passes B and C of the other, filling each other's tails) while chunks of one slot stay in order.
+  static constexpr int kMaxSlots = 2;
+  struct Scratch {
+    emc::DevBuf<float2> s1, s2;
+    emc::DevBuf<emc::EvalStats> stats;
+    emc::DevBuf<unsigned long long> keys;
+    emc::DevBuf<unsigned> done;
+    void release() {
+      s1.release();
+      s2.release();
+      stats.release();
+      keys.release();
+      done.release();
+    }
+  };
+  Scratch slot[kMaxSlots];
+  int overlap = kMaxSlots;        // slots used by recorded runs (profiled runs use one)
+  cudaStream_t branch = nullptr;  // the second branch's stream during capture
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 
   const double* run_energy = nullptr;  // device energies of the run being recorded (or null)
   cudaStream_t cap_stream = nullptr;
@@ -380,9 +417,16 @@ emc_status emc_search_create(emc_search_t* out) {
       s->scratch_budget = std::max<size_t>(free_b / 8, 16ull << 20);
   }
   s->graphs.reserve(emc_search_s::kGraphCache);
-  if (cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->branch, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->join_ev, cudaEventDisableTiming) != cudaSuccess) {
+    if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
+    if (s->branch) cudaStreamDestroy(s->branch);
+    if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+    if (s->join_ev) cudaEventDestroy(s->join_ev);
     delete s;
-    emc::set_error("emc_search_create: stream creation failed");
+    emc::set_error("emc_search_create: stream or event creation failed");
     return EMC_E_CUDA;
   }
   *out = s;
@@ -409,6 +453,10 @@ emc_status emc_search_add_reference(emc_search_t s, const float* d_ref, int n, c
   if (d_mask) {
     EMC_CUDA(cudaMalloc(&r.mask, nv * sizeof(float)));
     EMC_CUDA(cudaMemcpyAsync(r.mask, d_mask, nv * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    // each row's x extent of non-zero mask voxels: the gather skips the cells outside it
+    EMC_CUDA(cudaMalloc(&r.mask_rows, sizeof(unsigned) * (size_t)n * n));
+    emc::k_mask_rows<<<(n * n + 7) / 8, 256, 0, st>>>(r.mask, n, r.mask_rows);
+    EMC_LAUNCH_CHECK();
   }
   if (d_wref) {
     EMC_CUDA(cudaMalloc(&r.wref, nhalf * sizeof(float)));
@@ -474,20 +522,21 @@ static emc_status harvest_slot(emc_search_t s, int slot) {
   return EMC_OK;
 }
 
-static emc::SearchChunkArgs chunk_args(emc_search_t s, const Chunk& c) {
+static emc::SearchChunkArgs chunk_args(emc_search_t s, const Chunk& c, int slot = 0) {
+  const emc_search_s::Scratch& sc = s->slot[slot];
   emc::SearchChunkArgs a;
   a.items = s->cur->items.p + c.item_offset;
   a.parts = s->cur->parts.p;
   a.refs = s->d_refs.p;
   a.dmat = s->d_dmat.p;
-  a.s1 = s->s1.p;
-  a.s2 = s->s2.p;
-  a.stats = s->stats.p;
-  a.keys = s->keys.p;
+  a.s1 = sc.s1.p;
+  a.s2 = sc.s2.p;
+  a.stats = sc.stats.p;
+  a.keys = sc.keys.p;
   a.n_items = c.count;
   a.radius = effective_radius(s, c.n);
   a.interp = s->interp;
-  a.done = s->done.p;
+  a.done = sc.done.p;
   a.results = s->d_results.p;
   a.best_keys = s->d_best_keys.p;
   return a;
@@ -544,17 +593,30 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
                                 float* d_cc, int* d_peak, emc_search_hit* d_best, cudaStream_t st) {
   EMC_CUDA(cudaMemsetAsync(s->d_best_keys.p, 0, sizeof(unsigned long long) * np, st));
   // per-evaluation scratch starts clear; the last pass-C CTA of each evaluation clears it again
-  EMC_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(emc::EvalStats) * s->stats.cap, st));
-  EMC_CUDA(cudaMemsetAsync(s->keys.p, 0, sizeof(unsigned long long) * s->keys.cap, st));
-  EMC_CUDA(cudaMemsetAsync(s->done.p, 0, sizeof(unsigned) * s->done.cap, st));
+  const int nslots = s->profiling ? 1 : s->overlap;
+  for (int k = 0; k < nslots; ++k) {
+    emc_search_s::Scratch& sc = s->slot[k];
+    EMC_CUDA(cudaMemsetAsync(sc.stats.p, 0, sizeof(emc::EvalStats) * sc.stats.cap, st));
+    EMC_CUDA(cudaMemsetAsync(sc.keys.p, 0, sizeof(unsigned long long) * sc.keys.cap, st));
+    EMC_CUDA(cudaMemsetAsync(sc.done.p, 0, sizeof(unsigned) * sc.done.cap, st));
+  }
   long launches = 0;
   if (s->run_energy) {
     emc::k_search_energies<<<(np + 255) / 256, 256, 0, st>>>(s->cur->parts.p, np, s->run_energy);
     EMC_LAUNCH_CHECK();
     ++launches;
   }
-  for (const Chunk& c : chunks) {
-    const emc::SearchChunkArgs a = chunk_args(s, c);
+  // the second branch forks from the stream after the set-up above and joins before the outputs
+  const bool two = nslots > 1 && chunks.size() > 1;
+  if (two) {
+    EMC_CUDA(cudaEventRecord(s->fork_ev, st));
+    EMC_CUDA(cudaStreamWaitEvent(s->branch, s->fork_ev, 0));
+  }
+  for (size_t ci = 0; ci < chunks.size(); ++ci) {
+    const Chunk& c = chunks[ci];
+    const int slot = two ? (int)(ci % 2) : 0;
+    const cudaStream_t cst = slot ? s->branch : st;
+    const emc::SearchChunkArgs a = chunk_args(s, c, slot);
     cudaEvent_t* ev = nullptr;
     if (s->profiling) {
       const int slot = s->ev_next;
@@ -563,13 +625,17 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
       ev = s->ev[slot];
       s->ev_pending[slot] = true;
     }
-    EMC_TRY(emc::launch_chunk_any(c.n, c.dtype, planes_slot(s, c.n, c.dtype), a, st, ev));
-    if (ev) EMC_CUDA(cudaEventRecord(ev[4], st));  // decode runs inside pass C
+    EMC_TRY(emc::launch_chunk_any(c.n, c.dtype, planes_slot(s, c.n, c.dtype), a, cst, ev));
+    if (ev) EMC_CUDA(cudaEventRecord(ev[4], cst));  // decode runs inside pass C
     launches += 3;
     if (s->profiling) {
       for (int k = 0; k < 4; ++k) s->prof_launches[k] += 1;
       s->prof_evals += c.count;
     }
+  }
+  if (two) {
+    EMC_CUDA(cudaEventRecord(s->join_ev, s->branch));
+    EMC_CUDA(cudaStreamWaitEvent(st, s->join_ev, 0));
   }
   if (d_best) {
     emc::k_search_best<<<(np + 127) / 128, 128, 0, st>>>(s->cur->parts.p, np, s->d_results.p, s->d_best_keys.p, d_best);
@@ -667,12 +733,23 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
       }
     }
   // ---- shared scratch (a reallocation invalidates every recorded request)
-  const void* before[7] = {s->d_results.p, s->d_best_keys.p, s->stats.p, s->keys.p, s->done.p, s->s1.p, s->s2.p};
+  const int nslots = s->profiling ? 1 : s->overlap;
+  auto scratch_ptrs = [&](std::vector<const void*>& v) {
+    v = {s->d_results.p, s->d_best_keys.p};
+    for (int k = 0; k < emc_search_s::kMaxSlots; ++k) {
+      const emc_search_s::Scratch& sc = s->slot[k];
+      v.insert(v.end(), {sc.stats.p, sc.keys.p, sc.done.p, sc.s1.p, sc.s2.p});
+    }
+  };
+  std::vector<const void*> before, after;
+  scratch_ptrs(before);
   EMC_TRY(s->d_results.reserve(total));
   EMC_TRY(s->d_best_keys.reserve(np));
-  EMC_TRY(s->stats.reserve(max_chunk));
-  EMC_TRY(s->keys.reserve(max_chunk));
-  EMC_TRY(s->done.reserve(max_chunk));
+  for (int k = 0; k < nslots; ++k) {
+    EMC_TRY(s->slot[k].stats.reserve(max_chunk));
+    EMC_TRY(s->slot[k].keys.reserve(max_chunk));
+    EMC_TRY(s->slot[k].done.reserve(max_chunk));
+  }
   {
     // split scratch between S1 and S2 proportionally to the largest chunk of each size
     size_t s1n = 0, s2n = 0;
@@ -682,17 +759,18 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
       s1n = std::max(s1n, (size_t)c.count * c.n * c.n * nh);
       s2n = std::max(s2n, (size_t)c.count * (2 * r + 1) * c.n * nh);
     }
-    EMC_TRY(s->s1.reserve(s1n));
-    EMC_TRY(s->s2.reserve(s2n));
+    for (int k = 0; k < nslots; ++k) {
+      EMC_TRY(s->slot[k].s1.reserve(s1n));
+      EMC_TRY(s->slot[k].s2.reserve(s2n));
+    }
   }
-  {
-    const void* after[7] = {s->d_results.p, s->d_best_keys.p, s->stats.p, s->keys.p, s->done.p, s->s1.p, s->s2.p};
-    if (memcmp(before, after, sizeof(before)) != 0) drop_graphs(s);
-  }
+  scratch_ptrs(after);
+  if (before != after) drop_graphs(s);
   if (s->refs_dirty) {
     std::vector<emc::DevRef> dr(s->refs.size());
     for (size_t i = 0; i < s->refs.size(); ++i)
-      dr[i] = {s->refs[i].data, s->refs[i].mask, s->refs[i].wref, s->refs[i].n, s->refs[i].dtype, s->refs[i].cells};
+      dr[i] = {s->refs[i].data, s->refs[i].mask,  s->refs[i].wref,     s->refs[i].n,
+               s->refs[i].dtype, s->refs[i].cells, s->refs[i].mask_rows};
     EMC_TRY(s->d_refs.reserve(dr.size()));
     EMC_CUDA(cudaMemcpy(s->d_refs.p, dr.data(), sizeof(emc::DevRef) * dr.size(), cudaMemcpyHostToDevice));
     s->refs_dirty = false;
@@ -858,6 +936,15 @@ emc_status emc_search_set_planes(emc_search_t s, int box, int planes) {
   return EMC_OK;
 }
 
+emc_status emc_search_set_overlap(emc_search_t s, int slots) {
+  EMC_CHECK_ARG(s, "emc_search_set_overlap: null handle");
+  EMC_CHECK_ARG(slots >= 1 && slots <= emc_search_s::kMaxSlots, "emc_search_set_overlap: %d slots (1 or %d)", slots,
+                emc_search_s::kMaxSlots);
+  s->overlap = slots;
+  drop_graphs(s);
+  return EMC_OK;
+}
+
 emc_status emc_search_get_planes(emc_search_t s, int box, int dtype, int* planes, float ms_per_option[4]) {
   EMC_CHECK_ARG(s && planes, "emc_search_get_planes: null argument");
   EMC_CHECK_ARG(emc::box_supported(box), "emc_search_get_planes: box %d not supported (64, 96, 128)", box);
@@ -881,16 +968,16 @@ emc_status emc_search_destroy(emc_search_t s) {
     cudaFree(r.mask);
     cudaFree(r.wref);
     cudaFree(r.cells);
+    cudaFree(r.mask_rows);
   }
   s->d_refs.release();
   s->d_dmat.release();
   s->d_results.release();
   s->d_best_keys.release();
-  s->s1.release();
-  s->s2.release();
-  s->stats.release();
-  s->keys.release();
-  s->done.release();
+  for (auto& sc : s->slot) sc.release();
+  if (s->branch) cudaStreamDestroy(s->branch);
+  if (s->fork_ev) cudaEventDestroy(s->fork_ev);
+  if (s->join_ev) cudaEventDestroy(s->join_ev);
   if (s->cap_stream) cudaStreamDestroy(s->cap_stream);
   delete s;
   return EMC_OK;

@@ -38,6 +38,7 @@ struct DevRef {
   int n;
   int dtype;
   const void* cells;   // (n+1)^3 trilinear corner cells (see build_cells) or null
+  const unsigned* mask_rows;  // per (z, y) row: lo | hi << 16, the x extent [lo, hi) of mask != 0, or null
 };
 
 // Trilinear corner cells: cell (i, j, k), i, j, k in [-1, n-1], holds the 8 voxels
@@ -313,10 +314,13 @@ __device__ __forceinline__ Tv block_sum(Tv v, Tv* red) {
 // its sample point once per row and steps 32 voxels along x by adding 32 x (first column of the
 // sampling matrix); its RU * N / 32 cell loads are all issued before any is used.  Sums of r and
 // r^2 are formed per step in FP32 and accumulated in FP64.
+// A lane whose voxel lies outside its row's mask extent (mask_rows) skips its cell: it reads cell 0,
+// which every such lane of the warp shares, and its value is 0 as the mask would make it.
 template <int N, typename T, int MODE, int GG>
 __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells, const float* __restrict__ mask,
-                                             const float m[9], float tx, float ty, float tz, int z0,
-                                             float* __restrict__ fplanes, double& s1, double& s2) {
+                                             const unsigned* __restrict__ mask_rows, const float m[9], float tx,
+                                             float ty, float tz, int z0, float* __restrict__ fplanes, double& s1,
+                                             double& s2) {
   using C = SearchCfg<N, GG>;
   constexpr int G = C::G, NT = C::NT_A, NH = C::NH;
   constexpr int SEG = N / 32;                     // row segments per lane
@@ -338,6 +342,8 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
 #pragma unroll
     for (int ru = 0; ru < RU; ++ru) {
       const int row = r0 + ru, y = row % N, zl = row / N, z = z0 + zl;
+      const unsigned ext = mask_rows ? __ldg(mask_rows + z * N + y) : ((unsigned)N << 16);
+      const int lo = (int)(ext & 0xffffu), hi = (int)(ext >> 16);
       const float pu = (float)(lane - c) - tx, pv = (float)(y - c) - ty, pw = (float)(z - c) - tz;
       float sx = fmaf(m[0], pu, fmaf(m[1], pv, m[2] * pw)) + (float)c;
       float sy = fmaf(m[3], pu, fmaf(m[4], pv, m[5] * pw)) + (float)c;
@@ -345,9 +351,13 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
 #pragma unroll
       for (int k = 0; k < SEG; ++k) {
         const int u = ru * SEG + k;
-        const unsigned ci = cell_index_gather<MODE>(N, sx, sy, sz, fr[u], ok[u]);
+        const int x = lane + 32 * k;
+        const bool in = x >= lo && x < hi;
+        unsigned ci = cell_index_gather<MODE>(N, sx, sy, sz, fr[u], ok[u]);
+        ci = in ? ci : 0u;
+        ok[u] = ok[u] && in;
         cv[u] = load_cell(cells + ci);
-        mk[u] = mask ? __ldg(mask + ((long)z * N + y) * N + lane + 32 * k) : 1.f;
+        mk[u] = !mask ? 1.f : (in ? __ldg(mask + ((long)z * N + y) * N + x) : 0.f);
         sx += step_x;
         sy += step_y;
         sz += step_z;
@@ -417,11 +427,11 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
   double s1 = 0.0, s2 = 0.0;
   float* fplanes = reinterpret_cast<float*>(planes);
   if (rf.cells && a.interp == EMC_INTERP_LINEAR) {
-    gather_cells<N, T, EMC_INTERP_LINEAR, GG>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, m, tx, ty, tz, z0,
-                                          fplanes, s1, s2);
+    gather_cells<N, T, EMC_INTERP_LINEAR, GG>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, rf.mask_rows, m, tx,
+                                              ty, tz, z0, fplanes, s1, s2);
   } else if (rf.cells && a.interp == EMC_INTERP_LINEAR_BORDER) {
-    gather_cells<N, T, EMC_INTERP_LINEAR_BORDER, GG>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, m, tx, ty, tz,
-                                                 z0, fplanes, s1, s2);
+    gather_cells<N, T, EMC_INTERP_LINEAR_BORDER, GG>(reinterpret_cast<const CellT<T>*>(rf.cells), mask, rf.mask_rows,
+                                                     m, tx, ty, tz, z0, fplanes, s1, s2);
   } else {
     for (int idx = threadIdx.x; idx < G * N * N; idx += C::NT_A) {
       const int x = idx % N, y = (idx / N) % N, zl = idx / (N * N);

@@ -122,8 +122,11 @@ emc_status set_attrs_noalloc() {
 }
 
 // Once per device, with that device current: resolve the device address of the scratch array
-// (its host-side name is only a stand-in), upload the twiddle tables, set kernel attributes.
-emc_status setup_device(unsigned char** base) {
+// (its host-side name is only a stand-in), upload the twiddle tables on the caller's stream and wait
+// for that stream (so no other thread's call on another stream can read them early, and the legacy
+// default stream is not involved), set kernel attributes.  Under CUDA's lazy module loading the
+// array itself is allocated when this first call loads the module.
+emc_status setup_device(unsigned char** base, cudaStream_t stream) {
   int dev = 0;
   EMC_CUDA(cudaGetDevice(&dev));
   EMC_CHECK_ARG(dev >= 0 && dev < kMaxDev, "emc_search_plain_noalloc: device %d out of range", dev);
@@ -138,7 +141,9 @@ emc_status setup_device(unsigned char** base) {
         const double a = -2.0 * M_PI * (double)m / (double)n;
         tw[tw_offset(n) + m] = make_float2((float)cos(a), (float)sin(a));
       }
-    EMC_CUDA(cudaMemcpy((unsigned char*)p + kTwOff, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    EMC_CUDA(cudaMemcpyAsync((unsigned char*)p + kTwOff, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice,
+                             stream));
+    EMC_CUDA(cudaStreamSynchronize(stream));
     EMC_TRY((set_attrs_noalloc<64, float>()));
     EMC_TRY((set_attrs_noalloc<96, float>()));
     EMC_TRY((set_attrs_noalloc<128, float>()));
@@ -194,8 +199,8 @@ emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int
   EMC_CHECK_ARG(chunk >= 1, "emc_search_plain_noalloc: box %d with radius %d needs %zu B of scratch per "
                 "evaluation, more than the %zu B available", n, peak_radius, per_eval, avail);
   unsigned char* base = nullptr;
-  EMC_TRY(setup_device(&base));
   cudaStream_t st = as_stream(stream);
+  EMC_TRY(setup_device(&base, st));
 
   // one host-to-device copy of everything the kernels read besides the caller's buffers
   const size_t hdr = kHdrOff, dm = kDmatOff, it = kItemOff;

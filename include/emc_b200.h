@@ -343,16 +343,25 @@ EMC_API emc_status emc_search_timings(emc_search_t s, double ms[4], long launche
  * timed; may be NULL). */
 EMC_API emc_status emc_search_set_planes(emc_search_t s, int box, int planes);
 EMC_API emc_status emc_search_get_planes(emc_search_t s, int box, int dtype, int* planes, float ms_per_option[4]);
+/* Tuning hook (no counterpart in the reference).  A recorded run keeps slots = 1 or 2 sets of chunk
+ * scratch (2 by default); with 2, consecutive chunks go to two branches of the CUDA graph and run
+ * concurrently (the passes of one chunk fill the tails of the other's), chunks of one slot in order.
+ * Profiled runs (emc_search_set_profiling) use one slot so that per-pass times stay separable. */
+EMC_API emc_status emc_search_set_overlap(emc_search_t s, int slots);
 
 
 /* Single-particle search that allocates no device memory.  No counterpart in the reference.
  * For callers that may not call cudaMalloc after start-up: hosts whose own pool owns the GPU
  * memory (MATLAB's gpuArray allocator, a framework caching allocator), where a raw allocation
  * can fail or fragment the pool, and loops that must keep a bounded latency.  All scratch lives
- * in one static 24 MiB device array per GPU (held from library load until exit).  The first call
- * on a device resolves that array's address and uploads FFT twiddles (make it before any stream
- * capture).  Every call reuses the same array, so calls that overlap on the GPU race; the call
- * synchronises the stream before returning.  Limits (EMC_E_ARG beyond them): box 64, 96 or 128,
+ * in one static 24 MiB device array per GPU, held until the process exits.  The first call on a
+ * device resolves that array's address and uploads FFT twiddles on the caller's stream (make it
+ * before any stream capture); under CUDA's default lazy module loading that first call is also
+ * when the driver allocates the array, so make it (any valid small search) at start-up, before the
+ * caller's pool takes the GPU's memory, or load modules eagerly (CUDA_MODULE_LOADING=EAGER).
+ * Every call reuses the same array, so calls that overlap on the GPU race; the call synchronises
+ * the stream before returning.  The search runs with no particle wedge (wdgMask = 1): fold any
+ * particle-side weight into d_spectrum.  Limits (EMC_E_ARG beyond them): box 64, 96 or 128,
  * FP32 reference, 1..4096 orientations (host (phi, theta, psi) triples), peak radius 1..15.
  * Same arguments and outputs as emc_search_run for one particle (device outputs may be NULL). */
 EMC_API emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int n,
@@ -478,12 +487,20 @@ EMC_API emc_status emc_average_reset(emc_average_t a, void* stream);
 EMC_API emc_status emc_average_boxes(emc_average_t a, int* n, int* nw);
 EMC_API emc_status emc_average_destroy(emc_average_t a);
 
+/* ifftshift of count centred volumes (nx*ny*nz each, x fastest) cropped to their half spectra
+ * ((nx/2+1)*ny*nz each, FFT order): the weight volumes of the reference (SF3D, wedge masks; centred
+ * as the reference builds them, then ifftshift-ed before use, e.g. iMaxWedgeIfft at
+ * BH_alignRaw3d_v2.m:1092-1099) in the form the search reads as wdgMask.  Not in place. */
+EMC_API emc_status emc_centred_to_half(const float* d_in, int nx, int ny, int nz, int count, float* d_out,
+                                       void* stream);
 /* BH_weightMaskMex(SIZE, SAMPLING, TLT, xyzSubTomo, reconGeometry) (masking/BH_weightMaskMex.m:1-60)
  * for count particles: the tilt table (rows x cols, row-major as emc_tlt_read; columns as
  * :16-30) is sorted on column 1 and cast to single; each particle's defocus is offset by the
  * height of its position along every tilt's beam; the volumes come from emc_sf3d (full grid, CTF
  * squared) and are shifted by -(min - 1e-4).  xyz: [count][3]; recon_geometry: the 2 x 3
- * reconGeometry, row-major (size, then shift); d_out: [count][size^3]. */
+ * reconGeometry, row-major (size, then shift); d_out: [count][size^3].  All particles' tilt images
+ * are made by one launch per chunk of particles (under 1 GiB of images) and accumulated by a
+ * second; the call synchronises the stream once. */
 EMC_API emc_status emc_sf3d_particles(const unsigned size[3], double sampling, const double* tlt, int rows,
                                       int cols, const double* xyz, const double recon_geometry[6], int count,
                                       float* d_out, void* stream);

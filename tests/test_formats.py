@@ -6,7 +6,9 @@ import pytest
 
 from oracle import oracle as O
 
-REF_TLT = "/root/reference/docs/anticipatedTiltAlignment/ctf/riboNew05_ali1_ctf.tlt"
+# The reference's own tilt tables, where its tree is available: EMC_REFERENCE_DIR names its root.
+REF_DIR = os.environ.get("EMC_REFERENCE_DIR", "")
+REF_TLT = os.path.join(REF_DIR, "docs", "anticipatedTiltAlignment", "ctf", "riboNew05_ali1_ctf.tlt") if REF_DIR else ""
 
 
 @pytest.mark.parametrize("mode", [0, 1, 2, 6])
@@ -78,7 +80,7 @@ def test_tilt_table_parsing(built_lib, tmp_path):
         api.tlt_read(bad)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_TLT), reason="reference tree not present")
+@pytest.mark.skipif(not REF_TLT or not os.path.exists(REF_TLT), reason="EMC_REFERENCE_DIR not set or tree absent")
 def test_reference_tilt_table_parses(built_lib):
     from emclarity_b200 import api
     t = api.tlt_read(REF_TLT)

@@ -76,3 +76,50 @@ def test_sf3d_particles_match_restatement(built_lib, cuda):
         assert np.abs(g - r).max() <= 2e-4 * np.abs(r).max(), np.abs(g - r).max()
     # the two positions differ in height, so their defocus and weights differ
     assert np.abs(got[0] - got[1]).max() > 1e-3 * np.abs(got[0]).max()
+
+
+def test_sf3d_particles_batched_equals_one_at_a_time(built_lib, cuda):
+    """One call over 1,700 particles (two chunks of tilt images) gives every particle the volume a
+    one-particle call gives it."""
+    from emclarity_b200 import api
+    rng = np.random.default_rng(7)
+    t = _tilt_table(rng)
+    size = (32, 32, 32)
+    rg = np.array([[512, 512, 256], [0.0, 1.0, -2.0]])
+    xyz = np.column_stack([rng.uniform(0, 512, 1700), rng.uniform(0, 512, 1700), rng.uniform(0, 256, 1700)])
+    batch = api.sf3d_particles(size, 2.0, t, xyz, rg)
+    for i in (0, 1, 911, 1597, 1598, 1699):
+        one = api.sf3d_particles(size, 2.0, t, xyz[i:i + 1], rg)[0]
+        assert torch.equal(batch[i], one), i
+
+
+def test_sf3d_weight_as_the_search_wedge(built_lib, cuda):
+    """The per-particle SF3D weight, ifftshift-ed to a half spectrum (iMaxWedgeIfft), as the search's
+    wdgMask: the search against the FP64 oracle with the same weight."""
+    from emclarity_b200 import api, synthetic
+    from tests.searchcheck import check_best, check_cc_and_peaks
+    rng = np.random.default_rng(8)
+    n = 64
+    t = _tilt_table(rng)
+    rg = np.array([[512, 512, 256], [0.0, 0.0, 0.0]])
+    sf = api.sf3d_particles((n, n, n), 4.0, t, np.array([[256.0, 300.0, 90.0]]), rg)
+    w = api.centred_to_half(sf)[0].contiguous()
+    assert torch.equal(w.cpu(), torch.from_numpy(np.fft.ifftshift(sf[0].cpu().numpy())[:, :, : n // 2 + 1].copy()))
+    ref = synthetic.blob_reference(rng, n)
+    mask = synthetic.soft_sphere_mask(n, 28)
+    truth = api.define_matrix([10.0, 20.0, -15.0], "inv")
+    part = synthetic.make_particle(torch.from_numpy(ref).cuda(), rng, truth, (2, -1, 0), w, 0.2)
+    grid = synthetic.local_grid(64, 8.0, 2.0)
+    prior = api.define_matrix([10.0, 20.0, -15.0], "inv") @ api.define_matrix([3.0, 2.0, -1.0], "inv").T
+    s = api.Search(peak_radius=6)
+    rid = s.add_reference(torch.from_numpy(ref).cuda(), torch.from_numpy(mask).cuda())
+    s.set_orientations(grid)
+    q, e = api.particle_spectrum(part)
+    cc, pk, best = s.run_host([s.particle(q, e.item(), rid, prior=prior, orient_count=len(grid), wedge=w)])
+    s.close()
+    P, _ = O.particle_spectrum(part.cpu().numpy())
+    mats = api.search_matrices(grid, prior)
+    kw = dict(mask=mask, wdg_mask=w.cpu().numpy())
+    cc_o, pk_o = O.search(ref, P, mats, radius=6, **kw)
+    check_cc_and_peaks(cc, pk, cc_o, pk_o, lambda o: O.xcf_translational(ref, P, mats[o], **kw)[2], "sf3d wedge")
+    check_best(best[0][1], cc_o, what="sf3d wedge")

@@ -418,3 +418,30 @@ def test_bf16_storage_against_fp64_oracle_on_unrounded_reference(built_lib, cuda
     gaps = np.array(gaps)
     assert np.median(rel) < 1e-3 and rel.max() < 1e-2, (np.median(rel), rel.max())
     assert np.all(gaps <= 2e-3), gaps.max()
+
+
+def test_chunk_overlap_gives_identical_results(built_lib, cuda):
+    """Two scratch slots (consecutive chunks on two graph branches) and one slot (chunks in order) give
+    bit-identical CCs, peaks and best orientations over many small chunks of uneven boxes."""
+    from emclarity_b200 import api, synthetic
+    rng = np.random.default_rng(77)
+    grid = synthetic.local_grid(40, 8.0, 2.0)
+    s = api.Search(peak_radius=5, chunk_evals=37)
+    s.set_orientations(grid)
+    descs, keep, _ = _uneven_batch(rng, s, [64, 96, 64, 128, 64, 96], grid, 5)
+    total = sum(d.orient_count for d in descs)
+    out = {}
+    for slots in (1, 2):
+        s.set_overlap(slots)
+        cc = torch.empty(total, device="cuda")
+        pk = torch.empty((total, 3), dtype=torch.int32, device="cuda")
+        best = torch.empty((len(descs), 5), dtype=torch.int32, device="cuda")
+        for _ in range(2):  # recorded, then replayed
+            cc.fill_(-7.0)
+            s.run(descs, cc=cc, peak=pk, best=best)
+            torch.cuda.synchronize()
+            out.setdefault(slots, []).append((cc.cpu().numpy(), pk.cpu().numpy(), best.cpu().numpy()))
+    s.close()
+    ref = out[1][0]
+    for cc, pk, best in out[1][1:] + out[2]:
+        assert np.array_equal(cc, ref[0]) and np.array_equal(pk, ref[1]) and np.array_equal(best, ref[2])
