@@ -271,7 +271,60 @@ struct SearchCfg {
   static constexpr size_t SMEM_B =
       sizeof(float2) * ((size_t)PY * TPB + N) + (PREF_B ? (sizeof(float2) + sizeof(float)) * (size_t)N * NHB : 0);
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
+  // Pass B keeps the product between the two z transforms in registers when a line is two equal
+  // radix-R stages with one butterfly per lane (N = R^2, team of R lanes): the forward transform's
+  // last stage leaves lane j holding elements j + R r, exactly the inputs the inverse transform's
+  // first stage gives it (64 = 8 x 8).
+  static constexpr bool FUSE_B = radix_of(N, 0) == radix_of(N, 1) && radix_of(N, 2) == 1 &&
+                                 radix_of(N, 0) * radix_of(N, 0) == N && P == radix_of(N, 0);
 };
+
+// Pass B's z line of local column kl for FUSE_B sizes: forward stage 1 in shared memory; forward
+// stage 2 into registers; there, element z = j + R r is weighted (wdgMask and wref, prefetched into
+// s_w), its |.|^2 added to E_R, multiplied into Q conj(R) (0 at the origin); the inverse stage 1 runs
+// on the same registers and inverse stage 2 in shared memory.  Same arithmetic as the separate
+// transforms and multiply loop, two shared-memory passes over the line fewer.
+template <int N>
+__device__ __forceinline__ void zline_fused(float2* buf, int stride, int lane, const float2* tw, bool active, int kl,
+                                            int kx, int ky, const float2* s_q, const float* s_w, bool weighted,
+                                            double& en) {
+  using C = SearchCfg<N>;
+  constexpr int R = radix_of(N, 0), P = C::P, NB = C::NHB;
+  stockham_stage<N, R, 1, -1, P, 1, 0>(buf, stride, lane, tw, active, nullptr);
+  float2 v[R];
+  const int j = lane;
+  if (active) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = buf[lpos<1>(j + r * R) * stride];
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle<-1>(tw, (r * j) % N));
+    Dft<R, -1>::run(v);
+    const double hw = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int z = j + R * r, i = z * NB + kl;
+      const bool origin = z == 0 && ky == 0 && kx == 0;
+      float2 rr = v[r];
+      if (weighted) {
+        const float wv = s_w[i];
+        rr.x *= wv;
+        rr.y *= wv;
+        if (!origin) en += hw * ((double)rr.x * rr.x + (double)rr.y * rr.y);
+      }
+      float2 x = cmulc(s_q[i], rr);
+      if (origin) x = make_float2(0.f, 0.f);
+      v[r] = x;
+    }
+    Dft<R, 1>::run(v);
+  }
+  __syncwarp();  // every lane has read the line before any writes it
+  if (active) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) buf[lpos<1>(j * R + r) * stride] = v[r];
+  }
+  __syncwarp();
+  stockham_stage<N, R, R, 1, P, 1, 1>(buf, stride, lane, tw, active, nullptr);
+}
 
 // Line li of a strided-FFT round handled by team `team`: consecutive teams get kx values 8
 // apart (NH is odd, so kx -> 8 kx mod NH is a permutation), which puts the teams of a warp on
@@ -447,7 +500,9 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
       s2 += (double)val * (double)val;
     }
   }
-  {
+  if (!(rf.wref || pt.wedge)) {
+    // E_R from the real-space sums (Parseval) is needed only without a weight on the reference;
+    // with one, pass B forms the weighted spectral energy (the branch is uniform over the block)
     double t1 = block_sum(s1, red[0]);
     double t2 = block_sum(s2, red[1]);
     if (threadIdx.x == 0) {
@@ -592,10 +647,42 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_
       if (i < N * NB && i % NB < cnt) tile[lpos<1>(i / NB) * TPB + i % NB] = v[k];
     }
   }
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  if constexpr (C::FUSE_B) {
+    // the prefetched slabs are read by other threads' lines: wait for this thread's copies (and fold
+    // a second weight into them), then the barrier publishes everyone's
+    cp_async_wait<0>();
+    if (w2) {
+#pragma unroll 1
+      for (int k = 0; k < IT; ++k) {
+        const int i = threadIdx.x + k * NT;
+        if (i < N * NB && i % NB < cnt) s_w[i] *= __ldg(w2 + ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB);
+      }
+    }
+    __syncthreads();
+    double en = 0.0;
+    for (int base = 0; base < TPB; base += C::TEAMS_B) {
+      const int li = base + team;
+      const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
+      zline_fused<N>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt, kl, k0 + kl, ky, s_q, s_w, w1 != nullptr, en);
+    }
+    if (w1) {
+      double t = block_sum(en, red);
+      if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
+    }
+    __syncthreads();
+    float2* dst = a.s2 + (size_t)e * w * N * NH + (size_t)ky * NH + k0;
+    for (int i = threadIdx.x; i < w * NB; i += NT) {
+      const int j = i / NB, kl = i % NB;
+      if (kl >= cnt) continue;
+      const int z = (j - a.radius + N) % N;
+      dst[(size_t)j * N * NH + kl] = tile[lpos<1>(z) * TPB + kl];
+    }
+    return;
+  }
   __syncthreads();
   // lines li in [0, TPB) -> local column (8 li) mod TPB (a permutation: TPB is odd), which puts the
   // teams of a warp on different banks; columns >= cnt are idle
-  const int team = threadIdx.x / P, lane = threadIdx.x % P;
   for (int base = 0; base < TPB; base += C::TEAMS_B) {
     const int li = base + team;
     const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
