@@ -422,6 +422,82 @@ __device__ __forceinline__ void fft_line_in(const Ld& ld, float2* buf, int strid
   StageChain<L, SIGN, P, PAD, 1, R0>::run(buf, stride, lane, tw, active, tc ? &tc->next : nullptr);
 }
 
+// Number of Stockham stages of a length-L plan and the product of the radices before stage s.
+__host__ __device__ constexpr int n_stages(int L, int s = 0) { return radix_of(L, s) <= 1 ? s : n_stages(L, s + 1); }
+__host__ __device__ constexpr int radix_product(int L, int s) { return s == 0 ? 1 : radix_of(L, s - 1) * radix_product(L, s - 1); }
+
+// Forward stages S .. LAST-1 of a length-L line (NS = product of the radices before S).
+template <int L, int P, int PAD, int S, int LAST>
+struct ForwardStages {
+  static __device__ __forceinline__ void run(float2* buf, int stride, int lane, const float2* tw, bool active) {
+    if constexpr (S < LAST) {
+      stockham_stage<L, radix_of(L, S), radix_product(L, S), -1, P, PAD, S>(buf, stride, lane, tw, active, nullptr);
+      ForwardStages<L, P, PAD, S + 1, LAST>::run(buf, stride, lane, tw, active);
+    }
+  }
+};
+// Inverse stages with the forward radices taken in reverse order, from forward stage S down to 0
+// (NS = product of the radices already applied).  A mixed-radix transform may take its radices in
+// any order; this one starts with the forward plan's last radix.
+template <int L, int P, int PAD, int S, int NS>
+struct InverseStagesReversed {
+  static __device__ __forceinline__ void run(float2* buf, int stride, int lane, const float2* tw, bool active) {
+    if constexpr (S >= 0) {
+      stockham_stage<L, radix_of(L, S), NS, 1, P, PAD, S>(buf, stride, lane, tw, active, nullptr);
+      InverseStagesReversed<L, P, PAD, S - 1, NS * radix_of(L, S)>::run(buf, stride, lane, tw, active);
+    }
+  }
+};
+template <int L, int P, int PAD, int NS>
+struct InverseStagesReversed<L, P, PAD, -1, NS> {
+  static __device__ __forceinline__ void run(float2*, int, int, const float2*, bool) {}
+};
+
+// Forward transform, elementwise product, inverse transform of one line, with the product formed in
+// registers.  The forward transform's stages but the last run in shared memory; its last stage
+// (radix RL, NS = L / RL) leaves lane j of the team holding, for each of its butterflies
+// j' = j + b P, the elements z = j' + (L / RL) r -- the elements the inverse transform's first stage
+// needs when the inverse takes the radices in reverse order (radix RL first, NB = L / RL).  So
+// mul(z, X(z)) -> Y(z) is applied to those registers, the inverse's first stage runs on them and its
+// remaining stages in shared memory: two shared-memory passes over the line fewer than
+// fft_line(-1), a separate product and fft_line(+1).  Element i of the line lives at
+// buf[lpos<PAD>(i) * stride]; the result (unnormalised) is left there in natural order.
+template <int L, int P, int PAD, class Mul>
+__device__ __forceinline__ void fft_line_fwd_mul_inv(float2* buf, int stride, int lane, const float2* tw, bool active,
+                                                     Mul&& mul) {
+  constexpr int LAST = n_stages(L) - 1;
+  constexpr int RL = radix_of(L, LAST), NSL = L / RL, PER = (NSL + P - 1) / P;
+  ForwardStages<L, P, PAD, 0, LAST>::run(buf, stride, lane, tw, active);
+  float2 v[PER][RL];
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int j = lane + b * P;
+    if (active && (PER * P == NSL || j < NSL)) {
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[b][r] = buf[lpos<PAD>(j + r * NSL) * stride];
+      if constexpr (LAST > 0) {
+#pragma unroll
+        for (int r = 1; r < RL; ++r) v[b][r] = cmul(v[b][r], twiddle<-1>(tw, (r * j) % L));
+      }
+      Dft<RL, -1>::run(v[b]);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[b][r] = mul(j + NSL * r, v[b][r]);
+      Dft<RL, 1>::run(v[b]);
+    }
+  }
+  __syncwarp();  // every lane has read the line before any writes it
+#pragma unroll
+  for (int b = 0; b < PER; ++b) {
+    const int j = lane + b * P;
+    if (active && (PER * P == NSL || j < NSL)) {
+#pragma unroll
+      for (int r = 0; r < RL; ++r) buf[lpos<PAD>(j * RL + r) * stride] = v[b][r];
+    }
+  }
+  __syncwarp();
+  InverseStagesReversed<L, P, PAD, LAST - 1, RL>::run(buf, stride, lane, tw, active);
+}
+
 // Loads the length-L twiddle table into shared memory (cooperatively, whole block).
 template <int L>
 __device__ __forceinline__ void load_twiddles(float2* s_tw, const float2* g_tw) {

@@ -2,11 +2,13 @@
 //
 // Data flow per evaluation e (box n, half width nh = n/2+1, peak radius r, window w = 2r+1):
 //   pass A  (CTA = G z-planes)   gather r = mask .* I(M (p - c - t) + c)  -> smem
-//                                FP64 sums of r and r^2 (DC-free energy by Parseval)
+//                                (no weight on the reference: FP64 sums of r and r^2, the
+//                                DC-free energy by Parseval)
 //                                R2C along x (two rows per complex FFT), FFT along y
 //                                -> S1[e][z][y][kx]                         (n * n * nh c64)
 //   pass B  (CTA = one ky row)   FFT along z, X = Q .* conj(wref .* R) .* wdgMask, X(0) = 0,
-//                                E_R = sum |wref .* R .* wdgMask|^2 when either weight is set,
+//                                E_R = sum |wref .* R .* wdgMask|^2 when either weight is set
+//                                (formed in registers between the transforms, zline_fused),
 //                                inverse FFT along z, keep the w output planes |sz| <= r
 //                                -> S2[e][j][ky][kx]                        (w * n * nh c64)
 //   pass C  (CTA = one sz plane) inverse FFT along y, C2R along x for the w rows |sy| <= r,
@@ -258,10 +260,9 @@ struct SearchCfg {
   // Pass B: a CTA transforms the z lines of one ky and one of KS_B parts of the kx columns (NHB
   // columns at most, tile pitch TPB odd so the spread of lines over banks stays a permutation).
   // It prefetches its particle-spectrum and weight slabs into shared memory (64^3: four CTAs per
-  // SM; 96^3: the prefetch also frees the registers that held them, 68 instead of 105, so two
-  // CTAs fit instead of one).  128^3 splits the columns in two: with the whole ky row a CTA needed
-  // 544 threads and 95 registers (one CTA per SM, latency-bound); half rows fit two per SM.
-  static constexpr bool PREF_B = true;
+  // SM; 96^3: the prefetch also frees the registers that held them, so two CTAs fit instead of
+  // one).  128^3 splits the columns in two: with the whole ky row a CTA needed 544 threads and 95
+  // registers (one CTA per SM, latency-bound); half rows fit two per SM.
   static constexpr int KS_B = N >= 128 ? 2 : 1;
   static constexpr int NHB = (NH + KS_B - 1) / KS_B;
   static constexpr int TPB = NHB | 1;
@@ -269,61 +270,32 @@ struct SearchCfg {
   static constexpr int TEAMS_B = NT_B / P;
   static constexpr int GRID_BX = N * KS_B;
   static constexpr size_t SMEM_B =
-      sizeof(float2) * ((size_t)PY * TPB + N) + (PREF_B ? (sizeof(float2) + sizeof(float)) * (size_t)N * NHB : 0);
+      sizeof(float2) * ((size_t)PY * TPB + N) + (sizeof(float2) + sizeof(float)) * (size_t)N * NHB;
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
-  // Pass B keeps the product between the two z transforms in registers when a line is two equal
-  // radix-R stages with one butterfly per lane (N = R^2, team of R lanes): the forward transform's
-  // last stage leaves lane j holding elements j + R r, exactly the inputs the inverse transform's
-  // first stage gives it (64 = 8 x 8).
-  static constexpr bool FUSE_B = radix_of(N, 0) == radix_of(N, 1) && radix_of(N, 2) == 1 &&
-                                 radix_of(N, 0) * radix_of(N, 0) == N && P == radix_of(N, 0);
 };
 
-// Pass B's z line of local column kl for FUSE_B sizes: forward stage 1 in shared memory; forward
-// stage 2 into registers; there, element z = j + R r is weighted (wdgMask and wref, prefetched into
-// s_w), its |.|^2 added to E_R, multiplied into Q conj(R) (0 at the origin); the inverse stage 1 runs
-// on the same registers and inverse stage 2 in shared memory.  Same arithmetic as the separate
-// transforms and multiply loop, two shared-memory passes over the line fewer.
+// Pass B's z line of local column kl (fft_line_fwd_mul_inv): between the forward and the inverse
+// transform, in registers, element z is weighted (wdgMask and wref, prefetched into s_w), its
+// |.|^2 added to E_R and multiplied into Q conj(R) (0 at the origin).
 template <int N>
 __device__ __forceinline__ void zline_fused(float2* buf, int stride, int lane, const float2* tw, bool active, int kl,
                                             int kx, int ky, const float2* s_q, const float* s_w, bool weighted,
                                             double& en) {
   using C = SearchCfg<N>;
-  constexpr int R = radix_of(N, 0), P = C::P, NB = C::NHB;
-  stockham_stage<N, R, 1, -1, P, 1, 0>(buf, stride, lane, tw, active, nullptr);
-  float2 v[R];
-  const int j = lane;
-  if (active) {
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = buf[lpos<1>(j + r * R) * stride];
-#pragma unroll
-    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle<-1>(tw, (r * j) % N));
-    Dft<R, -1>::run(v);
-    const double hw = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int z = j + R * r, i = z * NB + kl;
-      const bool origin = z == 0 && ky == 0 && kx == 0;
-      float2 rr = v[r];
-      if (weighted) {
-        const float wv = s_w[i];
-        rr.x *= wv;
-        rr.y *= wv;
-        if (!origin) en += hw * ((double)rr.x * rr.x + (double)rr.y * rr.y);
-      }
-      float2 x = cmulc(s_q[i], rr);
-      if (origin) x = make_float2(0.f, 0.f);
-      v[r] = x;
+  constexpr int NB = C::NHB;
+  const double hw = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
+  fft_line_fwd_mul_inv<N, C::P, 1>(buf, stride, lane, tw, active, [&](int z, float2 rr) {
+    const int i = z * NB + kl;
+    const bool origin = z == 0 && ky == 0 && kx == 0;
+    if (weighted) {
+      const float wv = s_w[i];
+      rr.x *= wv;
+      rr.y *= wv;
+      if (!origin) en += hw * ((double)rr.x * rr.x + (double)rr.y * rr.y);
     }
-    Dft<R, 1>::run(v);
-  }
-  __syncwarp();  // every lane has read the line before any writes it
-  if (active) {
-#pragma unroll
-    for (int r = 0; r < R; ++r) buf[lpos<1>(j * R + r) * stride] = v[r];
-  }
-  __syncwarp();
-  stockham_stage<N, R, R, 1, P, 1, 1>(buf, stride, lane, tw, active, nullptr);
+    const float2 x = cmulc(s_q[i], rr);
+    return origin ? make_float2(0.f, 0.f) : x;
+  });
 }
 
 // Line li of a strided-FFT round handled by team `team`: consecutive teams get kx values 8
@@ -607,7 +579,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_
   const DevParticle& pt = a.parts[it.particle];
   // weights on the rotated reference: the reference's bandpass wref and the particle's wdgMask
   // (BH_multi_xcf_Translational_2.m:35-38).  The first present one (the wedge when both are) is
-  // prefetched into shared memory with the spectrum; a second one is read at use.
+  // prefetched into shared memory with the spectrum; a second one is folded into that copy.
   const float* __restrict__ wref = a.refs[pt.ref].wref;
   const float* __restrict__ w1 = pt.wedge ? pt.wedge : wref;
   const float* __restrict__ w2 = pt.wedge ? wref : nullptr;
@@ -615,22 +587,20 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_
   const int w = 2 * a.radius + 1;
   constexpr int IT = (N * NB + NT - 1) / NT;
 
-  // (PREF_B) this thread's elements i of the particle spectrum and of the first weight,
-  // copied asynchronously while the slab loads and the forward transform run
+  // this thread's elements i of the particle spectrum and of the first weight, copied
+  // asynchronously while the slab loads run
   float2* s_q = s_tw + N;                                     // [N * NHB]
   float* s_w = reinterpret_cast<float*>(s_q + N * C::NHB);    // [N * NHB]
-  if constexpr (C::PREF_B) {
 #pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * NT;
-      if (i < N * NB && i % NB < cnt) {
-        const size_t gi = ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB;
-        cp_async8(s_q + i, q + gi);
-        if (w1) cp_async4(s_w + i, w1 + gi);
-      }
+  for (int k = 0; k < IT; ++k) {
+    const int i = threadIdx.x + k * NT;
+    if (i < N * NB && i % NB < cnt) {
+      const size_t gi = ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB;
+      cp_async8(s_q + i, q + gi);
+      if (w1) cp_async4(s_w + i, w1 + gi);
     }
-    cp_async_commit();
   }
+  cp_async_commit();
   load_twiddles<N>(s_tw, g_tw);
   const float2* src = a.s1 + (size_t)e * N * N * NH + (size_t)ky * NH + k0;
   {
@@ -648,97 +618,26 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_
     }
   }
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
-  if constexpr (C::FUSE_B) {
-    // the prefetched slabs are read by other threads' lines: wait for this thread's copies (and fold
-    // a second weight into them), then the barrier publishes everyone's
-    cp_async_wait<0>();
-    if (w2) {
+  // the prefetched slabs are read by other threads' lines: wait for this thread's copies (and fold
+  // a second weight into them), then the barrier publishes everyone's
+  cp_async_wait<0>();
+  if (w2) {
 #pragma unroll 1
-      for (int k = 0; k < IT; ++k) {
-        const int i = threadIdx.x + k * NT;
-        if (i < N * NB && i % NB < cnt) s_w[i] *= __ldg(w2 + ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB);
-      }
+    for (int k = 0; k < IT; ++k) {
+      const int i = threadIdx.x + k * NT;
+      if (i < N * NB && i % NB < cnt) s_w[i] *= __ldg(w2 + ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB);
     }
-    __syncthreads();
-    double en = 0.0;
-    for (int base = 0; base < TPB; base += C::TEAMS_B) {
-      const int li = base + team;
-      const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
-      zline_fused<N>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt, kl, k0 + kl, ky, s_q, s_w, w1 != nullptr, en);
-    }
-    if (w1) {
-      double t = block_sum(en, red);
-      if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
-    }
-    __syncthreads();
-    float2* dst = a.s2 + (size_t)e * w * N * NH + (size_t)ky * NH + k0;
-    for (int i = threadIdx.x; i < w * NB; i += NT) {
-      const int j = i / NB, kl = i % NB;
-      if (kl >= cnt) continue;
-      const int z = (j - a.radius + N) % N;
-      dst[(size_t)j * N * NH + kl] = tile[lpos<1>(z) * TPB + kl];
-    }
-    return;
-  }
-  __syncthreads();
-  // lines li in [0, TPB) -> local column (8 li) mod TPB (a permutation: TPB is odd), which puts the
-  // teams of a warp on different banks; columns >= cnt are idle
-  for (int base = 0; base < TPB; base += C::TEAMS_B) {
-    const int li = base + team;
-    const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
-    fft_line<N, -1, P, 1>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt);
   }
   __syncthreads();
   double en = 0.0;
-  {
-    float2 qv[C::PREF_B ? 1 : IT];
-    if constexpr (C::PREF_B) {
-      cp_async_wait<0>();  // this thread's own copies; no other thread reads them
-      if (w2) {
-        // both weights: fold the second into this thread's prefetched elements (a separate loop,
-        // so its loads do not hold registers across the multiply below)
-#pragma unroll 1
-        for (int k = 0; k < IT; ++k) {
-          const int i = threadIdx.x + k * NT;
-          if (i < N * NB && i % NB < cnt) s_w[i] *= __ldg(w2 + ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < IT; ++k) {
-        const int i = threadIdx.x + k * NT;
-        if (i < N * NB && i % NB < cnt) qv[k] = __ldg(q + ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * NT;
-      if (i >= N * NB || i % NB >= cnt) continue;
-      const int z = i / NB, kl = i % NB, kx = k0 + kl;
-      const size_t gi = ((size_t)z * N + ky) * NH + kx;
-      float2& slot = tile[lpos<1>(z) * TPB + kl];
-      float2 r = slot;
-      if (w1) {
-        float wv = C::PREF_B ? s_w[i] : __ldg(w1 + gi);
-        if (!C::PREF_B && w2) wv *= __ldg(w2 + gi);
-        r.x *= wv;
-        r.y *= wv;
-        if (gi != 0) en += (kx == 0 || 2 * kx == N ? 1.0 : 2.0) * ((double)r.x * r.x + (double)r.y * r.y);
-      }
-      float2 x = cmulc(C::PREF_B ? s_q[i] : qv[C::PREF_B ? 0 : k], r);
-      if (gi == 0) x = make_float2(0.f, 0.f);
-      slot = x;
-    }
+  for (int base = 0; base < TPB; base += C::TEAMS_B) {
+    const int li = base + team;
+    const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
+    zline_fused<N>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt, kl, k0 + kl, ky, s_q, s_w, w1 != nullptr, en);
   }
   if (w1) {
     double t = block_sum(en, red);
     if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
-  }
-  __syncthreads();
-  for (int base = 0; base < TPB; base += C::TEAMS_B) {
-    const int li = base + team;
-    const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
-    fft_line<N, 1, P, 1>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt);
   }
   __syncthreads();
   float2* dst = a.s2 + (size_t)e * w * N * NH + (size_t)ky * NH + k0;

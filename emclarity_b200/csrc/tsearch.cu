@@ -101,7 +101,8 @@ __global__ void __launch_bounds__(256) k_ts_rows(const float* __restrict__ tmpl,
 
 // Per tile of TT consecutive (ky, kx) z-lines: G = FFT_z of the t planes at z = pl[2].. (zeros
 // elsewhere), X = T .* conj(G), inverse FFT_z into s.  stats[0] += sum over the full spectrum of
-// |X|^2 (Hermitian weights), stats[1] = X(0).
+// |X|^2 (Hermitian weights), stats[1] = X(0).  The product and statistics are formed in registers
+// between the two transforms (fft_line_fwd_mul_inv).
 // Resident CTAs per SM asked of the compiler: 20 warps' worth when a lane holds at most 16 complex
 // values per stage (the register cap then leaves room for them), else no constraint.
 constexpr int zfused_min_blocks(int L, int P, int TT) {
@@ -113,10 +114,11 @@ __global__ void __launch_bounds__(P * TT, zfused_min_blocks(L, P, TT)) k_ts_zfus
                                                       float2* __restrict__ s, const TsGeom g,
                                                       double* __restrict__ stats, const float2* __restrict__ g_tw) {
   extern __shared__ float2 smem[];
-  float2* s_tw = smem;
-  float2* tile = smem + L;  // [padded L][TT+1], element n of line t at lpos<PAD>(n) * TP + t
   constexpr int TP = TT + 1;
   constexpr int PAD = line_pad(L);
+  float2* s_tw = smem;
+  float2* tile = smem + L;                                // [padded L][TP], element n of line t at lpos<PAD>(n) * TP + t
+  float2* s_t = tile + (size_t)padded_len(L, PAD) * TP;  // [L][TT], the tomogram spectrum of the tile's lines
   static_assert((P * TT) % 32 == 0, "the statistics reduction needs whole warps");
   __shared__ double red[32];
   load_twiddles<L>(s_tw, g_tw);
@@ -124,6 +126,14 @@ __global__ void __launch_bounds__(P * TT, zfused_min_blocks(L, P, TT)) k_ts_zfus
   const long i0 = (long)blockIdx.x * TT;
   constexpr int NT = P * TT;
   constexpr int IT = (L * TT + NT - 1) / NT;
+  // the tomogram spectrum of this tile, copied asynchronously while the template planes load
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    const int idx = threadIdx.x + k * NT;
+    const int n = idx / TT, t = idx % TT;
+    if (idx < L * TT && i0 + t < inner) cp_async8(s_t + idx, T + (long)n * stride + i0 + t);
+  }
+  cp_async_commit();
   {
     float2 v[IT];
 #pragma unroll
@@ -140,32 +150,21 @@ __global__ void __launch_bounds__(P * TT, zfused_min_blocks(L, P, TT)) k_ts_zfus
       if (idx < L * TT) tile[lpos<PAD>(idx / TT) * TP + idx % TT] = v[k];
     }
   }
-  // the tomogram spectrum of this tile, fetched while the forward transform runs
-  float2 tv[IT];
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    const int idx = threadIdx.x + k * NT;
-    const int n = idx / TT, t = idx % TT;
-    tv[k] = (idx < L * TT && i0 + t < inner) ? __ldg(T + (long)n * stride + i0 + t) : make_float2(0.f, 0.f);
-  }
+  cp_async_wait<0>();
   __syncthreads();
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
-  const bool line_active = i0 + team < inner;
-  fft_line<L, -1, P, PAD>(tile + team, TP, lane, s_tw, line_active);
-  __syncthreads();
+  const long i = i0 + team;
+  const bool line_active = i < inner;
+  const double hw = ((int)(i % g.nxh) == 0 || 2 * (int)(i % g.nxh) == g.nx) ? 1.0 : 2.0;
+  // forward z transform of the template planes, X = T .* conj(G) and its statistics in registers,
+  // inverse z transform (fft_line_fwd_mul_inv)
   double e = 0.0;
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    const int idx = threadIdx.x + k * NT;
-    const int n = idx / TT, t = idx % TT;
-    const long i = i0 + t;
-    if (idx >= L * TT || i >= inner) continue;
-    const float2 x = cmulc(tv[k], tile[lpos<PAD>(n) * TP + t]);
-    tile[lpos<PAD>(n) * TP + t] = x;
-    const int kx = (int)(i % g.nxh);
-    e += (kx == 0 || 2 * kx == g.nx ? 1.0 : 2.0) * ((double)x.x * x.x + (double)x.y * x.y);
+  fft_line_fwd_mul_inv<L, P, PAD>(tile + team, TP, lane, s_tw, line_active, [&](int n, float2 gz) {
+    const float2 x = cmulc(s_t[n * TT + team], gz);
+    e += hw * ((double)x.x * x.x + (double)x.y * x.y);
     if (i == 0 && n == 0) stats[1] = (double)x.x;
-  }
+    return x;
+  });
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
@@ -175,12 +174,9 @@ __global__ void __launch_bounds__(P * TT, zfused_min_blocks(L, P, TT)) k_ts_zfus
     for (int w = 0; w < NT / 32; ++w) tot += red[w];
     atomicAdd(stats, tot);
   }
-  fft_line<L, 1, P, PAD>(tile + team, TP, lane, s_tw, line_active);
-  __syncthreads();
   for (int idx = threadIdx.x; idx < L * TT; idx += NT) {
     const int n = idx / TT, t = idx % TT;
-    const long i = i0 + t;
-    if (i < inner) s[(long)n * stride + i] = tile[lpos<PAD>(n) * TP + t];
+    if (i0 + t < inner) s[(long)n * stride + i0 + t] = tile[lpos<PAD>(n) * TP + t];
   }
 }
 
@@ -366,7 +362,7 @@ static emc_status launch_ts_zfused(const float2* gt, const float2* T, float2* s,
   // resident per SM, so one CTA's loads overlap another's transforms.
   constexpr int TT = C::P >= 4 ? 8 : 32 / C::P;
   auto kern = k_ts_zfused<L, C::P, TT>;
-  constexpr size_t smem = sizeof(float2) * (L + (size_t)padded_len(L, line_pad(L)) * (TT + 1));
+  constexpr size_t smem = sizeof(float2) * (L + (size_t)padded_len(L, line_pad(L)) * (TT + 1) + (size_t)L * TT);
   static bool attr_set[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
