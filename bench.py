@@ -187,7 +187,7 @@ def run_ours(args, world, rank, local):
     from emclarity_b200 import api
     n = args.particles
     b = build_batch(1000 + rank, n)
-    s = api.Search(peak_radius=PEAK_RADIUS)
+    s = api.Search(peak_radius=PEAK_RADIUS, chunk_evals=args.chunk)
     if args.planes:
         s.set_planes(BOX, args.planes)
     if args.overlap:
@@ -321,7 +321,7 @@ def run_ours(args, world, rank, local):
                                (n, N_ORIENT, PEAK_RADIUS),
                    "box": BOX, "particles_per_gpu": n, "orientations": N_ORIENT, "evals_per_step_per_gpu": evals,
                    "l2": "inputs larger than L2 (%.2f GB of particle spectra per GPU)" % (spec.numel() * 8 / 1e9),
-                   "chunk_overlap_slots": args.overlap or 2,
+                   "chunk_overlap_slots": args.overlap or 2, "chunk_evals": args.chunk or "library default",
                    "parallelism": "replicas%d" % world},
         "e2e": {"value": world * evals / (e2e_ms / 1e3), "unit": "CC evals/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h),
@@ -1156,6 +1156,7 @@ def main():
                     help="skip the batched-uneven (FP32, BF16) and refinement keys of the default line")
     ap.add_argument("--planes", type=int, default=0, help="pass-A z-planes per CTA (0: timed choice)")
     ap.add_argument("--overlap", type=int, default=0, help="chunk scratch slots (0: the library default, 2)")
+    ap.add_argument("--chunk", type=int, default=0, help="evaluations per chunk (0: the library default)")
     ap.add_argument("--workload", default="batched64", choices=["batched64", "mixed", "bf16", "tsearch", "refine", "average", "formats",
                                                                     "tsearch_post"])
     args = ap.parse_args()
