@@ -105,6 +105,8 @@ SIGNATURES = {
     "emc_search_set_planes": (_i, [_vp, _i, _i]),
     "emc_search_get_planes": (_i, [_vp, _i, _i, _pi, _pf]),
     "emc_search_set_overlap": (_i, [_vp, _i]),
+    "emc_search_status": (_i, [_vp, _vp]),
+    "emc_search_test_wait": (_i, [_vp, C.c_longlong, C.c_uint]),
     "emc_search_plain_noalloc": (_i, [_vp, _vp, _i, _vp, _d, _pd, _pf, _pd, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "emc_cc_adjoint_batch": (_i, [_vp, _i, _pi, C.POINTER(_vp), _pd, _pd, _pd, _i, _pd, _pd, _vp]),
     "emc_cc_adjoint": (_i, [_vp, _i, _vp, _d, _pd, _pd, _i, _pd, _pd, _vp]),

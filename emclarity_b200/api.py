@@ -410,8 +410,19 @@ class Search:
         L.call("emc_search_set_planes", self._h, int(box), int(planes))
 
     def set_overlap(self, slots):
-        """Chunk scratch slots of recorded runs: 2 (default) runs consecutive chunks concurrently, 1 in order."""
+        """Chunk scratch slots of recorded runs: 2 (default) runs consecutive chunks of boxes below 128
+        concurrently, 1 in order."""
         L.call("emc_search_set_overlap", self._h, int(slots))
+
+    def status(self):
+        """Synchronises the current stream; raises EmcError (EMC_E_TIMEOUT) if a device-side wait of a
+        run since the last check gave up (those runs' results are invalid)."""
+        L.call("emc_search_status", self._h, _stream())
+
+    def test_wait(self, wait_cycles=1 << 31, phantom_bytes=0):
+        """Test hook: bound later runs' device-side waits at wait_cycles SM cycles and announce
+        phantom_bytes more bytes than they copy (> 0 makes every such wait run out)."""
+        L.call("emc_search_test_wait", self._h, int(wait_cycles), int(phantom_bytes))
 
     def planes(self, box, dtype="f32"):
         """(planes in use, {planes option: pass-A ms per launch at tuning}) for (box, dtype); 0 = not tuned yet."""

@@ -233,7 +233,7 @@ static emc_status set_attrs_any(int n, int dtype) {
 
 static size_t per_eval_scratch(int n, int radius) {
   const size_t nh = n / 2 + 1;
-  return sizeof(float2) * nh * n * (n + (size_t)(2 * radius + 1));
+  return sizeof(float2) * (s1_eval_elems(n) + nh * n * (size_t)(2 * radius + 1));
 }
 
 // Device buffer that grows on demand.
@@ -337,6 +337,11 @@ struct emc_search_s {
   RunTables* cur = nullptr;        // tables of the run being recorded or launched eagerly
   emc::DevBuf<emc::EvalResult> d_results;
   emc::DevBuf<unsigned long long> d_best_keys;
+  // device status word of bounded waits (emc::kStatusWaitTimeout), read and cleared by
+  // emc_search_status and emc_search_run_host; the wait limit and the test hook's phantom bytes
+  emc::DevBuf<unsigned> d_status;
+  long long wait_cycles = 1ll << 31;
+  unsigned phantom_tx = 0;
   // Per-evaluation scratch of a chunk, one set per overlap slot: chunk i of a recorded run uses slot
   // i % overlap and its own branch of the graph, so consecutive chunks run concurrently (pass A of one
   // beside passes B and C of the other, filling each other's tails) while chunks of one slot stay in order.
@@ -417,6 +422,11 @@ emc_status emc_search_create(emc_search_t* out) {
       s->scratch_budget = std::max<size_t>(free_b / 8, 16ull << 20);
   }
   s->graphs.reserve(emc_search_s::kGraphCache);
+  if (s->d_status.reserve(1) != EMC_OK || cudaMemset(s->d_status.p, 0, sizeof(unsigned)) != cudaSuccess) {
+    delete s;
+    emc::set_error("emc_search_create: status word allocation failed");
+    return EMC_E_OOM;
+  }
   if (cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->branch, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
@@ -539,7 +549,20 @@ static emc::SearchChunkArgs chunk_args(emc_search_t s, const Chunk& c, int slot 
   a.done = sc.done.p;
   a.results = s->d_results.p;
   a.best_keys = s->d_best_keys.p;
+  a.status = s->d_status.p;
+  a.wait_cycles = s->wait_cycles;
+  a.phantom_tx = s->phantom_tx;
   return a;
+}
+
+// Reads and clears the status word (the stream synchronised by the caller).
+static emc_status take_status(emc_search_t s) {
+  unsigned v = 0;
+  EMC_CUDA(cudaMemcpy(&v, s->d_status.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (!v) return EMC_OK;
+  EMC_CUDA(cudaMemset(s->d_status.p, 0, sizeof(unsigned)));
+  emc::set_error("search: a device-side wait for bulk copies gave up; that run's results are invalid");
+  return EMC_E_TIMEOUT;
 }
 
 static int& planes_slot(emc_search_t s, int n, int dtype) {
@@ -606,15 +629,26 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
     EMC_LAUNCH_CHECK();
     ++launches;
   }
-  // the second branch forks from the stream after the set-up above and joins before the outputs
+  // The second branch forks from the stream after the set-up above and joins before the outputs.
+  // Chunks of boxes of 128 and above run alone on the stream (the branch joined first): their
+  // passes fill the SMs by themselves, and beside another chunk's they ran slower (128^3: 40.2k
+  // evaluations/s with two slots against 44.9k with one).
   const bool two = nslots > 1 && chunks.size() > 1;
-  if (two) {
-    EMC_CUDA(cudaEventRecord(s->fork_ev, st));
-    EMC_CUDA(cudaStreamWaitEvent(s->branch, s->fork_ev, 0));
-  }
+  bool forked = false;
+  long alternate = 0;
   for (size_t ci = 0; ci < chunks.size(); ++ci) {
     const Chunk& c = chunks[ci];
-    const int slot = two ? (int)(ci % 2) : 0;
+    const bool overlapped = two && c.n < 128;
+    if (overlapped && !forked) {
+      EMC_CUDA(cudaEventRecord(s->fork_ev, st));
+      EMC_CUDA(cudaStreamWaitEvent(s->branch, s->fork_ev, 0));
+      forked = true;
+    } else if (!overlapped && forked) {
+      EMC_CUDA(cudaEventRecord(s->join_ev, s->branch));
+      EMC_CUDA(cudaStreamWaitEvent(st, s->join_ev, 0));
+      forked = false;
+    }
+    const int slot = overlapped ? (int)(alternate++ % 2) : 0;
     const cudaStream_t cst = slot ? s->branch : st;
     const emc::SearchChunkArgs a = chunk_args(s, c, slot);
     cudaEvent_t* ev = nullptr;
@@ -633,7 +667,7 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
       s->prof_evals += c.count;
     }
   }
-  if (two) {
+  if (forked) {
     EMC_CUDA(cudaEventRecord(s->join_ev, s->branch));
     EMC_CUDA(cudaStreamWaitEvent(st, s->join_ev, 0));
   }
@@ -756,7 +790,7 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
     for (const Chunk& c : chunks) {
       const size_t nh = c.n / 2 + 1;
       const int r = effective_radius(s, c.n);
-      s1n = std::max(s1n, (size_t)c.count * c.n * c.n * nh);
+      s1n = std::max(s1n, (size_t)c.count * emc::s1_eval_elems(c.n));
       s2n = std::max(s2n, (size_t)c.count * (2 * r + 1) * c.n * nh);
     }
     for (int k = 0; k < nslots; ++k) {
@@ -884,12 +918,30 @@ emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particle
   if (rs == EMC_OK && cudaStreamSynchronize(st) != cudaSuccess) rs = EMC_E_CUDA;
   if (rs == EMC_E_OOM) emc::set_error("emc_search_run_host: device allocation failed");
   if (rs == EMC_E_CUDA) emc::set_error("emc_search_run_host: copy back failed");
+  if (rs == EMC_OK) rs = take_status(s);
   cudaFree(d_cc);
   cudaFree(d_peak);
   cudaFree(d_best);
   // the graph was recorded with these temporary outputs: do not replay it
   drop_graphs(s);
   return rs;
+}
+
+emc_status emc_search_status(emc_search_t s, void* stream) {
+  EMC_CHECK_ARG(s, "emc_search_status: null handle");
+  EMC_CUDA(cudaStreamSynchronize(emc::as_stream(stream)));
+  return take_status(s);
+}
+
+emc_status emc_search_test_wait(emc_search_t s, long long wait_cycles, unsigned phantom_bytes) {
+  EMC_CHECK_ARG(s, "emc_search_test_wait: null handle");
+  EMC_CHECK_ARG(wait_cycles > 0 && phantom_bytes % 16 == 0 && phantom_bytes <= 4096,
+                "emc_search_test_wait: wait_cycles %lld > 0, phantom_bytes %u a multiple of 16 up to 4096",
+                wait_cycles, phantom_bytes);
+  s->wait_cycles = wait_cycles;
+  s->phantom_tx = phantom_bytes;
+  drop_graphs(s);  // recorded graphs hold the old values
+  return EMC_OK;
 }
 
 emc_status emc_search_set_profiling(emc_search_t s, int enable) {

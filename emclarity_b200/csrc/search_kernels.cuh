@@ -189,7 +189,13 @@ struct SearchChunkArgs {
   unsigned* done = nullptr;                  // [E] pass-C CTAs finished
   EvalResult* results = nullptr;             // [total evaluations of the run]
   unsigned long long* best_keys = nullptr;   // [particles]
+  // Bounded device-side waits: a wait that gives up after wait_cycles SM clock cycles ORs
+  // kStatusWaitTimeout into *status (when set) and its CTA returns without a result.
+  unsigned* status = nullptr;
+  long long wait_cycles = 1ll << 31;         // about a second at the B200's 1.965 GHz
+  unsigned phantom_tx = 0;                   // test hook: bytes announced but never copied (0)
 };
+constexpr unsigned kStatusWaitTimeout = 1u;
 
 // Decodes evaluation e of a chunk from its peak key and folds it into its particle's
 // best-orientation key (cc, then the first orientation on ties).
@@ -239,7 +245,13 @@ struct SearchCfg {
   static constexpr int G = GG ? GG : default_planes(N);  // planes per pass-A CTA
   static constexpr int NT_A = 256;
   static constexpr int TEAMS_A = NT_A / P;
-  static constexpr int NT_BC = ((NH * P + 31) / 32) * 32;
+  // Pass C uses half as many teams as the y transforms have lines (two rounds of y lines), so
+  // that the C2R phase, where (2 r + 1 + 1) / 2 row pairs (8 at r = 7) keep as many teams busy,
+  // leaves fewer idle and more CTAs fit per SM: 64^3 20 teams of 8 lanes, six CTAs per SM at 64
+  // registers (88.7 us per 602-evaluation chunk against 131.1 with 33 teams); 96^3 28 teams and
+  // 128^3 36, where the whole-row CTAs (416 and 544 threads) fitted once per SM by registers
+  static constexpr int NT_BC = ((NH * P / 2 + 31) / 32) * 32;
+  static constexpr int MINB_C = N <= 64 ? 6 : 2;
   static constexpr int TEAMS_BC = NT_BC / P;
   // FFT lines use padded positions (lpos<1>): a strided line of N elements spans PY rows, a
   // contiguous line buffer LP slots; LP = 8 (mod 16) puts neighbouring teams 16 banks apart.
@@ -249,6 +261,7 @@ struct SearchCfg {
   // idle during those loops, which keeps two pass-A CTAs per SM for every box size
   static constexpr int TEAMS_LA = N <= 64 ? TEAMS_A : 16;
   static constexpr int TEAMS_LC = 16;  // (2 r + 1 + 1) / 2 <= 16 row pairs for r <= 15
+  static_assert(TEAMS_BC >= TEAMS_LC, "pass C needs a team for every line buffer");
   static constexpr size_t SMEM_A = sizeof(float2) * ((size_t)G * PY * NH + (size_t)TEAMS_LA * LP + N) + 64;
   // resident pass-A CTAs per SM that shared memory allows (228 KB per SM, 1 KB reserved per CTA),
   // and the target the register budget is capped for: 5 at 64^3 with one plane per CTA (48
@@ -269,26 +282,57 @@ struct SearchCfg {
   static constexpr int NT_B = ((NHB * P + 31) / 32) * 32;
   static constexpr int TEAMS_B = NT_B / P;
   static constexpr int GRID_BX = N * KS_B;
+  // The weight slab is prefetched too up to 96^3; at 128^3 it is read from L2 when the product is
+  // formed, so that three CTAs per SM fit in shared memory instead of two.
+  static constexpr bool PREF_W = N <= 96;
+  // 64^3: pass A writes S1 as pass B's shared-memory tiles -- per (evaluation, ky) a slab of PY rows
+  // (row z at lpos<1>(z)) of TPB_K float2 -- which pass B fetches with one bulk copy.  The particle
+  // spectrum and weight rows (the caller's layout) come in 16-byte cp.async pieces from the 16-byte
+  // boundary at or below each row start, into rows of even pitch (QP_K float2, WP_K floats), and are
+  // read at the row's offset from that boundary (the same for every row of a CTA: a z step is N NH
+  // elements, a multiple of 16 bytes).  The teams of a warp take consecutive columns: with the even
+  // tile pitch the two teams of a half-warp then fall on complementary banks in every stage, and the
+  // four of a warp read the weight rows (pitch 36) on disjoint banks.
+  static constexpr bool BULK_B = N == 64;
+  static constexpr int TPB_K = NHB + 1 + (NHB + 1) % 2;                 // >= NHB + 1, even
+  static constexpr int QP_K = TPB_K;
+  static constexpr int WP_K = ((NHB + 3 + 3) / 4) * 4;                   // >= NHB + 3, 16-byte rows
+  // S1 elements per evaluation
+  static constexpr size_t S1_EVAL = BULK_B ? (size_t)N * PY * TPB_K : (size_t)N * N * NH;
   static constexpr size_t SMEM_B =
-      sizeof(float2) * ((size_t)PY * TPB + N) + (sizeof(float2) + sizeof(float)) * (size_t)N * NHB;
+      BULK_B ? sizeof(float2) * ((size_t)PY * TPB_K + (size_t)N * QP_K + N) + sizeof(float) * (size_t)N * WP_K
+             : sizeof(float2) * ((size_t)PY * TPB + N) +
+                   (sizeof(float2) + (PREF_W ? sizeof(float) : 0)) * (size_t)N * NHB;
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
 };
 
+// S1 elements per evaluation of box n (the 64^3 slabs are padded to the z pass's tiles).
+inline size_t s1_eval_elems(int n) {
+  return n == 64 ? SearchCfg<64>::S1_EVAL : n == 96 ? SearchCfg<96>::S1_EVAL : SearchCfg<128>::S1_EVAL;
+}
+
 // Pass B's z line of local column kl (fft_line_fwd_mul_inv): between the forward and the inverse
-// transform, in registers, element z is weighted (wdgMask and wref, prefetched into s_w), its
-// |.|^2 added to E_R and multiplied into Q conj(R) (0 at the origin).
+// transform, in registers, element z is weighted (wdgMask and wref: prefetched into s_w, or read from
+// w1 / w2 when PREF_W is off), its |.|^2 added to E_R and multiplied into Q conj(R) (0 at the origin).
 template <int N>
 __device__ __forceinline__ void zline_fused(float2* buf, int stride, int lane, const float2* tw, bool active, int kl,
                                             int kx, int ky, const float2* s_q, const float* s_w, bool weighted,
-                                            double& en) {
+                                            const float* w1, const float* w2, double& en) {
   using C = SearchCfg<N>;
-  constexpr int NB = C::NHB;
+  constexpr int NB = C::NHB, NH = C::NH;
   const double hw = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
   fft_line_fwd_mul_inv<N, C::P, 1>(buf, stride, lane, tw, active, [&](int z, float2 rr) {
     const int i = z * NB + kl;
     const bool origin = z == 0 && ky == 0 && kx == 0;
     if (weighted) {
-      const float wv = s_w[i];
+      float wv;
+      if constexpr (C::PREF_W) {
+        wv = s_w[i];
+      } else {
+        const size_t gi = ((size_t)z * N + ky) * NH + kx;
+        wv = __ldg(w1 + gi);
+        if (w2) wv *= __ldg(w2 + gi);
+      }
       rr.x *= wv;
       rr.y *= wv;
       if (!origin) en += hw * ((double)rr.x * rr.x + (double)rr.y * rr.y);
@@ -536,30 +580,44 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
   //    0 and N/2 are separated from the packed column 0: with Z = F(X(0) + i X(N/2)),
   //    F X(0)(y) = (Z(y) + conj Z(-y)) / 2 and F X(N/2)(y) = (Z(y) - conj Z(-y)) / 2i
   {
-    float2* dst = a.s1 + ((size_t)e * N + z0) * N * NH;
-    constexpr int NV = G * N * NH;
-    for (int i = threadIdx.x; i < NV; i += C::NT_A) {
-      const int row = i / NH, kx = i % NH;  // row = zl * N + y
-      const int zl = row / N, y = row % N;
+    // F X(kx)(y) of local plane zl: columns 0 and N/2 separated from the packed column 0
+    auto s1_value = [&](int zl, int y, int kx) {
       const float2* pl = planes + (size_t)zl * PY * NH;
-      float2 v;
+      if (kx >= NH) return make_float2(0.f, 0.f);
       if (kx == 0 || kx == NH - 1) {
         const float2 zp = pl[lpos<1>(y) * NH], zm = pl[lpos<1>((N - y) % N) * NH];
-        v = kx == 0 ? make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y))
-                    : make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
-      } else {
-        v = pl[lpos<1>(y) * NH + kx];
+        return kx == 0 ? make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y))
+                       : make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
       }
-      dst[i] = v;
+      return pl[lpos<1>(y) * NH + kx];
+    };
+    float2* dst = a.s1 + (size_t)e * C::S1_EVAL;
+    if constexpr (C::BULK_B) {
+      // slabs [ky][lpos(z)][TPB_K]: whole rows, pad columns zero, two elements per 16-byte store
+      constexpr int RP = C::TPB_K / 2;
+      constexpr int NV = G * N * RP;
+      for (int i = threadIdx.x; i < NV; i += C::NT_A) {
+        const int row = i / RP, c = i % RP;  // row = zl * N + y
+        const int zl = row / N, y = row % N;
+        const float2 v0 = s1_value(zl, y, 2 * c), v1 = s1_value(zl, y, 2 * c + 1);
+        *reinterpret_cast<float4*>(dst + ((size_t)y * PY + lpos<1>(z0 + zl)) * C::TPB_K + 2 * c) =
+            make_float4(v0.x, v0.y, v1.x, v1.y);
+      }
+    } else {
+      // [z][y][kx]
+      constexpr int NV = G * N * NH;
+      for (int i = threadIdx.x; i < NV; i += C::NT_A) {
+        const int row = i / NH, kx = i % NH;
+        dst[((size_t)(z0 + row / N) * N + row % N) * NH + kx] = s1_value(row / N, row % N, kx);
+      }
     }
   }
 }
 
 // ------------------------------------------------------------------ pass B
-// 64^3: four resident 288-thread CTAs per SM asked of the compiler (56 registers)
+// Pass B with the slabs staged through registers and cp.async (96^3, 128^3).
 template <int N>
-__global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_z_mul(const SearchChunkArgs a,
-                                                                      const float2* __restrict__ g_tw) {
+__device__ __forceinline__ void z_mul_staged(const SearchChunkArgs& a, const float2* __restrict__ g_tw) {
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, P = C::P, TPB = C::TPB, NT = C::NT_B;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -587,17 +645,17 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_
   const int w = 2 * a.radius + 1;
   constexpr int IT = (N * NB + NT - 1) / NT;
 
-  // this thread's elements i of the particle spectrum and of the first weight, copied
+  // this thread's elements i of the particle spectrum and (PREF_W) of the first weight, copied
   // asynchronously while the slab loads run
   float2* s_q = s_tw + N;                                     // [N * NHB]
-  float* s_w = reinterpret_cast<float*>(s_q + N * C::NHB);    // [N * NHB]
+  float* s_w = reinterpret_cast<float*>(s_q + N * C::NHB);    // [N * NHB] (PREF_W)
 #pragma unroll
   for (int k = 0; k < IT; ++k) {
     const int i = threadIdx.x + k * NT;
     if (i < N * NB && i % NB < cnt) {
       const size_t gi = ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB;
       cp_async8(s_q + i, q + gi);
-      if (w1) cp_async4(s_w + i, w1 + gi);
+      if (C::PREF_W && w1) cp_async4(s_w + i, w1 + gi);
     }
   }
   cp_async_commit();
@@ -621,7 +679,7 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_
   // the prefetched slabs are read by other threads' lines: wait for this thread's copies (and fold
   // a second weight into them), then the barrier publishes everyone's
   cp_async_wait<0>();
-  if (w2) {
+  if (C::PREF_W && w2) {
 #pragma unroll 1
     for (int k = 0; k < IT; ++k) {
       const int i = threadIdx.x + k * NT;
@@ -633,7 +691,8 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_
   for (int base = 0; base < TPB; base += C::TEAMS_B) {
     const int li = base + team;
     const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
-    zline_fused<N>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt, kl, k0 + kl, ky, s_q, s_w, w1 != nullptr, en);
+    zline_fused<N>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt, kl, k0 + kl, ky, s_q, s_w, w1 != nullptr,
+                   C::PREF_W ? nullptr : w1, C::PREF_W ? nullptr : w2, en);
   }
   if (w1) {
     double t = block_sum(en, red);
@@ -649,11 +708,138 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_
   }
 }
 
-// ------------------------------------------------------------------ pass C
-// 64^3: 4 resident CTAs per SM asked of the compiler (56 registers, no spill; 68 before): a chunk's
-// 990 CTAs then take two waves instead of three (22.0 us per chunk from 24.6)
+// Pass B with the S1 slab bulk-copied (BULK_B): pass A left the (evaluation, ky) slab in the tile's
+// layout, so one cp.async.bulk completed on an mbarrier brings it in; the particle spectrum and
+// weight rows arrive meanwhile as 16-byte cp.async pieces, and the fused z lines read them at the
+// rows' offsets from their 16-byte boundaries.  A spectrum or weight whose base is not 16-byte
+// aligned (a caller's buffer at an odd element offset) is copied element by element, at offset 0.
 template <int N>
-__global__ void __launch_bounds__(SearchCfg<N>::NT_BC, N <= 64 ? 4 : 0) k_search_inv_peak(const SearchChunkArgs a,
+__device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float2* __restrict__ g_tw) {
+  using C = SearchCfg<N>;
+  constexpr int NH = C::NH, P = C::P, NT = C::NT_B, NB = C::NHB, TP = C::TPB_K, QP = C::QP_K, WP = C::WP_K;
+  static_assert(C::KS_B == 1 && NB == NH, "bulk pass B takes whole ky rows");
+  static_assert(C::TEAMS_B >= NB, "one round of z lines");
+  constexpr unsigned SLAB_BYTES = (unsigned)(sizeof(float2) * C::PY * TP);
+  static_assert(SLAB_BYTES % 16 == 0, "bulk copy size");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* tile = reinterpret_cast<float2*>(smem_raw);                // [PY][TP], row z at lpos<1>(z)
+  float2* s_q = tile + (size_t)C::PY * TP;                            // [N][QP]
+  float* s_w = reinterpret_cast<float*>(s_q + (size_t)N * QP);       // [N][WP]
+  float2* s_tw = reinterpret_cast<float2*>(s_w + (size_t)N * WP);    // [N]
+  __shared__ double red[32];
+  __shared__ uint64_t bar;
+
+  const int e = blockIdx.y;
+  if (e >= a.n_items) return;
+  const int ky = blockIdx.x;
+  const EvalItem it = a.items[e];
+  const DevParticle& pt = a.parts[it.particle];
+  // weights on the rotated reference (BH_multi_xcf_Translational_2.m:35-38): the particle's wdgMask
+  // and the reference's bandpass wref; the first present one is copied, a second folded into it
+  const float* __restrict__ wref = a.refs[pt.ref].wref;
+  const float* __restrict__ w1 = pt.wedge ? pt.wedge : wref;
+  const float* __restrict__ w2 = pt.wedge ? wref : nullptr;
+  const int w = 2 * a.radius + 1;
+  constexpr size_t ZS = (size_t)N * NH;  // elements per z step of the spectrum and weight
+  const float2* slab = a.s1 + (size_t)e * C::S1_EVAL + (size_t)ky * C::PY * TP;
+  const float2* qrow = pt.spec + (size_t)ky * NH;
+  const float* wrow = w1 ? w1 + (size_t)ky * NH : nullptr;
+  const bool piece_q = ((uintptr_t)pt.spec & 15) == 0;
+  const bool piece_w = w1 && ((uintptr_t)w1 & 15) == 0;
+  // row offsets (elements) from the 16-byte boundary below each row start, and 16-byte pieces per row
+  const int offq = piece_q ? (int)(((uintptr_t)qrow & 15) >> 3) : 0;
+  const int offw = piece_w ? (int)(((uintptr_t)wrow & 15) >> 2) : 0;
+  const int pq = ((offq + NB) * 8 + 15) >> 4;
+  const int pw = ((offw + NB) * 4 + 15) >> 4;
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, SLAB_BYTES + a.phantom_tx);
+    bulk_copy_g2s(tile, slab, SLAB_BYTES, &bar);
+  }
+  if (piece_q) {
+    const char* src = reinterpret_cast<const char*>(qrow - offq);
+    for (int i = threadIdx.x; i < N * pq; i += NT) {
+      const int z = i / pq, c = i % pq;
+      cp_async16(reinterpret_cast<char*>(s_q + (size_t)z * QP) + 16 * c, src + z * ZS * sizeof(float2) + 16 * c);
+    }
+  } else {
+    for (int i = threadIdx.x; i < N * NB; i += NT) cp_async8(s_q + (i / NB) * QP + i % NB, qrow + (i / NB) * ZS + i % NB);
+  }
+  if (piece_w) {
+    const char* src = reinterpret_cast<const char*>(wrow - offw);
+    for (int i = threadIdx.x; i < N * pw; i += NT) {
+      const int z = i / pw, c = i % pw;
+      cp_async16(reinterpret_cast<char*>(s_w + (size_t)z * WP) + 16 * c, src + z * ZS * sizeof(float) + 16 * c);
+    }
+  } else if (w1) {
+    for (int i = threadIdx.x; i < N * NB; i += NT) cp_async4(s_w + (i / NB) * WP + i % NB, wrow + (i / NB) * ZS + i % NB);
+  }
+  cp_async_commit();
+  load_twiddles<N>(s_tw, g_tw);
+  cp_async_wait<0>();
+  __syncthreads();  // the barrier is initialised before anyone polls it
+  // the next barrier also publishes the cp.async pieces; the whole CTA takes the same branch
+  const bool arrived = mbar_wait(&bar, 0, a.wait_cycles);
+  if (__syncthreads_or(!arrived)) {
+    // the copies did not complete in time: report, give them a second bounded wait, and leave
+    if (threadIdx.x == 0 && a.status) atomicOr(a.status, kStatusWaitTimeout);
+    mbar_wait(&bar, 0, a.wait_cycles);
+    return;
+  }
+  if (w2) {
+    for (int i = threadIdx.x; i < N * NB; i += NT)
+      s_w[(i / NB) * WP + offw + i % NB] *= __ldg(w2 + (size_t)(i / NB) * ZS + (size_t)ky * NH + i % NB);
+  }
+  __syncthreads();
+
+  const int team = threadIdx.x / P, lane = threadIdx.x % P;
+  const int kl = team;  // consecutive columns for the teams of a warp
+  const bool weighted = w1 != nullptr;
+  const double hw = (kl == 0 || 2 * kl == N) ? 1.0 : 2.0;
+  double en = 0.0;
+  {
+    const float2* sq = s_q + offq + kl;
+    const float* sw = s_w + offw + kl;
+    fft_line_fwd_mul_inv<N, P, 1>(tile + kl, TP, lane, s_tw, kl < NB, [&](int z, float2 rr) {
+      const bool origin = z == 0 && ky == 0 && kl == 0;
+      if (weighted) {
+        const float wv = sw[z * WP];
+        rr.x *= wv;
+        rr.y *= wv;
+        if (!origin) en += hw * ((double)rr.x * rr.x + (double)rr.y * rr.y);
+      }
+      const float2 x = cmulc(sq[z * QP], rr);
+      return origin ? make_float2(0.f, 0.f) : x;
+    });
+  }
+  if (weighted) {
+    double t = block_sum(en, red);
+    if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
+  }
+  __syncthreads();
+  float2* dst = a.s2 + (size_t)e * w * ZS + (size_t)ky * NH;
+  for (int i = threadIdx.x; i < w * NB; i += NT) {
+    const int j = i / NB, c = i % NB;
+    const int z = (j - a.radius + N) % N;
+    dst[(size_t)j * ZS + c] = tile[lpos<1>(z) * TP + c];
+  }
+}
+
+// 64^3: four resident 288-thread CTAs per SM asked of the compiler
+template <int N>
+__global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_z_mul(const SearchChunkArgs a,
+                                                                      const float2* __restrict__ g_tw) {
+  if constexpr (SearchCfg<N>::BULK_B) {
+    z_mul_bulk<N>(a, g_tw);
+  } else {
+    z_mul_staged<N>(a, g_tw);
+  }
+}
+
+// ------------------------------------------------------------------ pass C
+template <int N>
+__global__ void __launch_bounds__(SearchCfg<N>::NT_BC, SearchCfg<N>::MINB_C) k_search_inv_peak(const SearchChunkArgs a,
                                                                           const float2* __restrict__ g_tw) {
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, P = C::P;
@@ -678,17 +864,22 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC, N <= 64 ? 4 : 0) k_search
   if (threadIdx.x == 0) s_best = 0ull;
   const float2* src = a.s2 + ((size_t)e * w + j) * N * NH;
   {
+    // the slab in groups of at most 16 loads in flight per thread
     constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
-    float2 v[IT];
+    constexpr int KB = IT < 16 ? IT : 16;
+#pragma unroll 1
+    for (int k0 = 0; k0 < IT; k0 += KB) {
+      float2 v[KB];
 #pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * C::NT_BC;
-      if (i < N * NH) v[k] = src[i];
-    }
+      for (int k = 0; k < KB; ++k) {
+        const int i = threadIdx.x + (k0 + k) * C::NT_BC;
+        if (i < N * NH) v[k] = src[i];
+      }
 #pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * C::NT_BC;
-      if (i < N * NH) tile[lpos<1>(i / NH) * NH + i % NH] = v[k];
+      for (int k = 0; k < KB; ++k) {
+        const int i = threadIdx.x + (k0 + k) * C::NT_BC;
+        if (i < N * NH) tile[lpos<1>(i / NH) * NH + i % NH] = v[k];
+      }
     }
   }
   __syncthreads();

@@ -45,7 +45,7 @@ constexpr size_t kItemOff = kDmatOff + kDmatBytes;                        // Eva
 constexpr size_t kItemBytes = sizeof(EvalItem) * EMC_NOALLOC_MAX_ORIENT;
 constexpr size_t kResOff = kItemOff + kItemBytes;                         // per-orientation results
 constexpr size_t kResBytes = sizeof(NoallocResult) * EMC_NOALLOC_MAX_ORIENT;
-constexpr size_t kBestOff = kResOff + kResBytes;                          // best key
+constexpr size_t kBestOff = kResOff + kResBytes;                          // best key, status word at +8
 constexpr size_t kBestBytes = 256;
 constexpr size_t kStatOff = kBestOff + kBestBytes;                        // stats + keys per chunk slot
 constexpr size_t kMaxChunk = 64;
@@ -193,7 +193,7 @@ emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int
                 "emc_search_plain_noalloc: peak radius %d not in [1, %d]", peak_radius, EMC_NOALLOC_MAX_RADIUS);
   EMC_CHECK_ARG(interp >= 0 && interp <= 2, "emc_search_plain_noalloc: interp %d", interp);
   EMC_CHECK_ARG(energy > 0.0, "emc_search_plain_noalloc: energy must be > 0");
-  const size_t per_eval = sizeof(float2) * (size_t)(n / 2 + 1) * n * (n + 2 * peak_radius + 1);
+  const size_t per_eval = sizeof(float2) * (s1_eval_elems(n) + (size_t)(n / 2 + 1) * n * (2 * peak_radius + 1));
   const size_t avail = EMC_NOALLOC_SCRATCH_BYTES - kSpecOff;
   const int chunk = (int)std::min<size_t>(kMaxChunk, avail / per_eval);
   EMC_CHECK_ARG(chunk >= 1, "emc_search_plain_noalloc: box %d with radius %d needs %zu B of scratch per "
@@ -230,7 +230,8 @@ emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int
   EMC_CUDA(cudaMemcpyAsync(base + hdr, host.data(), used, cudaMemcpyHostToDevice, st));
 
   unsigned long long* best = reinterpret_cast<unsigned long long*>(base + kBestOff);
-  EMC_CUDA(cudaMemsetAsync(best, 0, sizeof(unsigned long long), st));
+  unsigned* status = reinterpret_cast<unsigned*>(base + kBestOff + 8);
+  EMC_CUDA(cudaMemsetAsync(best, 0, 16, st));  // best key and status word
   SearchChunkArgs a;
   a.items = reinterpret_cast<const EvalItem*>(base + it);
   a.parts = reinterpret_cast<const DevParticle*>(base + hdr);
@@ -239,10 +240,11 @@ emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int
   a.stats = reinterpret_cast<EvalStats*>(base + kStatOff);
   a.keys = reinterpret_cast<unsigned long long*>(base + kStatOff + sizeof(EvalStats) * kMaxChunk);
   a.s1 = reinterpret_cast<float2*>(base + kSpecOff);
-  a.s2 = a.s1 + (size_t)chunk * n * n * (n / 2 + 1);
+  a.s2 = a.s1 + (size_t)chunk * s1_eval_elems(n);
   a.n_items = 0;
   a.radius = peak_radius;
   a.interp = interp;
+  a.status = status;
   const float2* tw = reinterpret_cast<const float2*>(base + kTwOff) + tw_offset(n);
   NoallocResult* res = reinterpret_cast<NoallocResult*>(base + kResOff);
   emc_status rs = n == 64 ? run_chunks<64>(a, n_orient, chunk, tw, res, best, st)
@@ -253,6 +255,12 @@ emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int
   EMC_LAUNCH_CHECK();
   // the host staging vector must stay alive until the copy has been consumed
   EMC_CUDA(cudaStreamSynchronize(st));
+  unsigned waited_out = 0;
+  EMC_CUDA(cudaMemcpy(&waited_out, status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (waited_out) {
+    set_error("emc_search_plain_noalloc: a device-side wait for bulk copies gave up; results are invalid");
+    return EMC_E_TIMEOUT;
+  }
   return EMC_OK;
 }
 

@@ -316,10 +316,21 @@ EMC_API emc_status emc_search_run(emc_search_t s, const emc_particle_desc* parti
 EMC_API emc_status emc_search_run_energies(emc_search_t s, const emc_particle_desc* particles,
                                    int n_particles, const double* d_energy, float* d_cc,
                                    int* d_peak, emc_search_hit* d_best, void* stream);
-/* Same as emc_search_run with host output buffers (copies inside, synchronises). */
+/* Same as emc_search_run with host output buffers (copies inside, synchronises).  Returns
+ * EMC_E_TIMEOUT when a device-side wait of the run gave up (see emc_search_status). */
 EMC_API emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particles,
                                int n_particles, float* h_cc, int* h_peak,
                                emc_search_hit* h_best, void* stream);
+/* No counterpart in the reference.  Synchronises `stream` and reports whether a device-side wait of
+ * the handle's runs since the last check gave up (EMC_E_TIMEOUT; the results of those runs are
+ * invalid), clearing the report.  The waits (for the bulk copies of the 64^3 z pass) are bounded
+ * at about a second, after which the CTA leaves without a result; the context stays usable. */
+EMC_API emc_status emc_search_status(emc_search_t s, void* stream);
+/* Test hook (no counterpart in the reference): waits of later runs give up after wait_cycles SM
+ * clock cycles (default 2^31), and announce phantom_bytes (a multiple of 16, at most 4096) more
+ * bytes than they copy, so that with phantom_bytes > 0 every such wait runs out.
+ * emc_search_test_wait(s, 1ll << 31, 0) restores the defaults. */
+EMC_API emc_status emc_search_test_wait(emc_search_t s, long long wait_cycles, unsigned phantom_bytes);
 EMC_API emc_status emc_search_destroy(emc_search_t s);
 /* Measurement hook (no counterpart in the reference).  With profiling enabled, emc_search_run
  * launches eagerly instead of through the graph and brackets each pass launch with CUDA events
@@ -344,9 +355,10 @@ EMC_API emc_status emc_search_timings(emc_search_t s, double ms[4], long launche
 EMC_API emc_status emc_search_set_planes(emc_search_t s, int box, int planes);
 EMC_API emc_status emc_search_get_planes(emc_search_t s, int box, int dtype, int* planes, float ms_per_option[4]);
 /* Tuning hook (no counterpart in the reference).  A recorded run keeps slots = 1 or 2 sets of chunk
- * scratch (2 by default); with 2, consecutive chunks go to two branches of the CUDA graph and run
- * concurrently (the passes of one chunk fill the tails of the other's), chunks of one slot in order.
- * Profiled runs (emc_search_set_profiling) use one slot so that per-pass times stay separable. */
+ * scratch (2 by default); with 2, consecutive chunks of boxes below 128 go to two branches of the
+ * CUDA graph and run concurrently (the passes of one chunk fill the tails of the other's), chunks of
+ * one slot in order; chunks of 128^3 and larger always run one at a time.  Profiled runs
+ * (emc_search_set_profiling) use one slot so that per-pass times stay separable. */
 EMC_API emc_status emc_search_set_overlap(emc_search_t s, int slots);
 
 
@@ -363,7 +375,8 @@ EMC_API emc_status emc_search_set_overlap(emc_search_t s, int slots);
  * the stream before returning.  The search runs with no particle wedge (wdgMask = 1): fold any
  * particle-side weight into d_spectrum.  Limits (EMC_E_ARG beyond them): box 64, 96 or 128,
  * FP32 reference, 1..4096 orientations (host (phi, theta, psi) triples), peak radius 1..15.
- * Same arguments and outputs as emc_search_run for one particle (device outputs may be NULL). */
+ * Same arguments and outputs as emc_search_run for one particle (device outputs may be NULL);
+ * EMC_E_TIMEOUT (results invalid) if a bounded device-side wait gave up, as emc_search_status. */
 EMC_API emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int n,
                                             const float* d_spectrum, double energy, const double prior[9],
                                             const float shift[3], const double* phi_theta_psi, int n_orient,

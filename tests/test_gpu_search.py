@@ -445,3 +445,65 @@ def test_chunk_overlap_gives_identical_results(built_lib, cuda):
     ref = out[1][0]
     for cc, pk, best in out[1][1:] + out[2]:
         assert np.array_equal(cc, ref[0]) and np.array_equal(pk, ref[1]) and np.array_equal(best, ref[2])
+
+
+def _aligned_run(s, rid, q, e, w, grid):
+    return s.run_host([s.particle(q, e, rid, orient_count=len(grid), wedge=w)])
+
+
+def test_z_pass_copies_any_alignment(plain_case):
+    """64^3 pass B copies the slabs in 16-byte rows from the boundary below each row start; a spectrum
+    or weight at an odd element offset (no 16-byte aligned base) is copied element by element.  Every
+    placement gives the same bits."""
+    from emclarity_b200 import api
+    case, g = plain_case
+    grid = case.grid[:24]
+    q, e = api.particle_spectrum(g["particle"])
+    w = g["weight"].contiguous()
+    s = api.Search(peak_radius=case.peak_radius)
+    rid = s.add_reference(g["ref"], g["mask"])
+    s.set_orientations(grid)
+    cc0, pk0, best0 = _aligned_run(s, rid, q, e.item(), w, grid)
+    for qo, wo in ((1, 0), (0, 1), (1, 2), (0, 3), (1, 3)):
+        qb = torch.zeros(q.numel() + 2, dtype=q.dtype, device=q.device)
+        qb[qo:qo + q.numel()] = q.flatten()
+        wb = torch.zeros(w.numel() + 4, dtype=w.dtype, device=w.device)
+        wb[wo:wo + w.numel()] = w.flatten()
+        q2, w2 = qb[qo:qo + q.numel()].view(q.shape), wb[wo:wo + w.numel()].view(w.shape)
+        assert (q2.data_ptr() % 16 != 0) == (qo == 1) and (w2.data_ptr() % 16 != 0) == (wo != 0)
+        cc, pk, best = _aligned_run(s, rid, q2, e.item(), w2, grid)
+        assert np.array_equal(cc, cc0) and np.array_equal(pk, pk0) and best == best0, (qo, wo)
+    s.close()
+
+
+def test_bounded_wait_reports_timeout_and_context_stays_usable(plain_case):
+    """A pass-B wait that runs out (the test hook announces 16 bytes that are never copied) is
+    reported as EMC_E_TIMEOUT by run_host and by status() after a device-output run; with the
+    defaults restored the same handle gives the same results as before."""
+    from emclarity_b200 import _lib as L
+    from emclarity_b200 import api
+    case, g = plain_case
+    grid = case.grid[:16]
+    q, e = api.particle_spectrum(g["particle"])
+    s = api.Search(peak_radius=case.peak_radius)
+    rid = s.add_reference(g["ref"], g["mask"])
+    s.set_orientations(grid)
+    desc = [s.particle(q, e.item(), rid, orient_count=len(grid), wedge=g["weight"])]
+    cc0, pk0, best0 = s.run_host(desc)
+    s.test_wait(wait_cycles=100_000, phantom_bytes=16)
+    with pytest.raises(L.EmcError) as ei:
+        s.run_host(desc)
+    assert ei.value.status == L.EMC_E_TIMEOUT
+    cc_d = torch.empty(len(grid), device="cuda")
+    s.run(desc, cc=cc_d)
+    with pytest.raises(L.EmcError) as ei:
+        s.status()
+    assert ei.value.status == L.EMC_E_TIMEOUT
+    s.status()  # the report was cleared
+    s.test_wait()
+    cc1, pk1, best1 = s.run_host(desc)
+    assert np.array_equal(cc1, cc0) and np.array_equal(pk1, pk0) and best1 == best0
+    s.run(desc, cc=cc_d)
+    s.status()
+    assert np.array_equal(cc_d.cpu().numpy(), cc0)
+    s.close()
