@@ -410,8 +410,8 @@ class Search:
         L.call("emc_search_set_planes", self._h, int(box), int(planes))
 
     def set_overlap(self, slots):
-        """Chunk scratch slots of recorded runs: 2 (default) runs consecutive chunks of boxes below 128
-        concurrently, 1 in order."""
+        """Chunk scratch slots of recorded runs: 2 (default) runs consecutive 64^3 chunks concurrently,
+        1 in order (larger boxes always run in order)."""
         L.call("emc_search_set_overlap", self._h, int(slots))
 
     def status(self):

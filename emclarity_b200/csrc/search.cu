@@ -630,15 +630,15 @@ static emc_status search_record(emc_search_t s, const std::vector<Chunk>& chunks
     ++launches;
   }
   // The second branch forks from the stream after the set-up above and joins before the outputs.
-  // Chunks of boxes of 128 and above run alone on the stream (the branch joined first): their
-  // passes fill the SMs by themselves, and beside another chunk's they ran slower (128^3: 40.2k
-  // evaluations/s with two slots against 44.9k with one).
+  // Only 64^3 chunks overlap; larger ones run alone on the stream (the branch joined first): their
+  // passes fill the SMs by themselves, and beside another chunk's they ran slower (96^3: 96.0k
+  // evaluations/s with two slots against 101.1k with one; 128^3: 40.2k against 44.9k).
   const bool two = nslots > 1 && chunks.size() > 1;
   bool forked = false;
   long alternate = 0;
   for (size_t ci = 0; ci < chunks.size(); ++ci) {
     const Chunk& c = chunks[ci];
-    const bool overlapped = two && c.n < 128;
+    const bool overlapped = two && c.n <= 64;
     if (overlapped && !forked) {
       EMC_CUDA(cudaEventRecord(s->fork_ev, st));
       EMC_CUDA(cudaStreamWaitEvent(s->branch, s->fork_ev, 0));

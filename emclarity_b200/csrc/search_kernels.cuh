@@ -285,7 +285,7 @@ struct SearchCfg {
   // The weight slab is prefetched too up to 96^3; at 128^3 it is read from L2 when the product is
   // formed, so that three CTAs per SM fit in shared memory instead of two.
   static constexpr bool PREF_W = N <= 96;
-  // 64^3: pass A writes S1 as pass B's shared-memory tiles -- per (evaluation, ky) a slab of PY rows
+  // 64^3 and 96^3: pass A writes S1 as pass B's shared-memory tiles -- per (evaluation, ky) a slab of PY rows
   // (row z at lpos<1>(z)) of TPB_K float2 -- which pass B fetches with one bulk copy.  The particle
   // spectrum and weight rows (the caller's layout) come in 16-byte cp.async pieces from the 16-byte
   // boundary at or below each row start, into rows of even pitch (QP_K float2, WP_K floats), and are
@@ -293,7 +293,7 @@ struct SearchCfg {
   // elements, a multiple of 16 bytes).  The teams of a warp take consecutive columns: with the even
   // tile pitch the two teams of a half-warp then fall on complementary banks in every stage, and the
   // four of a warp read the weight rows (pitch 36) on disjoint banks.
-  static constexpr bool BULK_B = N == 64;
+  static constexpr bool BULK_B = N <= 96;
   static constexpr int TPB_K = NHB + 1 + (NHB + 1) % 2;                 // >= NHB + 1, even
   static constexpr int QP_K = TPB_K;
   static constexpr int WP_K = ((NHB + 3 + 3) / 4) * 4;                   // >= NHB + 3, 16-byte rows
@@ -306,7 +306,7 @@ struct SearchCfg {
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
 };
 
-// S1 elements per evaluation of box n (the 64^3 slabs are padded to the z pass's tiles).
+// S1 elements per evaluation of box n (the 64^3 and 96^3 slabs are padded to the z pass's tiles).
 inline size_t s1_eval_elems(int n) {
   return n == 64 ? SearchCfg<64>::S1_EVAL : n == 96 ? SearchCfg<96>::S1_EVAL : SearchCfg<128>::S1_EVAL;
 }

@@ -323,7 +323,7 @@ EMC_API emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* 
                                emc_search_hit* h_best, void* stream);
 /* No counterpart in the reference.  Synchronises `stream` and reports whether a device-side wait of
  * the handle's runs since the last check gave up (EMC_E_TIMEOUT; the results of those runs are
- * invalid), clearing the report.  The waits (for the bulk copies of the 64^3 z pass) are bounded
+ * invalid), clearing the report.  The waits (for the bulk copies of the 64^3 and 96^3 z pass) are bounded
  * at about a second, after which the CTA leaves without a result; the context stays usable. */
 EMC_API emc_status emc_search_status(emc_search_t s, void* stream);
 /* Test hook (no counterpart in the reference): waits of later runs give up after wait_cycles SM
@@ -355,9 +355,9 @@ EMC_API emc_status emc_search_timings(emc_search_t s, double ms[4], long launche
 EMC_API emc_status emc_search_set_planes(emc_search_t s, int box, int planes);
 EMC_API emc_status emc_search_get_planes(emc_search_t s, int box, int dtype, int* planes, float ms_per_option[4]);
 /* Tuning hook (no counterpart in the reference).  A recorded run keeps slots = 1 or 2 sets of chunk
- * scratch (2 by default); with 2, consecutive chunks of boxes below 128 go to two branches of the
- * CUDA graph and run concurrently (the passes of one chunk fill the tails of the other's), chunks of
- * one slot in order; chunks of 128^3 and larger always run one at a time.  Profiled runs
+ * scratch (2 by default); with 2, consecutive 64^3 chunks go to two branches of the CUDA graph and
+ * run concurrently (the passes of one chunk fill the tails of the other's), chunks of one slot in
+ * order; chunks of larger boxes always run one at a time.  Profiled runs
  * (emc_search_set_profiling) use one slot so that per-pass times stay separable. */
 EMC_API emc_status emc_search_set_overlap(emc_search_t s, int slots);
 
