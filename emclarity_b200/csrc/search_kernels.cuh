@@ -5,11 +5,13 @@
 //                                (no weight on the reference: FP64 sums of r and r^2, the
 //                                DC-free energy by Parseval)
 //                                R2C along x (two rows per complex FFT), FFT along y
-//                                -> S1[e][z][y][kx]                         (n * n * nh c64)
-//   pass B  (CTA = one ky row)   FFT along z, X = Q .* conj(wref .* R) .* wdgMask, X(0) = 0,
-//                                E_R = sum |wref .* R .* wdgMask|^2 when either weight is set
-//                                (formed in registers between the transforms, zline_fused),
-//                                inverse FFT along z, keep the w output planes |sz| <= r
+//                                -> S1[e][ky][part][z][kx], one padded slab per (ky, column part)
+//                                   in pass B's tile layout                (~n * n * nh c64)
+//   pass B  (CTA = one ky row    slab in by one bulk copy; FFT along z, X = Q .* conj(wref .* R)
+//            or half of one)     .* wdgMask, X(0) = 0, E_R = sum |wref .* R .* wdgMask|^2 when
+//                                either weight is set (formed in registers between the
+//                                transforms, fft_line_fwd_mul_inv), inverse FFT along z, keep the
+//                                w output planes |sz| <= r
 //                                -> S2[e][j][ky][kx]                        (w * n * nh c64)
 //   pass C  (CTA = one sz plane) inverse FFT along y, C2R along x for the w rows |sy| <= r,
 //                                normalise by sqrt(E_R E_P), spherical peak mask,
@@ -271,75 +273,38 @@ struct SearchCfg {
   static constexpr int SMEM_CTAS_A = (int)((228 * 1024) / (SMEM_A + 1024));
   static constexpr int MINB_A = N <= 64 ? (G == 1 ? 5 : 0) : (SMEM_CTAS_A < 2 ? SMEM_CTAS_A : 2);
   // Pass B: a CTA transforms the z lines of one ky and one of KS_B parts of the kx columns (NHB
-  // columns at most, tile pitch TPB odd so the spread of lines over banks stays a permutation).
-  // It prefetches its particle-spectrum and weight slabs into shared memory (64^3: four CTAs per
-  // SM; 96^3: the prefetch also frees the registers that held them, so two CTAs fit instead of
-  // one).  128^3 splits the columns in two: with the whole ky row a CTA needed 544 threads and 95
-  // registers (one CTA per SM, latency-bound); half rows fit two per SM.
+  // columns at most).  128^3 splits the columns in two: with the whole ky row a CTA needed 544
+  // threads and 95 registers (one CTA per SM, latency-bound); half rows fit three per SM.
+  // Pass A writes S1 as pass B's shared-memory tiles: per (evaluation, ky, column part) a slab of PY
+  // rows (row z at lpos<1>(z)) of TPB_K float2, which pass B fetches with one bulk copy.  The
+  // particle spectrum and weight rows (the caller's layout) come in 16-byte cp.async pieces from the
+  // 16-byte boundary at or below each row start, into rows of even pitch (QP_K float2, WP_K floats),
+  // and are read at the row's offset from that boundary (the same for every row of a CTA: a z step
+  // is N NH elements, a multiple of 16 bytes).  The teams of a warp take consecutive columns: with
+  // the even tile pitch the two teams of a half-warp fall on complementary banks in every stage at
+  // 64^3 (96^3 and 128^3 keep the few conflicts their radix-3 / radix-16 stages had with an odd
+  // pitch), and the four of a warp read the weight rows (pitch WP_K) on disjoint banks.
   static constexpr int KS_B = N >= 128 ? 2 : 1;
   static constexpr int NHB = (NH + KS_B - 1) / KS_B;
-  static constexpr int TPB = NHB | 1;
   static constexpr int NT_B = ((NHB * P + 31) / 32) * 32;
   static constexpr int TEAMS_B = NT_B / P;
   static constexpr int GRID_BX = N * KS_B;
-  // The weight slab is prefetched too up to 96^3; at 128^3 it is read from L2 when the product is
-  // formed, so that three CTAs per SM fit in shared memory instead of two.
-  static constexpr bool PREF_W = N <= 96;
-  // 64^3 and 96^3: pass A writes S1 as pass B's shared-memory tiles -- per (evaluation, ky) a slab of PY rows
-  // (row z at lpos<1>(z)) of TPB_K float2 -- which pass B fetches with one bulk copy.  The particle
-  // spectrum and weight rows (the caller's layout) come in 16-byte cp.async pieces from the 16-byte
-  // boundary at or below each row start, into rows of even pitch (QP_K float2, WP_K floats), and are
-  // read at the row's offset from that boundary (the same for every row of a CTA: a z step is N NH
-  // elements, a multiple of 16 bytes).  The teams of a warp take consecutive columns: with the even
-  // tile pitch the two teams of a half-warp then fall on complementary banks in every stage, and the
-  // four of a warp read the weight rows (pitch 36) on disjoint banks.
-  static constexpr bool BULK_B = N <= 96;
   static constexpr int TPB_K = NHB + 1 + (NHB + 1) % 2;                 // >= NHB + 1, even
   static constexpr int QP_K = TPB_K;
   static constexpr int WP_K = ((NHB + 3 + 3) / 4) * 4;                   // >= NHB + 3, 16-byte rows
-  // S1 elements per evaluation
-  static constexpr size_t S1_EVAL = BULK_B ? (size_t)N * PY * TPB_K : (size_t)N * N * NH;
-  static constexpr size_t SMEM_B =
-      BULK_B ? sizeof(float2) * ((size_t)PY * TPB_K + (size_t)N * QP_K + N) + sizeof(float) * (size_t)N * WP_K
-             : sizeof(float2) * ((size_t)PY * TPB + N) +
-                   (sizeof(float2) + (PREF_W ? sizeof(float) : 0)) * (size_t)N * NHB;
+  // The weight rows are copied too up to 96^3; at 128^3 the weight is read from L2 when the product
+  // is formed, so that three CTAs per SM fit in shared memory instead of two.
+  static constexpr bool PREF_W = N <= 96;
+  // S1 elements per evaluation: a slab per (ky, column part)
+  static constexpr size_t S1_EVAL = (size_t)N * KS_B * PY * TPB_K;
+  static constexpr size_t SMEM_B = sizeof(float2) * ((size_t)PY * TPB_K + (size_t)N * QP_K + N) +
+                                   (PREF_W ? sizeof(float) * (size_t)N * WP_K : 0);
   static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
 };
 
-// S1 elements per evaluation of box n (the 64^3 and 96^3 slabs are padded to the z pass's tiles).
+// S1 elements per evaluation of box n (slabs padded to the z pass's tiles).
 inline size_t s1_eval_elems(int n) {
   return n == 64 ? SearchCfg<64>::S1_EVAL : n == 96 ? SearchCfg<96>::S1_EVAL : SearchCfg<128>::S1_EVAL;
-}
-
-// Pass B's z line of local column kl (fft_line_fwd_mul_inv): between the forward and the inverse
-// transform, in registers, element z is weighted (wdgMask and wref: prefetched into s_w, or read from
-// w1 / w2 when PREF_W is off), its |.|^2 added to E_R and multiplied into Q conj(R) (0 at the origin).
-template <int N>
-__device__ __forceinline__ void zline_fused(float2* buf, int stride, int lane, const float2* tw, bool active, int kl,
-                                            int kx, int ky, const float2* s_q, const float* s_w, bool weighted,
-                                            const float* w1, const float* w2, double& en) {
-  using C = SearchCfg<N>;
-  constexpr int NB = C::NHB, NH = C::NH;
-  const double hw = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
-  fft_line_fwd_mul_inv<N, C::P, 1>(buf, stride, lane, tw, active, [&](int z, float2 rr) {
-    const int i = z * NB + kl;
-    const bool origin = z == 0 && ky == 0 && kx == 0;
-    if (weighted) {
-      float wv;
-      if constexpr (C::PREF_W) {
-        wv = s_w[i];
-      } else {
-        const size_t gi = ((size_t)z * N + ky) * NH + kx;
-        wv = __ldg(w1 + gi);
-        if (w2) wv *= __ldg(w2 + gi);
-      }
-      rr.x *= wv;
-      rr.y *= wv;
-      if (!origin) en += hw * ((double)rr.x * rr.x + (double)rr.y * rr.y);
-    }
-    const float2 x = cmulc(s_q[i], rr);
-    return origin ? make_float2(0.f, 0.f) : x;
-  });
 }
 
 // Line li of a strided-FFT round handled by team `team`: consecutive teams get kx values 8
@@ -592,123 +557,27 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
       return pl[lpos<1>(y) * NH + kx];
     };
     float2* dst = a.s1 + (size_t)e * C::S1_EVAL;
-    if constexpr (C::BULK_B) {
-      // slabs [ky][lpos(z)][TPB_K]: whole rows, pad columns zero, two elements per 16-byte store
-      constexpr int RP = C::TPB_K / 2;
-      constexpr int NV = G * N * RP;
+    {
+      // slabs [ky][part][lpos(z)][TPB_K] (part: columns [part NHB, part NHB + NHB)): whole rows, pad
+      // columns zero, two elements per 16-byte store
+      constexpr int RP = C::TPB_K / 2, KS = C::KS_B, NB = C::NHB;
+      constexpr int NV = G * N * KS * RP;
       for (int i = threadIdx.x; i < NV; i += C::NT_A) {
-        const int row = i / RP, c = i % RP;  // row = zl * N + y
+        const int row = i / (KS * RP), rem = i % (KS * RP);  // row = zl * N + y
+        const int part = rem / RP, c = rem % RP;
         const int zl = row / N, y = row % N;
-        const float2 v0 = s1_value(zl, y, 2 * c), v1 = s1_value(zl, y, 2 * c + 1);
-        *reinterpret_cast<float4*>(dst + ((size_t)y * PY + lpos<1>(z0 + zl)) * C::TPB_K + 2 * c) =
+        const int k0 = part * NB + 2 * c;
+        const float2 v0 = 2 * c < NB ? s1_value(zl, y, k0) : make_float2(0.f, 0.f);
+        const float2 v1 = 2 * c + 1 < NB ? s1_value(zl, y, k0 + 1) : make_float2(0.f, 0.f);
+        *reinterpret_cast<float4*>(dst + (((size_t)y * KS + part) * PY + lpos<1>(z0 + zl)) * C::TPB_K + 2 * c) =
             make_float4(v0.x, v0.y, v1.x, v1.y);
-      }
-    } else {
-      // [z][y][kx]
-      constexpr int NV = G * N * NH;
-      for (int i = threadIdx.x; i < NV; i += C::NT_A) {
-        const int row = i / NH, kx = i % NH;
-        dst[((size_t)(z0 + row / N) * N + row % N) * NH + kx] = s1_value(row / N, row % N, kx);
       }
     }
   }
 }
 
 // ------------------------------------------------------------------ pass B
-// Pass B with the slabs staged through registers and cp.async (96^3, 128^3).
-template <int N>
-__device__ __forceinline__ void z_mul_staged(const SearchChunkArgs& a, const float2* __restrict__ g_tw) {
-  using C = SearchCfg<N>;
-  constexpr int NH = C::NH, P = C::P, TPB = C::TPB, NT = C::NT_B;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tile = reinterpret_cast<float2*>(smem_raw);  // [PY][TPB], row z at lpos<1>(z), local column
-  float2* s_tw = tile + (size_t)C::PY * TPB;
-  __shared__ double red[32];
-
-  const int e = blockIdx.y;
-  if (e >= a.n_items) return;
-  const int ky = blockIdx.x / C::KS_B;
-  // this CTA's columns: kx in [k0, k0 + cnt); element i = z * NHB + local column (constant divisor),
-  // local columns >= cnt (the short last part) skipped
-  const int k0 = C::KS_B == 1 ? 0 : (int)(blockIdx.x % C::KS_B) * C::NHB;
-  const int cnt = C::KS_B == 1 ? NH : min(C::NHB, NH - k0);
-  constexpr int NB = C::NHB;
-  const EvalItem it = a.items[e];
-  const DevParticle& pt = a.parts[it.particle];
-  // weights on the rotated reference: the reference's bandpass wref and the particle's wdgMask
-  // (BH_multi_xcf_Translational_2.m:35-38).  The first present one (the wedge when both are) is
-  // prefetched into shared memory with the spectrum; a second one is folded into that copy.
-  const float* __restrict__ wref = a.refs[pt.ref].wref;
-  const float* __restrict__ w1 = pt.wedge ? pt.wedge : wref;
-  const float* __restrict__ w2 = pt.wedge ? wref : nullptr;
-  const float2* __restrict__ q = pt.spec;
-  const int w = 2 * a.radius + 1;
-  constexpr int IT = (N * NB + NT - 1) / NT;
-
-  // this thread's elements i of the particle spectrum and (PREF_W) of the first weight, copied
-  // asynchronously while the slab loads run
-  float2* s_q = s_tw + N;                                     // [N * NHB]
-  float* s_w = reinterpret_cast<float*>(s_q + N * C::NHB);    // [N * NHB] (PREF_W)
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    const int i = threadIdx.x + k * NT;
-    if (i < N * NB && i % NB < cnt) {
-      const size_t gi = ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB;
-      cp_async8(s_q + i, q + gi);
-      if (C::PREF_W && w1) cp_async4(s_w + i, w1 + gi);
-    }
-  }
-  cp_async_commit();
-  load_twiddles<N>(s_tw, g_tw);
-  const float2* src = a.s1 + (size_t)e * N * N * NH + (size_t)ky * NH + k0;
-  {
-    // all of a thread's loads in flight before the first shared-memory store
-    float2 v[IT];
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * NT;
-      if (i < N * NB && i % NB < cnt) v[k] = src[(size_t)(i / NB) * N * NH + i % NB];
-    }
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * NT;
-      if (i < N * NB && i % NB < cnt) tile[lpos<1>(i / NB) * TPB + i % NB] = v[k];
-    }
-  }
-  const int team = threadIdx.x / P, lane = threadIdx.x % P;
-  // the prefetched slabs are read by other threads' lines: wait for this thread's copies (and fold
-  // a second weight into them), then the barrier publishes everyone's
-  cp_async_wait<0>();
-  if (C::PREF_W && w2) {
-#pragma unroll 1
-    for (int k = 0; k < IT; ++k) {
-      const int i = threadIdx.x + k * NT;
-      if (i < N * NB && i % NB < cnt) s_w[i] *= __ldg(w2 + ((size_t)(i / NB) * N + ky) * NH + k0 + i % NB);
-    }
-  }
-  __syncthreads();
-  double en = 0.0;
-  for (int base = 0; base < TPB; base += C::TEAMS_B) {
-    const int li = base + team;
-    const int kl = li < TPB ? (P == 8 ? pair_spread(li, TPB) : (li * 8) % TPB) : 0;
-    zline_fused<N>(tile + kl, TPB, lane, s_tw, li < TPB && kl < cnt, kl, k0 + kl, ky, s_q, s_w, w1 != nullptr,
-                   C::PREF_W ? nullptr : w1, C::PREF_W ? nullptr : w2, en);
-  }
-  if (w1) {
-    double t = block_sum(en, red);
-    if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
-  }
-  __syncthreads();
-  float2* dst = a.s2 + (size_t)e * w * N * NH + (size_t)ky * NH + k0;
-  for (int i = threadIdx.x; i < w * NB; i += NT) {
-    const int j = i / NB, kl = i % NB;
-    if (kl >= cnt) continue;
-    const int z = (j - a.radius + N) % N;
-    dst[(size_t)j * N * NH + kl] = tile[lpos<1>(z) * TPB + kl];
-  }
-}
-
-// Pass B with the S1 slab bulk-copied (BULK_B): pass A left the (evaluation, ky) slab in the tile's
+// Pass B: pass A left the (evaluation, ky, column part) slab in the tile's
 // layout, so one cp.async.bulk completed on an mbarrier brings it in; the particle spectrum and
 // weight rows arrive meanwhile as 16-byte cp.async pieces, and the fused z lines read them at the
 // rows' offsets from their 16-byte boundaries.  A spectrum or weight whose base is not 16-byte
@@ -717,21 +586,23 @@ template <int N>
 __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float2* __restrict__ g_tw) {
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, P = C::P, NT = C::NT_B, NB = C::NHB, TP = C::TPB_K, QP = C::QP_K, WP = C::WP_K;
-  static_assert(C::KS_B == 1 && NB == NH, "bulk pass B takes whole ky rows");
   static_assert(C::TEAMS_B >= NB, "one round of z lines");
   constexpr unsigned SLAB_BYTES = (unsigned)(sizeof(float2) * C::PY * TP);
   static_assert(SLAB_BYTES % 16 == 0, "bulk copy size");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* tile = reinterpret_cast<float2*>(smem_raw);                // [PY][TP], row z at lpos<1>(z)
   float2* s_q = tile + (size_t)C::PY * TP;                            // [N][QP]
-  float* s_w = reinterpret_cast<float*>(s_q + (size_t)N * QP);       // [N][WP]
-  float2* s_tw = reinterpret_cast<float2*>(s_w + (size_t)N * WP);    // [N]
+  float* s_w = reinterpret_cast<float*>(s_q + (size_t)N * QP);       // [N][WP] (PREF_W)
+  float2* s_tw = reinterpret_cast<float2*>(s_w + (C::PREF_W ? (size_t)N * WP : 0));  // [N]
   __shared__ double red[32];
   __shared__ uint64_t bar;
 
   const int e = blockIdx.y;
   if (e >= a.n_items) return;
-  const int ky = blockIdx.x;
+  // this CTA's columns: kx in [k0, k0 + cnt)
+  const int ky = blockIdx.x / C::KS_B;
+  const int k0 = (int)(blockIdx.x % C::KS_B) * NB;
+  const int cnt = min(NB, NH - k0);
   const EvalItem it = a.items[e];
   const DevParticle& pt = a.parts[it.particle];
   // weights on the rotated reference (BH_multi_xcf_Translational_2.m:35-38): the particle's wdgMask
@@ -741,16 +612,16 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
   const float* __restrict__ w2 = pt.wedge ? wref : nullptr;
   const int w = 2 * a.radius + 1;
   constexpr size_t ZS = (size_t)N * NH;  // elements per z step of the spectrum and weight
-  const float2* slab = a.s1 + (size_t)e * C::S1_EVAL + (size_t)ky * C::PY * TP;
-  const float2* qrow = pt.spec + (size_t)ky * NH;
-  const float* wrow = w1 ? w1 + (size_t)ky * NH : nullptr;
+  const float2* slab = a.s1 + (size_t)e * C::S1_EVAL + (size_t)blockIdx.x * C::PY * TP;
+  const float2* qrow = pt.spec + (size_t)ky * NH + k0;
+  const float* wrow = w1 ? w1 + (size_t)ky * NH + k0 : nullptr;
   const bool piece_q = ((uintptr_t)pt.spec & 15) == 0;
-  const bool piece_w = w1 && ((uintptr_t)w1 & 15) == 0;
+  const bool piece_w = C::PREF_W && w1 && ((uintptr_t)w1 & 15) == 0;
   // row offsets (elements) from the 16-byte boundary below each row start, and 16-byte pieces per row
   const int offq = piece_q ? (int)(((uintptr_t)qrow & 15) >> 3) : 0;
   const int offw = piece_w ? (int)(((uintptr_t)wrow & 15) >> 2) : 0;
-  const int pq = ((offq + NB) * 8 + 15) >> 4;
-  const int pw = ((offw + NB) * 4 + 15) >> 4;
+  const int pq = ((offq + cnt) * 8 + 15) >> 4;
+  const int pw = ((offw + cnt) * 4 + 15) >> 4;
 
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
@@ -764,7 +635,8 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
       cp_async16(reinterpret_cast<char*>(s_q + (size_t)z * QP) + 16 * c, src + z * ZS * sizeof(float2) + 16 * c);
     }
   } else {
-    for (int i = threadIdx.x; i < N * NB; i += NT) cp_async8(s_q + (i / NB) * QP + i % NB, qrow + (i / NB) * ZS + i % NB);
+    for (int i = threadIdx.x; i < N * NB; i += NT)
+      if (i % NB < cnt) cp_async8(s_q + (i / NB) * QP + i % NB, qrow + (i / NB) * ZS + i % NB);
   }
   if (piece_w) {
     const char* src = reinterpret_cast<const char*>(wrow - offw);
@@ -772,8 +644,9 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
       const int z = i / pw, c = i % pw;
       cp_async16(reinterpret_cast<char*>(s_w + (size_t)z * WP) + 16 * c, src + z * ZS * sizeof(float) + 16 * c);
     }
-  } else if (w1) {
-    for (int i = threadIdx.x; i < N * NB; i += NT) cp_async4(s_w + (i / NB) * WP + i % NB, wrow + (i / NB) * ZS + i % NB);
+  } else if (C::PREF_W && w1) {
+    for (int i = threadIdx.x; i < N * NB; i += NT)
+      if (i % NB < cnt) cp_async4(s_w + (i / NB) * WP + i % NB, wrow + (i / NB) * ZS + i % NB);
   }
   cp_async_commit();
   load_twiddles<N>(s_tw, g_tw);
@@ -787,24 +660,32 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
     mbar_wait(&bar, 0, a.wait_cycles);
     return;
   }
-  if (w2) {
+  if (C::PREF_W && w2) {
     for (int i = threadIdx.x; i < N * NB; i += NT)
-      s_w[(i / NB) * WP + offw + i % NB] *= __ldg(w2 + (size_t)(i / NB) * ZS + (size_t)ky * NH + i % NB);
+      if (i % NB < cnt) s_w[(i / NB) * WP + offw + i % NB] *= __ldg(w2 + (size_t)(i / NB) * ZS + (size_t)ky * NH + k0 + i % NB);
   }
   __syncthreads();
 
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
   const int kl = team;  // consecutive columns for the teams of a warp
+  const int kx = k0 + kl;
   const bool weighted = w1 != nullptr;
-  const double hw = (kl == 0 || 2 * kl == N) ? 1.0 : 2.0;
+  const double hw = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
   double en = 0.0;
   {
     const float2* sq = s_q + offq + kl;
     const float* sw = s_w + offw + kl;
-    fft_line_fwd_mul_inv<N, P, 1>(tile + kl, TP, lane, s_tw, kl < NB, [&](int z, float2 rr) {
-      const bool origin = z == 0 && ky == 0 && kl == 0;
+    fft_line_fwd_mul_inv<N, P, 1>(tile + kl, TP, lane, s_tw, kl < cnt, [&](int z, float2 rr) {
+      const bool origin = z == 0 && ky == 0 && kx == 0;
       if (weighted) {
-        const float wv = sw[z * WP];
+        float wv;
+        if constexpr (C::PREF_W) {
+          wv = sw[z * WP];
+        } else {  // read when the product is formed (128^3: no weight slab, three CTAs per SM)
+          const size_t gi = (size_t)z * ZS + (size_t)ky * NH + kx;
+          wv = __ldg(w1 + gi);
+          if (w2) wv *= __ldg(w2 + gi);
+        }
         rr.x *= wv;
         rr.y *= wv;
         if (!origin) en += hw * ((double)rr.x * rr.x + (double)rr.y * rr.y);
@@ -818,9 +699,10 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
     if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
   }
   __syncthreads();
-  float2* dst = a.s2 + (size_t)e * w * ZS + (size_t)ky * NH;
+  float2* dst = a.s2 + (size_t)e * w * ZS + (size_t)ky * NH + k0;
   for (int i = threadIdx.x; i < w * NB; i += NT) {
     const int j = i / NB, c = i % NB;
+    if (c >= cnt) continue;
     const int z = (j - a.radius + N) % N;
     dst[(size_t)j * ZS + c] = tile[lpos<1>(z) * TP + c];
   }
@@ -830,11 +712,7 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
 template <int N>
 __global__ void __launch_bounds__(SearchCfg<N>::NT_B, N <= 64 ? 4 : 0) k_search_z_mul(const SearchChunkArgs a,
                                                                       const float2* __restrict__ g_tw) {
-  if constexpr (SearchCfg<N>::BULK_B) {
-    z_mul_bulk<N>(a, g_tw);
-  } else {
-    z_mul_staged<N>(a, g_tw);
-  }
+  z_mul_bulk<N>(a, g_tw);
 }
 
 // ------------------------------------------------------------------ pass C
