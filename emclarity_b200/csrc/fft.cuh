@@ -378,6 +378,19 @@ template <int L, int SIGN, int P, int PAD, int S>
 struct StageChain<L, SIGN, P, PAD, S, L> {
   static __device__ __forceinline__ void run(float2*, int, int, const float2*, bool, const TwChain<L, P, S, L>*) {}
 };
+// Stages S .. LAST-1 only (NS = product of the radices before S).
+template <int L, int SIGN, int P, int PAD, int S, int NS, int LAST>
+struct ForwardMidStages {
+  static __device__ __forceinline__ void run(float2* buf, int stride, int lane, const float2* tw, bool active,
+                                             const TwChain<L, P, S, NS>* tc) {
+    if constexpr (S < LAST) {
+      constexpr int R = radix_of(L, S);
+      stockham_stage<L, R, NS, SIGN, P, PAD, S>(buf, stride, lane, tw, active, tc ? &tc->st : nullptr);
+      ForwardMidStages<L, SIGN, P, PAD, S + 1, NS * R, LAST>::run(buf, stride, lane, tw, active,
+                                                                 tc ? &tc->next : nullptr);
+    }
+  }
+};
 
 // First stage (NS = 1, no twiddles) with its inputs produced by ld(i) -- element i of the line
 // -- instead of loaded from the buffer, so a caller that builds the line (packing two real rows,
@@ -423,7 +436,70 @@ __device__ __forceinline__ void fft_line_in(const Ld& ld, float2* buf, int strid
 }
 
 // Number of Stockham stages of a length-L plan and the product of the radices before stage s.
-__host__ __device__ constexpr int n_stages(int L, int s = 0) { return radix_of(L, s) <= 1 ? s : n_stages(L, s + 1); }
+__host__ __device__ constexpr int n_stages(int L, int s = 0);
+__host__ __device__ constexpr int radix_product(int L, int s);
+
+// The last Stockham stage of a length-L plan for teams of P lanes: radix RL, NSL = L / RL
+// butterflies (the product of the earlier radices), PER butterflies per lane.
+template <int L, int P>
+struct LastStage {
+  static constexpr int S = n_stages(L) - 1;
+  static constexpr int RL = radix_of(L, S);
+  static constexpr int NSL = L / RL;
+  static constexpr int PER = (NSL + P - 1) / P;
+};
+
+// Register twiddles of stage S of a chain (nullptr when the chain holds none for it).
+template <int S, int L, int P, int S0, int NS>
+__device__ __forceinline__ const StageTw<L, P, S, radix_product(L, S)>* stage_tw(const TwChain<L, P, S0, NS>* tc) {
+  if constexpr (S0 == S) {
+    return tc ? &tc->st : nullptr;
+  } else {
+    return stage_tw<S>(tc ? &tc->next : (const TwChain<L, P, S0 + 1, NS * radix_of(L, S0)>*)nullptr);
+  }
+}
+
+// FFT of a line whose elements come from ld(i), like fft_line_in, with the last stage left in
+// registers: on return v[b][r] holds element (lane + b P) + NSL r of the transform for every
+// butterfly lane + b P < NSL of an active lane (LastStage<L, P>); buf holds the earlier stages'
+// scratch.  The caller synchronises the team before buf is written again.
+template <int L, int SIGN, int P, int PAD, class Ld>
+__device__ __forceinline__ void fft_line_in_regs(const Ld& ld, float2* buf, int stride, int lane, const float2* tw,
+                                                 bool active, const LineTw<L, P>* tc,
+                                                 float2 (&v)[LastStage<L, P>::PER][LastStage<L, P>::RL]) {
+  using LS = LastStage<L, P>;
+  constexpr int R0 = radix_of(L, 0);
+  static_assert(LS::S >= 1, "at least two stages");
+  stockham_first_stage_in<L, R0, SIGN, P, PAD>(ld, buf, stride, lane, active);
+  if constexpr (LS::S > 1) {
+    // stages 1 .. S-1 in shared memory
+    ForwardMidStages<L, SIGN, P, PAD, 1, R0, LS::S>::run(buf, stride, lane, tw, active, tc ? &tc->next : nullptr);
+  }
+  const auto* cache = stage_tw<LS::S>(tc);
+#pragma unroll
+  for (int b = 0; b < LS::PER; ++b) {
+    const int j = lane + b * P;
+    if (active && (LS::PER * P == LS::NSL || j < LS::NSL)) {
+#pragma unroll
+      for (int r = 0; r < LS::RL; ++r) v[b][r] = buf[lpos<PAD>(j + r * LS::NSL) * stride];
+      if constexpr (StageTw<L, P, LS::S, LS::NSL>::kOn) {
+        if (cache) {
+#pragma unroll
+          for (int r = 1; r < LS::RL; ++r)
+            v[b][r] = SIGN < 0 ? cmul(v[b][r], cache->w[b][r - 1]) : cmulc(v[b][r], cache->w[b][r - 1]);
+        } else {
+#pragma unroll
+          for (int r = 1; r < LS::RL; ++r) v[b][r] = cmul(v[b][r], twiddle<SIGN>(tw, (r * j) % L));
+        }
+      } else {
+#pragma unroll
+        for (int r = 1; r < LS::RL; ++r) v[b][r] = cmul(v[b][r], twiddle<SIGN>(tw, (r * j) % L));
+      }
+      Dft<LS::RL, SIGN>::run(v[b]);
+    }
+  }
+}
+__host__ __device__ constexpr int n_stages(int L, int s) { return radix_of(L, s) <= 1 ? s : n_stages(L, s + 1); }
 __host__ __device__ constexpr int radix_product(int L, int s) { return s == 0 ? 1 : radix_of(L, s - 1) * radix_product(L, s - 1); }
 
 // Forward stages S .. LAST-1 of a length-L line (NS = product of the radices before S).

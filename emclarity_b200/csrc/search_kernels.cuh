@@ -509,20 +509,43 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
       const size_t row_a = (size_t)zl * PY + lpos<1>(ya);
       const float* ra = fplanes + row_a * (2 * NH);
       const float* rb = ra + 2 * NH;
-      fft_line_in<N, -1, P, 1>([&](int n) { return make_float2(ra[n], rb[n]); }, buf, 1, lane, s_tw, active, &tc);
-      if (active) {
-        // columns 0 and N/2 of a row transform are real: row a's pair goes to slot 0 of row a,
-        // row b's to slot 0 of row b, as (X(0), X(N/2)), so the y pass needs N/2 complex lines
-        float2* oa = planes + row_a * NH;
-        float2* ob = oa + NH;
-        for (int k = lane; k < NH - 1; k += P) {
-          const float2 zk = buf[lpos<1>(k)], zm = buf[lpos<1>(k ? N - k : N / 2)];
-          if (k == 0) {
-            oa[0] = make_float2(zk.x, zm.x);
-            ob[0] = make_float2(zk.y, zm.y);
-          } else {
-            oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-            ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+      // the transform's last stage stays in registers: v[b][r] = Z(k), k = lane + b P + NSL r
+      using LS = LastStage<N, P>;
+      float2 v[LS::PER][LS::RL];
+      fft_line_in_regs<N, -1, P, 1>([&](int n) { return make_float2(ra[n], rb[n]); }, buf, 1, lane, s_tw, active,
+                                    &tc, v);
+      // Hermitian split of the two packed rows: Z(N - k) sits on lane (P - lane) mod P of the team,
+      // butterfly block NSL/P - 1 - b, index RL - 1 - r (lane 0 holds its own partners and Z(N/2)).
+      // Columns 0 and N/2 of a row transform are real: row a's pair goes to slot 0 of row a, row
+      // b's to slot 0 of row b, as (X(0), X(N/2)), so the y pass needs N/2 complex lines.
+      constexpr int NB_P = LS::NSL / P;
+      constexpr int JH = (N / 2) % LS::NSL, BH = JH / P, RH = (N / 2) / LS::NSL;
+      static_assert(JH % P == 0 && LS::NSL % P == 0, "Z(N/2) on lane 0");
+      const int wl = threadIdx.x & 31;
+      const int src = (wl & ~(P - 1)) | ((P - lane) & (P - 1));
+      float2* oa = planes + row_a * NH;
+      float2* ob = oa + NH;
+#pragma unroll
+      for (int b = 0; b < LS::PER; ++b) {
+#pragma unroll
+        for (int r = 0; r < LS::RL; ++r) {
+          if (b * P + r * LS::NSL < N / 2) {
+            const float2 sent = v[NB_P - 1 - b][LS::RL - 1 - r];
+            float2 zm = make_float2(__shfl_sync(0xffffffffu, sent.x, src), __shfl_sync(0xffffffffu, sent.y, src));
+            if (lane == 0) {
+              zm = b > 0 ? v[(NB_P - b) % LS::PER][LS::RL - 1 - r] : (r > 0 ? v[0][(LS::RL - r) % LS::RL] : v[BH][RH]);
+            }
+            const float2 zk = v[b][r];
+            const int k = lane + b * P + r * LS::NSL;
+            if (active && k < N / 2) {
+              if (k == 0) {
+                oa[0] = make_float2(zk.x, zm.x);
+                ob[0] = make_float2(zk.y, zm.y);
+              } else {
+                oa[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+                ob[k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+              }
+            }
           }
         }
       }
