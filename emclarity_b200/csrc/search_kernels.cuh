@@ -694,7 +694,9 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
   const int kx = k0 + kl;
   const bool weighted = w1 != nullptr;
   const double hw = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
-  double en = 0.0;
+  // E_R: each lane's |.|^2 over its elements of the line (8 to 16) in FP32, the lanes' partial sums
+  // then accumulated in FP64 (block_sum and the evaluation's atomicAdd)
+  float ef = 0.f;
   {
     const float2* sq = s_q + offq + kl;
     const float* sw = s_w + offw + kl;
@@ -711,14 +713,14 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
         }
         rr.x *= wv;
         rr.y *= wv;
-        if (!origin) en += hw * ((double)rr.x * rr.x + (double)rr.y * rr.y);
+        if (!origin) ef = fmaf(rr.x, rr.x, fmaf(rr.y, rr.y, ef));
       }
       const float2 x = cmulc(sq[z * QP], rr);
       return origin ? make_float2(0.f, 0.f) : x;
     });
   }
   if (weighted) {
-    double t = block_sum(en, red);
+    double t = block_sum(hw * (double)ef, red);
     if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
   }
   __syncthreads();
