@@ -111,6 +111,11 @@ __device__ __forceinline__ void bulk_copy_g2s(void* smem_dst, const void* gmem_s
                "l"(gmem_src), "r"(bytes), "r"(b)
                : "memory");
 }
+// Orders this thread's earlier generic-proxy accesses to shared memory before later asynchronous-
+// proxy ones (a bulk copy into a buffer the CTA has just read or written).
+__device__ __forceinline__ void fence_proxy_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
 // Waits for phase `parity` of the barrier to complete, giving up after about `max_cycles` SM
 // clock cycles.  Returns whether it completed.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, long long max_cycles) {

@@ -143,7 +143,7 @@ static emc_status launch_chunk(int g, const SearchChunkArgs& a, cudaStream_t st,
   if (ev) EMC_CUDA(cudaEventRecord(ev[0], st));
   EMC_TRY((launch_fwd<N, T>(g, a, tw, st)));
   if (ev) EMC_CUDA(cudaEventRecord(ev[1], st));
-  k_search_z_mul<N><<<dim3(C::GRID_BX, a.n_items), C::NT_B, C::SMEM_B, st>>>(a, tw);
+  k_search_z_mul<N><<<dim3(C::GRID_BX, (a.n_items + C::EVALS_B - 1) / C::EVALS_B), C::NT_B, C::SMEM_B, st>>>(a, tw);
   EMC_LAUNCH_CHECK();
   if (ev) EMC_CUDA(cudaEventRecord(ev[2], st));
   k_search_inv_peak<N><<<dim3(w, a.n_items), C::NT_BC, C::SMEM_C, st>>>(a, tw);

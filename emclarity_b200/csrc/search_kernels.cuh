@@ -289,6 +289,10 @@ struct SearchCfg {
   static constexpr int NT_B = ((NHB * P + 31) / 32) * 32;
   static constexpr int TEAMS_B = NT_B / P;
   static constexpr int GRID_BX = N * KS_B;
+  // evaluations per pass-B CTA (grid y = ceil(items / EVALS_B)): two at 64^3, where the second reuses
+  // the particle's spectrum and weight rows (pass B 321.5 -> 309.9 us per 534-evaluation chunk); at
+  // 96^3 the second evaluation's registers cost more than the reuse gave (502 -> 509 us)
+  static constexpr int EVALS_B = N <= 64 ? 2 : 1;
   static constexpr int TPB_K = NHB + 1 + (NHB + 1) % 2;                 // >= NHB + 1, even
   static constexpr int QP_K = TPB_K;
   static constexpr int WP_K = ((NHB + 3 + 3) / 4) * 4;                   // >= NHB + 3, 16-byte rows
@@ -620,116 +624,138 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
   __shared__ double red[32];
   __shared__ uint64_t bar;
 
-  const int e = blockIdx.y;
-  if (e >= a.n_items) return;
+  // EVALS_B consecutive evaluations of the chunk (consecutive orientations of one particle, but at
+  // a particle boundary): the spectrum and weight rows are copied again only when the particle changes
+  const int e_first = blockIdx.y * C::EVALS_B;
+  if (e_first >= a.n_items) return;
+  const int ne = min(C::EVALS_B, a.n_items - e_first);
   // this CTA's columns: kx in [k0, k0 + cnt)
   const int ky = blockIdx.x / C::KS_B;
   const int k0 = (int)(blockIdx.x % C::KS_B) * NB;
   const int cnt = min(NB, NH - k0);
-  const EvalItem it = a.items[e];
-  const DevParticle& pt = a.parts[it.particle];
-  // weights on the rotated reference (BH_multi_xcf_Translational_2.m:35-38): the particle's wdgMask
-  // and the reference's bandpass wref; the first present one is copied, a second folded into it
-  const float* __restrict__ wref = a.refs[pt.ref].wref;
-  const float* __restrict__ w1 = pt.wedge ? pt.wedge : wref;
-  const float* __restrict__ w2 = pt.wedge ? wref : nullptr;
   const int w = 2 * a.radius + 1;
   constexpr size_t ZS = (size_t)N * NH;  // elements per z step of the spectrum and weight
-  const float2* slab = a.s1 + (size_t)e * C::S1_EVAL + (size_t)blockIdx.x * C::PY * TP;
-  const float2* qrow = pt.spec + (size_t)ky * NH + k0;
-  const float* wrow = w1 ? w1 + (size_t)ky * NH + k0 : nullptr;
-  const bool piece_q = ((uintptr_t)pt.spec & 15) == 0;
-  const bool piece_w = C::PREF_W && w1 && ((uintptr_t)w1 & 15) == 0;
-  // row offsets (elements) from the 16-byte boundary below each row start, and 16-byte pieces per row
-  const int offq = piece_q ? (int)(((uintptr_t)qrow & 15) >> 3) : 0;
-  const int offw = piece_w ? (int)(((uintptr_t)wrow & 15) >> 2) : 0;
-  const int pq = ((offq + cnt) * 8 + 15) >> 4;
-  const int pw = ((offw + cnt) * 4 + 15) >> 4;
-
-  if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    mbar_arrive_expect_tx(&bar, SLAB_BYTES + a.phantom_tx);
-    bulk_copy_g2s(tile, slab, SLAB_BYTES, &bar);
-  }
-  if (piece_q) {
-    const char* src = reinterpret_cast<const char*>(qrow - offq);
-    for (int i = threadIdx.x; i < N * pq; i += NT) {
-      const int z = i / pq, c = i % pq;
-      cp_async16(reinterpret_cast<char*>(s_q + (size_t)z * QP) + 16 * c, src + z * ZS * sizeof(float2) + 16 * c);
-    }
-  } else {
-    for (int i = threadIdx.x; i < N * NB; i += NT)
-      if (i % NB < cnt) cp_async8(s_q + (i / NB) * QP + i % NB, qrow + (i / NB) * ZS + i % NB);
-  }
-  if (piece_w) {
-    const char* src = reinterpret_cast<const char*>(wrow - offw);
-    for (int i = threadIdx.x; i < N * pw; i += NT) {
-      const int z = i / pw, c = i % pw;
-      cp_async16(reinterpret_cast<char*>(s_w + (size_t)z * WP) + 16 * c, src + z * ZS * sizeof(float) + 16 * c);
-    }
-  } else if (C::PREF_W && w1) {
-    for (int i = threadIdx.x; i < N * NB; i += NT)
-      if (i % NB < cnt) cp_async4(s_w + (i / NB) * WP + i % NB, wrow + (i / NB) * ZS + i % NB);
-  }
-  cp_async_commit();
-  load_twiddles<N>(s_tw, g_tw);
-  cp_async_wait<0>();
-  __syncthreads();  // the barrier is initialised before anyone polls it
-  // the next barrier also publishes the cp.async pieces; the whole CTA takes the same branch
-  const bool arrived = mbar_wait(&bar, 0, a.wait_cycles);
-  if (__syncthreads_or(!arrived)) {
-    // the copies did not complete in time: report, give them a second bounded wait, and leave
-    if (threadIdx.x == 0 && a.status) atomicOr(a.status, kStatusWaitTimeout);
-    mbar_wait(&bar, 0, a.wait_cycles);
-    return;
-  }
-  if (C::PREF_W && w2) {
-    for (int i = threadIdx.x; i < N * NB; i += NT)
-      if (i % NB < cnt) s_w[(i / NB) * WP + offw + i % NB] *= __ldg(w2 + (size_t)(i / NB) * ZS + (size_t)ky * NH + k0 + i % NB);
-  }
-  __syncthreads();
-
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
   const int kl = team;  // consecutive columns for the teams of a warp
   const int kx = k0 + kl;
-  const bool weighted = w1 != nullptr;
   const double hw = (kx == 0 || 2 * kx == N) ? 1.0 : 2.0;
-  // E_R: each lane's |.|^2 over its elements of the line (8 to 16) in FP32, the lanes' partial sums
-  // then accumulated in FP64 (block_sum and the evaluation's atomicAdd)
-  float ef = 0.f;
-  {
-    const float2* sq = s_q + offq + kl;
-    const float* sw = s_w + offw + kl;
-    fft_line_fwd_mul_inv<N, P, 1>(tile + kl, TP, lane, s_tw, kl < cnt, [&](int z, float2 rr) {
-      const bool origin = z == 0 && ky == 0 && kx == 0;
-      if (weighted) {
-        float wv;
-        if constexpr (C::PREF_W) {
-          wv = sw[z * WP];
-        } else {  // read when the product is formed (128^3: no weight slab, three CTAs per SM)
-          const size_t gi = (size_t)z * ZS + (size_t)ky * NH + kx;
-          wv = __ldg(w1 + gi);
-          if (w2) wv *= __ldg(w2 + gi);
+
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  load_twiddles<N>(s_tw, g_tw);
+  __syncthreads();  // the barrier is initialised before anyone polls it
+  int loaded = -1;  // particle whose spectrum and weight rows are in shared memory
+  // one evaluation; returns false when its copy timed out (the CTA then leaves)
+  auto one = [&](const int k) -> bool {
+    const int e = e_first + k;
+    const EvalItem it = a.items[e];
+    const DevParticle& pt = a.parts[it.particle];
+    // weights on the rotated reference (BH_multi_xcf_Translational_2.m:35-38): the particle's
+    // wdgMask and the reference's bandpass wref; the first present one is copied, a second folded in
+    const float* __restrict__ wref = a.refs[pt.ref].wref;
+    const float* __restrict__ w1 = pt.wedge ? pt.wedge : wref;
+    const float* __restrict__ w2 = pt.wedge ? wref : nullptr;
+    const float2* qrow = pt.spec + (size_t)ky * NH + k0;
+    const float* wrow = w1 ? w1 + (size_t)ky * NH + k0 : nullptr;
+    const bool piece_q = ((uintptr_t)pt.spec & 15) == 0;
+    const bool piece_w = C::PREF_W && w1 && ((uintptr_t)w1 & 15) == 0;
+    // row offsets (elements) from the 16-byte boundary below each row start, 16-byte pieces per row
+    const int offq = piece_q ? (int)(((uintptr_t)qrow & 15) >> 3) : 0;
+    const int offw = piece_w ? (int)(((uintptr_t)wrow & 15) >> 2) : 0;
+    const bool reload = it.particle != loaded;  // the same for the whole CTA
+    if (k > 0) __syncthreads();  // the previous evaluation is done with the tile (and the rows)
+    if (threadIdx.x == 0) {
+      if (k > 0) fence_proxy_async_shared();
+      mbar_arrive_expect_tx(&bar, SLAB_BYTES + a.phantom_tx);
+      bulk_copy_g2s(tile, a.s1 + (size_t)e * C::S1_EVAL + (size_t)blockIdx.x * C::PY * TP, SLAB_BYTES, &bar);
+    }
+    if (reload) {
+      const int pq = ((offq + cnt) * 8 + 15) >> 4;
+      const int pw = ((offw + cnt) * 4 + 15) >> 4;
+      if (piece_q) {
+        const char* src = reinterpret_cast<const char*>(qrow - offq);
+        for (int i = threadIdx.x; i < N * pq; i += NT) {
+          const int z = i / pq, c = i % pq;
+          cp_async16(reinterpret_cast<char*>(s_q + (size_t)z * QP) + 16 * c, src + z * ZS * sizeof(float2) + 16 * c);
         }
-        rr.x *= wv;
-        rr.y *= wv;
-        if (!origin) ef = fmaf(rr.x, rr.x, fmaf(rr.y, rr.y, ef));
+      } else {
+        for (int i = threadIdx.x; i < N * NB; i += NT)
+          if (i % NB < cnt) cp_async8(s_q + (i / NB) * QP + i % NB, qrow + (i / NB) * ZS + i % NB);
       }
-      const float2 x = cmulc(sq[z * QP], rr);
-      return origin ? make_float2(0.f, 0.f) : x;
-    });
-  }
-  if (weighted) {
-    double t = block_sum(hw * (double)ef, red);
-    if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
-  }
-  __syncthreads();
-  float2* dst = a.s2 + (size_t)e * w * ZS + (size_t)ky * NH + k0;
-  for (int i = threadIdx.x; i < w * NB; i += NT) {
-    const int j = i / NB, c = i % NB;
-    if (c >= cnt) continue;
-    const int z = (j - a.radius + N) % N;
-    dst[(size_t)j * ZS + c] = tile[lpos<1>(z) * TP + c];
+      if (piece_w) {
+        const char* src = reinterpret_cast<const char*>(wrow - offw);
+        for (int i = threadIdx.x; i < N * pw; i += NT) {
+          const int z = i / pw, c = i % pw;
+          cp_async16(reinterpret_cast<char*>(s_w + (size_t)z * WP) + 16 * c, src + z * ZS * sizeof(float) + 16 * c);
+        }
+      } else if (C::PREF_W && w1) {
+        for (int i = threadIdx.x; i < N * NB; i += NT)
+          if (i % NB < cnt) cp_async4(s_w + (i / NB) * WP + i % NB, wrow + (i / NB) * ZS + i % NB);
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+    }
+    // the next barrier also publishes the cp.async pieces; the whole CTA takes the same branch
+    const bool arrived = mbar_wait(&bar, (unsigned)(k & 1), a.wait_cycles);
+    if (__syncthreads_or(!arrived)) {
+      // the copy did not complete in time: report, give it a second bounded wait, and leave
+      if (threadIdx.x == 0 && a.status) atomicOr(a.status, kStatusWaitTimeout);
+      mbar_wait(&bar, (unsigned)(k & 1), a.wait_cycles);
+      return false;
+    }
+    if (reload) {
+      if (C::PREF_W && w2) {
+        for (int i = threadIdx.x; i < N * NB; i += NT)
+          if (i % NB < cnt)
+            s_w[(i / NB) * WP + offw + i % NB] *= __ldg(w2 + (size_t)(i / NB) * ZS + (size_t)ky * NH + k0 + i % NB);
+        __syncthreads();
+      }
+      loaded = it.particle;
+    }
+
+    const bool weighted = w1 != nullptr;
+    // E_R: each lane's |.|^2 over its elements of the line (8 to 16) in FP32, the lanes' partial
+    // sums then accumulated in FP64 (block_sum and the evaluation's atomicAdd)
+    float ef = 0.f;
+    {
+      const float2* sq = s_q + offq + kl;
+      const float* sw = s_w + offw + kl;
+      fft_line_fwd_mul_inv<N, P, 1>(tile + kl, TP, lane, s_tw, kl < cnt, [&](int z, float2 rr) {
+        const bool origin = z == 0 && ky == 0 && kx == 0;
+        if (weighted) {
+          float wv;
+          if constexpr (C::PREF_W) {
+            wv = sw[z * WP];
+          } else {  // read when the product is formed (128^3: no weight slab, three CTAs per SM)
+            const size_t gi = (size_t)z * ZS + (size_t)ky * NH + kx;
+            wv = __ldg(w1 + gi);
+            if (w2) wv *= __ldg(w2 + gi);
+          }
+          rr.x *= wv;
+          rr.y *= wv;
+          if (!origin) ef = fmaf(rr.x, rr.x, fmaf(rr.y, rr.y, ef));
+        }
+        const float2 x = cmulc(sq[z * QP], rr);
+        return origin ? make_float2(0.f, 0.f) : x;
+      });
+    }
+    if (weighted) {
+      double t = block_sum(hw * (double)ef, red);
+      if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
+    }
+    __syncthreads();
+    float2* dst = a.s2 + (size_t)e * w * ZS + (size_t)ky * NH + k0;
+    for (int i = threadIdx.x; i < w * NB; i += NT) {
+      const int j = i / NB, c = i % NB;
+      if (c >= cnt) continue;
+      const int z = (j - a.radius + N) % N;
+      dst[(size_t)j * ZS + c] = tile[lpos<1>(z) * TP + c];
+    }
+    return true;
+  };
+  static_assert(C::EVALS_B == 1 || C::EVALS_B == 2, "one or two evaluations per CTA");
+  if (!one(0)) return;
+  if constexpr (C::EVALS_B > 1) {
+    if (ne > 1) one(1);
   }
 }
 

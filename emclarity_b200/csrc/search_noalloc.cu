@@ -166,7 +166,7 @@ emc_status run_chunks(const SearchChunkArgs& proto, int n_orient, int chunk, con
     EMC_CUDA(cudaMemsetAsync(a.stats, 0, sizeof(EvalStats) * a.n_items, st));
     EMC_CUDA(cudaMemsetAsync(a.keys, 0, sizeof(unsigned long long) * a.n_items, st));
     k_search_fwd_xy<N, float><<<dim3(N / C::G, a.n_items), C::NT_A, C::SMEM_A, st>>>(a, tw);
-    k_search_z_mul<N><<<dim3(C::GRID_BX, a.n_items), C::NT_B, C::SMEM_B, st>>>(a, tw);
+    k_search_z_mul<N><<<dim3(C::GRID_BX, (a.n_items + C::EVALS_B - 1) / C::EVALS_B), C::NT_B, C::SMEM_B, st>>>(a, tw);
     k_search_inv_peak<N><<<dim3(w, a.n_items), C::NT_BC, C::SMEM_C, st>>>(a, tw);
     k_noalloc_decode<<<(a.n_items + 127) / 128, 128, 0, st>>>(a, N, res, best);
     EMC_LAUNCH_CHECK();

@@ -157,14 +157,16 @@ __global__ void __launch_bounds__(P * TT, zfused_min_blocks(L, P, TT)) k_ts_zfus
   const bool line_active = i < inner;
   const double hw = ((int)(i % g.nxh) == 0 || 2 * (int)(i % g.nxh) == g.nx) ? 1.0 : 2.0;
   // forward z transform of the template planes, X = T .* conj(G) and its statistics in registers,
-  // inverse z transform (fft_line_fwd_mul_inv)
-  double e = 0.0;
+  // inverse z transform (fft_line_fwd_mul_inv).  Each lane sums its elements' |X|^2 in FP32 (L / P
+  // of them), the lanes' sums are accumulated in FP64.
+  float ef = 0.f;
   fft_line_fwd_mul_inv<L, P, PAD>(tile + team, TP, lane, s_tw, line_active, [&](int n, float2 gz) {
     const float2 x = cmulc(s_t[n * TT + team], gz);
-    e += hw * ((double)x.x * x.x + (double)x.y * x.y);
+    ef = fmaf(x.x, x.x, fmaf(x.y, x.y, ef));
     if (i == 0 && n == 0) stats[1] = (double)x.x;
     return x;
   });
+  double e = hw * (double)ef;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
