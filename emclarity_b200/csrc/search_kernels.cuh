@@ -289,10 +289,11 @@ struct SearchCfg {
   static constexpr int NT_B = ((NHB * P + 31) / 32) * 32;
   static constexpr int TEAMS_B = NT_B / P;
   static constexpr int GRID_BX = N * KS_B;
-  // evaluations per pass-B CTA (grid y = ceil(items / EVALS_B)): two at 64^3, where the second reuses
-  // the particle's spectrum and weight rows (pass B 321.5 -> 309.9 us per 534-evaluation chunk); at
-  // 96^3 the second evaluation's registers cost more than the reuse gave (502 -> 509 us)
-  static constexpr int EVALS_B = N <= 64 ? 2 : 1;
+  // evaluations per pass-B CTA (grid y = ceil(items / EVALS_B)): four at 64^3, where the later ones
+  // reuse the particle's spectrum and weight rows (pass B 321.5 -> 309.9 us per 534-evaluation chunk
+  // with two, 302.1 with four); at 96^3 a second evaluation's registers cost more than the reuse gave
+  // (502 -> 509 us)
+  static constexpr int EVALS_B = N <= 64 ? 4 : 1;
   static constexpr int TPB_K = NHB + 1 + (NHB + 1) % 2;                 // >= NHB + 1, even
   static constexpr int QP_K = TPB_K;
   static constexpr int WP_K = ((NHB + 3 + 3) / 4) * 4;                   // >= NHB + 3, 16-byte rows
@@ -752,10 +753,17 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
     }
     return true;
   };
-  static_assert(C::EVALS_B == 1 || C::EVALS_B == 2, "one or two evaluations per CTA");
+  // straight-line calls (a rolled loop over evaluations let the compiler hoist the transforms'
+  // addressing out of it and spill)
+  static_assert(C::EVALS_B == 1 || C::EVALS_B == 2 || C::EVALS_B == 4, "1, 2 or 4 evaluations per CTA");
   if (!one(0)) return;
   if constexpr (C::EVALS_B > 1) {
-    if (ne > 1) one(1);
+    if (ne < 2 || !one(1)) return;
+  }
+  if constexpr (C::EVALS_B > 2) {
+    if (ne < 3 || !one(2)) return;
+    if (ne < 4) return;
+    one(3);
   }
 }
 
