@@ -264,7 +264,14 @@ struct SearchCfg {
   static constexpr int TEAMS_LA = N <= 64 ? TEAMS_A : 16;
   static constexpr int TEAMS_LC = 16;  // (2 r + 1 + 1) / 2 <= 16 row pairs for r <= 15
   static_assert(TEAMS_BC >= TEAMS_LC, "pass C needs a team for every line buffer");
-  static constexpr size_t SMEM_A = sizeof(float2) * ((size_t)G * PY * NH + (size_t)TEAMS_LA * LP + N) + 64;
+  // Plane pitch of pass A (float2): nh rounded up to even.  With the even pitch the y transform's
+  // teams take consecutive columns, the row-pair R2C's four teams of a warp take the pairs
+  // q, q+2, q+1, q+3 of a group of four, and a bank model of every access puts each half-warp's
+  // two teams on complementary banks in the R2C's reads and writes and in every y-transform stage
+  // (64^3: 512 -> 256 R2C wavefronts per CTA; 96^3 / 128^3 also 3456 -> 2016 / 4096 -> 2560 in the
+  // y transform); the slab store then reads column pairs as 16-byte words.
+  static constexpr int PA = NH + (NH & 1);
+  static constexpr size_t SMEM_A = sizeof(float2) * ((size_t)G * PY * PA + (size_t)TEAMS_LA * LP + N) + 64;
   // resident pass-A CTAs per SM that shared memory allows (228 KB per SM, 1 KB reserved per CTA),
   // and the target the register budget is capped for: 5 at 64^3 with one plane per CTA (48
   // registers, a 12-byte spill; 863.7 us per 602-evaluation chunk against 875.2 at the compiler's
@@ -406,7 +413,7 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
 #pragma unroll
     for (int ru = 0; ru < RU; ++ru) {
       const int row = r0 + ru, y = row % N, zl = row / N;
-      float* dst = fplanes + ((size_t)zl * C::PY + lpos<1>(y)) * (2 * NH) + lane;
+      float* dst = fplanes + ((size_t)zl * C::PY + lpos<1>(y)) * (2 * C::PA) + lane;
 #pragma unroll
       for (int k = 0; k < SEG; ++k) {
         const int u = ru * SEG + k;
@@ -423,13 +430,6 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
   }
 }
 
-// Column of the y transforms handled as line li of a plane: the N/2 lines are spread so that the
-// teams of a half-warp touch different shared-memory banks (H = N/2, a multiple of 4).
-template <int H>
-__device__ __forceinline__ int spread_half(int li) {
-  return (li % 4) * (H / 4) + li / 4;
-}
-
 // ------------------------------------------------------------------ pass A
 template <int N, typename T, int GG = 0>
 __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB_A) k_search_fwd_xy(const SearchChunkArgs a,
@@ -438,8 +438,9 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
   constexpr int NH = C::NH, G = C::G, P = C::P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int PY = C::PY, LP = C::LP;
-  float2* planes = reinterpret_cast<float2*>(smem_raw);          // [G][PY][NH], row y at lpos<1>(y)
-  float2* lines = planes + (size_t)G * PY * NH;                   // [TEAMS][LP]
+  constexpr int PA = C::PA;
+  float2* planes = reinterpret_cast<float2*>(smem_raw);          // [G][PY][PA], row y at lpos<1>(y)
+  float2* lines = planes + (size_t)G * PY * PA;                   // [TEAMS][LP]
   float2* s_tw = lines + (size_t)C::TEAMS_LA * LP;                 // [N]
   float* s_m = reinterpret_cast<float*>(s_tw + N);                // 9 floats
   __shared__ double red[2][32];
@@ -481,7 +482,7 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
       const float sz = fmaf(m[6], u, fmaf(m[7], v, m[8] * w)) + (float)c;
       float val = sample(a.interp, src, N, N, N, sx, sy, sz);
       if (mask) val *= __ldg(mask + ((long)z * N + y) * N + x);
-      fplanes[((size_t)zl * PY + lpos<1>(y)) * (2 * NH) + x] = val;
+      fplanes[((size_t)zl * PY + lpos<1>(y)) * (2 * PA) + x] = val;
       s1 += (double)val;
       s2 += (double)val * (double)val;
     }
@@ -507,13 +508,13 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
     const bool has_line = team < C::TEAMS_LA;
     float2* buf = lines + (size_t)(has_line ? team : 0) * LP;
     for (int base = 0; base < NPAIRS; base += C::TEAMS_LA) {
-      const int q = base + team;
+      const int q = base + ((team & ~3) | ((team & 1) << 1) | ((team >> 1) & 1));  // pairs 0, 2, 1, 3
       const bool active = has_line && q < NPAIRS;
       // rows 2q, 2q+1 of the slab (same plane, adjacent padded rows since 2q+1 is odd)
       const int zl = (2 * q) / N, ya = (2 * q) % N;
       const size_t row_a = (size_t)zl * PY + lpos<1>(ya);
-      const float* ra = fplanes + row_a * (2 * NH);
-      const float* rb = ra + 2 * NH;
+      const float* ra = fplanes + row_a * (2 * PA);
+      const float* rb = ra + 2 * PA;
       // the transform's last stage stays in registers: v[b][r] = Z(k), k = lane + b P + NSL r
       using LS = LastStage<N, P>;
       float2 v[LS::PER][LS::RL];
@@ -528,8 +529,8 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
       static_assert(JH % P == 0 && LS::NSL % P == 0, "Z(N/2) on lane 0");
       const int wl = threadIdx.x & 31;
       const int src = (wl & ~(P - 1)) | ((P - lane) & (P - 1));
-      float2* oa = planes + row_a * NH;
-      float2* ob = oa + NH;
+      float2* oa = planes + row_a * PA;
+      float2* ob = oa + PA;
 #pragma unroll
       for (int b = 0; b < LS::PER; ++b) {
 #pragma unroll
@@ -564,8 +565,8 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
     for (int base = 0; base < NLINES; base += C::TEAMS_A) {
       const int li = base + team;
       const bool active = li < NLINES;
-      const int zl = active ? li / (N / 2) : 0, kx = active ? spread_half<N / 2>(li % (N / 2)) : 0;
-      fft_line<N, -1, P, 1>(planes + (size_t)zl * PY * NH + kx, NH, lane, s_tw, active, &tc);
+      const int zl = active ? li / (N / 2) : 0, kx = active ? li % (N / 2) : 0;
+      fft_line<N, -1, P, 1>(planes + (size_t)zl * PY * PA + kx, PA, lane, s_tw, active, &tc);
     }
   }
   __syncthreads();
@@ -575,14 +576,14 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
   {
     // F X(kx)(y) of local plane zl: columns 0 and N/2 separated from the packed column 0
     auto s1_value = [&](int zl, int y, int kx) {
-      const float2* pl = planes + (size_t)zl * PY * NH;
+      const float2* pl = planes + (size_t)zl * PY * PA;
       if (kx >= NH) return make_float2(0.f, 0.f);
       if (kx == 0 || kx == NH - 1) {
-        const float2 zp = pl[lpos<1>(y) * NH], zm = pl[lpos<1>((N - y) % N) * NH];
+        const float2 zp = pl[lpos<1>(y) * PA], zm = pl[lpos<1>((N - y) % N) * PA];
         return kx == 0 ? make_float2(0.5f * (zp.x + zm.x), 0.5f * (zp.y - zm.y))
                        : make_float2(0.5f * (zp.y + zm.y), -0.5f * (zp.x - zm.x));
       }
-      return pl[lpos<1>(y) * NH + kx];
+      return pl[lpos<1>(y) * PA + kx];
     };
     float2* dst = a.s1 + (size_t)e * C::S1_EVAL;
     {
@@ -595,8 +596,16 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
         const int part = rem / RP, c = rem % RP;
         const int zl = row / N, y = row % N;
         const int k0 = part * NB + 2 * c;
-        const float2 v0 = 2 * c < NB ? s1_value(zl, y, k0) : make_float2(0.f, 0.f);
-        const float2 v1 = 2 * c + 1 < NB ? s1_value(zl, y, k0 + 1) : make_float2(0.f, 0.f);
+        float2 v0, v1;
+        if (k0 % 2 == 0 && k0 + 1 < NH - 1 && k0 != 0 && 2 * c + 1 < NB) {
+          // an ordinary column pair: one 16-byte read (even pitch, even column)
+          const float4 q4 = *reinterpret_cast<const float4*>(planes + ((size_t)zl * PY + lpos<1>(y)) * PA + k0);
+          v0 = make_float2(q4.x, q4.y);
+          v1 = make_float2(q4.z, q4.w);
+        } else {
+          v0 = 2 * c < NB ? s1_value(zl, y, k0) : make_float2(0.f, 0.f);
+          v1 = 2 * c + 1 < NB ? s1_value(zl, y, k0 + 1) : make_float2(0.f, 0.f);
+        }
         *reinterpret_cast<float4*>(dst + (((size_t)y * KS + part) * PY + lpos<1>(z0 + zl)) * C::TPB_K + 2 * c) =
             make_float4(v0.x, v0.y, v1.x, v1.y);
       }
