@@ -70,47 +70,56 @@ struct CellSampler {
   }
 };
 
+// Each warp takes whole (y, z) rows, its lanes x = lane + 32 k: the row's index arithmetic and the
+// y / z parts of the sample point are formed once per row (the same FP32 operations as per voxel).
 template <typename S>
 __device__ __forceinline__ void adj_accumulate(const S sampler, const float* __restrict__ mask,
                                                const float* __restrict__ h, int n, const AdjPose& sp,
                                                float acc[kAdjSums]) {
   const int c = n / 2;
-  const long nv = (long)n * n * n;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nv; i += (long)gridDim.x * blockDim.x) {
-    const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((long)n * n));
-    const float u0 = (float)(x - c) - sp.t[0], u1 = (float)(y - c) - sp.t[1], u2 = (float)(z - c) - sp.t[2];
-    const float* m = sp.m;
-    const float sx = fmaf(m[0], u0, fmaf(m[1], u1, m[2] * u2)) + (float)c;
-    const float sy = fmaf(m[3], u0, fmaf(m[4], u1, m[5] * u2)) + (float)c;
-    const float sz = fmaf(m[6], u0, fmaf(m[7], u1, m[8] * u2)) + (float)c;
-    const float mk = mask ? __ldg(mask + i) : 1.f;
-    if (mk == 0.f) continue;  // a zero mask voxel adds nothing to any of the sums
-    float g[3];
-    const float v = sampler(sx, sy, sz, g);
-    const float r = mk * v;
-    const float hv = __ldg(h + i);
-    g[0] *= mk; g[1] *= mk; g[2] *= mk;
-    acc[0] += r * hv;
-    acc[1] += r;
-    acc[2] += r * r;
-    // angle derivatives: ds/dk = dm_k u
+  const int lane = threadIdx.x & 31;
+  const int warps = (int)(gridDim.x * (blockDim.x >> 5));
+  const float* m = sp.m;
+  for (int row = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)); row < n * n; row += warps) {
+    const int y = row % n, z = row / n;
+    const float u1 = (float)(y - c) - sp.t[1], u2 = (float)(z - c) - sp.t[2];
+    const float py = fmaf(m[1], u1, m[2] * u2), qy = fmaf(m[4], u1, m[5] * u2), ry = fmaf(m[7], u1, m[8] * u2);
+    const long rbase = (long)row * n;
+    for (int x = lane; x < n; x += 32) {
+      const long i = rbase + x;
+      const float u0 = (float)(x - c) - sp.t[0];
+      const float sx = fmaf(m[0], u0, py) + (float)c;
+      const float sy = fmaf(m[3], u0, qy) + (float)c;
+      const float sz = fmaf(m[6], u0, ry) + (float)c;
+      const float mk = mask ? __ldg(mask + i) : 1.f;
+      if (mk == 0.f) continue;  // a zero mask voxel adds nothing to any of the sums
+      float g[3];
+      const float v = sampler(sx, sy, sz, g);
+      const float r = mk * v;
+      const float hv = __ldg(h + i);
+      g[0] *= mk; g[1] *= mk; g[2] *= mk;
+      acc[0] += r * hv;
+      acc[1] += r;
+      acc[2] += r * r;
+      // angle derivatives: ds/dk = dm_k u
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float* d = sp.dm[k];
-      const float gk = g[0] * fmaf(d[0], u0, fmaf(d[1], u1, d[2] * u2)) +
-                       g[1] * fmaf(d[3], u0, fmaf(d[4], u1, d[5] * u2)) +
-                       g[2] * fmaf(d[6], u0, fmaf(d[7], u1, d[8] * u2));
-      acc[3 + 3 * k] += hv * gk;
-      acc[4 + 3 * k] += r * gk;
-      acc[5 + 3 * k] += gk;
-    }
-    // shift derivatives: ds/dt_j = -M[:, j]
+      for (int k = 0; k < 3; ++k) {
+        const float* d = sp.dm[k];
+        const float gk = g[0] * fmaf(d[0], u0, fmaf(d[1], u1, d[2] * u2)) +
+                         g[1] * fmaf(d[3], u0, fmaf(d[4], u1, d[5] * u2)) +
+                         g[2] * fmaf(d[6], u0, fmaf(d[7], u1, d[8] * u2));
+        acc[3 + 3 * k] += hv * gk;
+        acc[4 + 3 * k] += r * gk;
+        acc[5 + 3 * k] += gk;
+      }
+      // shift derivatives: ds/dt_j = -M[:, j]
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const float gk = -(g[0] * m[j] + g[1] * m[3 + j] + g[2] * m[6 + j]);
-      acc[12 + 3 * j] += hv * gk;
-      acc[13 + 3 * j] += r * gk;
-      acc[14 + 3 * j] += gk;
+      for (int j = 0; j < 3; ++j) {
+        const float gk = -(g[0] * m[j] + g[1] * m[3 + j] + g[2] * m[6 + j]);
+        acc[12 + 3 * j] += hv * gk;
+        acc[13 + 3 * j] += r * gk;
+        acc[14 + 3 * j] += gk;
+      }
     }
   }
 }
