@@ -72,6 +72,11 @@ struct CellSampler {
 
 // Each warp takes whole (y, z) rows, its lanes x = lane + 32 k: the row's index arithmetic and the
 // y / z parts of the sample point are formed once per row (the same FP32 operations as per voxel).
+// Whether an item samples through the trilinear corner cells (else tricubic from the volume).
+__host__ __device__ inline bool adj_uses_cells(const AdjItem& it) {
+  return it.interp == EMC_INTERP_LINEAR && it.cells != nullptr;
+}
+
 template <typename S>
 __device__ __forceinline__ void adj_accumulate(const S sampler, const float* __restrict__ mask,
                                                const float* __restrict__ h, int n, const AdjPose& sp,
@@ -124,32 +129,27 @@ __device__ __forceinline__ void adj_accumulate(const S sampler, const float* __r
   }
 }
 
-// One block-row (blockIdx.y) per item; partial sums reduced in FP64 and added atomically.
+// One block-row (blockIdx.y) per item; partial sums reduced in FP64 and added atomically.  One
+// instantiation per (storage type, sampler): an item whose combination differs leaves at once, so
+// each combination runs with the registers its own sampler needs (the tricubic sampler's gradient
+// needs far more than the trilinear one's).
+template <typename T, bool LIN>
 __global__ void __launch_bounds__(256) k_cc_adjoint(const AdjItem* __restrict__ items, double* __restrict__ sums) {
   __shared__ AdjItem it;
   __shared__ double red[kAdjSums][8];
   const int item = blockIdx.y;
   if (threadIdx.x == 0) it = items[item];
   __syncthreads();
+  constexpr int dtype = sizeof(T) == 4 ? EMC_DTYPE_F32 : EMC_DTYPE_BF16;
+  if (it.dtype != dtype || adj_uses_cells(it) != LIN) return;  // the same for the whole CTA
   float acc[kAdjSums];
 #pragma unroll
   for (int k = 0; k < kAdjSums; ++k) acc[k] = 0.f;
-  const bool lin = it.interp == EMC_INTERP_LINEAR && it.cells;
-  if (it.dtype == EMC_DTYPE_F32) {
-    if (lin)
-      adj_accumulate(CellSampler<float>{reinterpret_cast<const CellT<float>*>(it.cells), it.n}, it.mask, it.h,
-                     it.n, it.pose, acc);
-    else
-      adj_accumulate(CubicSampler<float>{reinterpret_cast<const float*>(it.ref), it.n}, it.mask, it.h, it.n,
-                     it.pose, acc);
-  } else {
-    if (lin)
-      adj_accumulate(CellSampler<__nv_bfloat16>{reinterpret_cast<const CellT<__nv_bfloat16>*>(it.cells), it.n},
-                     it.mask, it.h, it.n, it.pose, acc);
-    else
-      adj_accumulate(CubicSampler<__nv_bfloat16>{reinterpret_cast<const __nv_bfloat16*>(it.ref), it.n}, it.mask,
-                     it.h, it.n, it.pose, acc);
-  }
+  if constexpr (LIN)
+    adj_accumulate(CellSampler<T>{reinterpret_cast<const CellT<T>*>(it.cells), it.n}, it.mask, it.h, it.n, it.pose,
+                   acc);
+  else
+    adj_accumulate(CubicSampler<T>{reinterpret_cast<const T*>(it.ref), it.n}, it.mask, it.h, it.n, it.pose, acc);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
   for (int k = 0; k < kAdjSums; ++k) {
@@ -269,10 +269,18 @@ emc_status emc_cc_adjoint_batch(emc_search_t s, int n_items, const int* ref_ids,
   }
   if (rs == EMC_OK) {
     const long nv = (long)max_n * max_n * max_n;
-    // enough blocks per item to fill the GPU without starving the reduction
-    const long want = std::max<long>(1, (4L * emc::device_sm_count() + n_items - 1) / n_items);
+    // enough blocks per item to fill the GPU twice over (three trilinear CTAs fit per SM) without
+    // starving the reduction
+    const long want = std::max<long>(1, (8L * emc::device_sm_count() + n_items - 1) / n_items);
     const int bx = (int)std::max<long>(1, std::min<long>((nv + 2047) / 2048, want));
-    emc::k_cc_adjoint<<<dim3(bx, n_items), 256, 0, st>>>(d_items, d_sums);
+    // one launch per (storage type, sampler) present among the items
+    bool present[2][2] = {{false, false}, {false, false}};
+    for (const auto& it : items) present[it.dtype == EMC_DTYPE_BF16 ? 1 : 0][emc::adj_uses_cells(it) ? 1 : 0] = true;
+    const dim3 grid(bx, n_items);
+    if (present[0][0]) emc::k_cc_adjoint<float, false><<<grid, 256, 0, st>>>(d_items, d_sums);
+    if (present[0][1]) emc::k_cc_adjoint<float, true><<<grid, 256, 0, st>>>(d_items, d_sums);
+    if (present[1][0]) emc::k_cc_adjoint<__nv_bfloat16, false><<<grid, 256, 0, st>>>(d_items, d_sums);
+    if (present[1][1]) emc::k_cc_adjoint<__nv_bfloat16, true><<<grid, 256, 0, st>>>(d_items, d_sums);
     if (cudaGetLastError() != cudaSuccess ||
         cudaMemcpyAsync(sums.data(), d_sums, sum_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
