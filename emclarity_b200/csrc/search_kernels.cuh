@@ -179,7 +179,7 @@ struct SearchChunkArgs {
   const DevParticle* parts;
   const DevRef* refs;
   const double* dmat;        // [norient][9] column-major defineMatrix([phi,theta,psi-phi],'inv')
-  float2* s1;                // [E][n][n][nh]
+  float2* s1;                // [E][ky][part][lpos(z)][TPB_K] slabs, S1_EVAL per evaluation
   float2* s2;                // [E][w][n][nh]
   EvalStats* stats;          // [E]
   unsigned long long* keys;  // [E]
@@ -328,11 +328,10 @@ __device__ __forceinline__ int spread_kx(int li) {
 }
 
 // Column of line li of a strided-FFT round over `cols` columns of a tile whose row pitch is 1 (mod
-// 16) float2, for teams of 8 lanes: the two teams of a half-warp (lines 2p, 2p+1) get columns 8
-// apart, so their accesses (8 lanes each on 8 consecutive banks of the line's rows) fall on
-// complementary bank halves in every Stockham stage.  Columns past the last complete block of 16
-// keep their own index.  (8 li mod cols put some half-warp pairs 7 or 9 banks apart: 1.33 times
-// the conflict-free wavefronts in pass B's z transforms at 64^3.)
+// 16) float2 (pass C's y transforms), for teams of 8 lanes: the two teams of a half-warp (lines 2p,
+// 2p+1) get columns 8 apart, so their accesses (8 lanes each on 8 consecutive banks of the line's
+// rows) fall on complementary bank halves in every Stockham stage.  Columns past the last complete
+// block of 16 keep their own index.  (8 li mod cols put some half-warp pairs 7 or 9 banks apart.)
 __device__ __forceinline__ int pair_spread(int li, int cols) {
   const int full = (cols >> 4) << 4;
   if (li >= full) return li;
@@ -570,8 +569,9 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
     }
   }
   __syncthreads();
-  // 4. store the slab: S1[e][z0 + zl][y][kx], rows gathered from their padded positions; columns
-  //    0 and N/2 are separated from the packed column 0: with Z = F(X(0) + i X(N/2)),
+  // 4. store plane z0 + zl into the S1 slabs (row lpos(z) of slab (ky = y, column part)), values
+  //    gathered from their padded positions; columns 0 and N/2 are separated from the packed
+  //    column 0: with Z = F(X(0) + i X(N/2)),
   //    F X(0)(y) = (Z(y) + conj Z(-y)) / 2 and F X(N/2)(y) = (Z(y) - conj Z(-y)) / 2i
   {
     // F X(kx)(y) of local plane zl: columns 0 and N/2 separated from the packed column 0
