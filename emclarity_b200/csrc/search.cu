@@ -232,8 +232,7 @@ static emc_status set_attrs_any(int n, int dtype) {
 }
 
 static size_t per_eval_scratch(int n, int radius) {
-  const size_t nh = n / 2 + 1;
-  return sizeof(float2) * (s1_eval_elems(n) + nh * n * (size_t)(2 * radius + 1));
+  return sizeof(float2) * (s1_eval_elems(n) + s2_plane_elems(n) * (size_t)(2 * radius + 1));
 }
 
 // Device buffer that grows on demand.
@@ -788,10 +787,9 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
     // split scratch between S1 and S2 proportionally to the largest chunk of each size
     size_t s1n = 0, s2n = 0;
     for (const Chunk& c : chunks) {
-      const size_t nh = c.n / 2 + 1;
       const int r = effective_radius(s, c.n);
       s1n = std::max(s1n, (size_t)c.count * emc::s1_eval_elems(c.n));
-      s2n = std::max(s2n, (size_t)c.count * (2 * r + 1) * c.n * nh);
+      s2n = std::max(s2n, (size_t)c.count * (2 * r + 1) * emc::s2_plane_elems(c.n));
     }
     for (int k = 0; k < nslots; ++k) {
       EMC_TRY(s->slot[k].s1.reserve(s1n));

@@ -12,7 +12,7 @@
 //                                either weight is set (formed in registers between the
 //                                transforms, fft_line_fwd_mul_inv), inverse FFT along z, keep the
 //                                w output planes |sz| <= r
-//                                -> S2[e][j][ky][kx]                        (w * n * nh c64)
+//                                -> S2[e][j][ky][kx], planes in pass C's tile layout  (~w * n * nh c64)
 //   pass C  (CTA = one sz plane) inverse FFT along y, C2R along x for the w rows |sy| <= r,
 //                                normalise by sqrt(E_R E_P), spherical peak mask,
 //                                argmax -> atomicMax on a 64-bit (cc, -index) key
@@ -180,7 +180,7 @@ struct SearchChunkArgs {
   const DevRef* refs;
   const double* dmat;        // [norient][9] column-major defineMatrix([phi,theta,psi-phi],'inv')
   float2* s1;                // [E][ky][part][lpos(z)][TPB_K] slabs, S1_EVAL per evaluation
-  float2* s2;                // [E][w][n][nh]
+  float2* s2;                // [E][w][lpos(ky)][PC] planes, S2_PLANE each
   EvalStats* stats;          // [E]
   unsigned long long* keys;  // [E]
   int n_items;
@@ -311,32 +311,22 @@ struct SearchCfg {
   static constexpr size_t S1_EVAL = (size_t)N * KS_B * PY * TPB_K;
   static constexpr size_t SMEM_B = sizeof(float2) * ((size_t)PY * TPB_K + (size_t)N * QP_K + N) +
                                    (PREF_W ? sizeof(float) * (size_t)N * WP_K : 0);
-  static constexpr size_t SMEM_C = sizeof(float2) * ((size_t)PY * NH + N + (size_t)TEAMS_LC * LP);
+  // Pass C's tile: S2 planes are written by pass B in this layout (rows ky at lpos<1>(ky), even
+  // pitch PC), so pass C brings a plane in with one bulk copy; its y transforms then take
+  // consecutive columns (a bank model gives the same wavefronts as the odd pitch with paired
+  // columns).
+  static constexpr int PC = NH + (NH & 1);
+  static constexpr size_t S2_PLANE = (size_t)PY * PC;
+  static constexpr size_t SMEM_C = sizeof(float2) * (S2_PLANE + N + (size_t)TEAMS_LC * LP);
 };
 
 // S1 elements per evaluation of box n (slabs padded to the z pass's tiles).
 inline size_t s1_eval_elems(int n) {
   return n == 64 ? SearchCfg<64>::S1_EVAL : n == 96 ? SearchCfg<96>::S1_EVAL : SearchCfg<128>::S1_EVAL;
 }
-
-// Line li of a strided-FFT round handled by team `team`: consecutive teams get kx values 8
-// apart (NH is odd, so kx -> 8 kx mod NH is a permutation), which puts the teams of a warp on
-// different shared-memory banks.
-template <int NH>
-__device__ __forceinline__ int spread_kx(int li) {
-  return (li * 8) % NH;
-}
-
-// Column of line li of a strided-FFT round over `cols` columns of a tile whose row pitch is 1 (mod
-// 16) float2 (pass C's y transforms), for teams of 8 lanes: the two teams of a half-warp (lines 2p,
-// 2p+1) get columns 8 apart, so their accesses (8 lanes each on 8 consecutive banks of the line's
-// rows) fall on complementary bank halves in every Stockham stage.  Columns past the last complete
-// block of 16 keep their own index.  (8 li mod cols put some half-warp pairs 7 or 9 banks apart.)
-__device__ __forceinline__ int pair_spread(int li, int cols) {
-  const int full = (cols >> 4) << 4;
-  if (li >= full) return li;
-  const int p = li >> 1;
-  return ((p >> 3) << 4) + (p & 7) + ((li & 1) << 3);
+// S2 elements per output plane of box n (pass C's tile layout).
+inline size_t s2_plane_elems(int n) {
+  return n == 64 ? SearchCfg<64>::S2_PLANE : n == 96 ? SearchCfg<96>::S2_PLANE : SearchCfg<128>::S2_PLANE;
 }
 
 template <typename Tv>
@@ -753,12 +743,12 @@ __device__ __forceinline__ void z_mul_bulk(const SearchChunkArgs& a, const float
       if (threadIdx.x == 0) atomicAdd(&a.stats[e].energy_spec, t);
     }
     __syncthreads();
-    float2* dst = a.s2 + (size_t)e * w * ZS + (size_t)ky * NH + k0;
+    float2* dst = a.s2 + (size_t)e * w * C::S2_PLANE + (size_t)lpos<1>(ky) * C::PC + k0;
     for (int i = threadIdx.x; i < w * NB; i += NT) {
       const int j = i / NB, c = i % NB;
       if (c >= cnt) continue;
       const int z = (j - a.radius + N) % N;
-      dst[(size_t)j * ZS + c] = tile[lpos<1>(z) * TP + c];
+      dst[(size_t)j * C::S2_PLANE + c] = tile[lpos<1>(z) * TP + c];
     }
     return true;
   };
@@ -789,11 +779,15 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC, SearchCfg<N>::MINB_C) k_s
                                                                           const float2* __restrict__ g_tw) {
   using C = SearchCfg<N>;
   constexpr int NH = C::NH, P = C::P;
+  constexpr int PC = C::PC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* tile = reinterpret_cast<float2*>(smem_raw);   // [PY][NH], row y at lpos<1>(y)
-  float2* s_tw = tile + (size_t)C::PY * NH;
+  float2* tile = reinterpret_cast<float2*>(smem_raw);   // [PY][PC], row y at lpos<1>(y)
+  float2* s_tw = tile + C::S2_PLANE;
   float2* lines = s_tw + N;                              // [TEAMS][LP]
   __shared__ unsigned long long s_best;
+  __shared__ uint64_t bar;
+  constexpr unsigned PLANE_BYTES = (unsigned)(sizeof(float2) * C::S2_PLANE);
+  static_assert(PLANE_BYTES % 16 == 0, "bulk copy size");
 
   const int e = blockIdx.y;
   if (e >= a.n_items) return;
@@ -806,36 +800,28 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC, SearchCfg<N>::MINB_C) k_s
   // DC-free real-space energy of the rotated, masked reference (pass A, by Parseval)
   const bool weighted = a.refs[pt.ref].wref != nullptr || pt.wedge != nullptr;
 
-  load_twiddles<N>(s_tw, g_tw);
-  if (threadIdx.x == 0) s_best = 0ull;
-  const float2* src = a.s2 + ((size_t)e * w + j) * N * NH;
-  {
-    // the slab in groups of at most 16 loads in flight per thread
-    constexpr int IT = (N * NH + C::NT_BC - 1) / C::NT_BC;
-    constexpr int KB = IT < 16 ? IT : 16;
-#pragma unroll 1
-    for (int k0 = 0; k0 < IT; k0 += KB) {
-      float2 v[KB];
-#pragma unroll
-      for (int k = 0; k < KB; ++k) {
-        const int i = threadIdx.x + (k0 + k) * C::NT_BC;
-        if (i < N * NH) v[k] = src[i];
-      }
-#pragma unroll
-      for (int k = 0; k < KB; ++k) {
-        const int i = threadIdx.x + (k0 + k) * C::NT_BC;
-        if (i < N * NH) tile[lpos<1>(i / NH) * NH + i % NH] = v[k];
-      }
-    }
+  // the plane (pass B wrote it in this tile's layout) with one bulk copy, on a bounded wait
+  if (threadIdx.x == 0) {
+    s_best = 0ull;
+    mbar_init(&bar, 1);
+    mbar_arrive_expect_tx(&bar, PLANE_BYTES + a.phantom_tx);
+    bulk_copy_g2s(tile, a.s2 + ((size_t)e * w + j) * C::S2_PLANE, PLANE_BYTES, &bar);
   }
-  __syncthreads();
+  load_twiddles<N>(s_tw, g_tw);
+  __syncthreads();  // the barrier is initialised before anyone polls it
+  const bool arrived = mbar_wait(&bar, 0, a.wait_cycles);
+  if (__syncthreads_or(!arrived)) {
+    // the copy did not complete in time: report, give it a second bounded wait, and leave
+    if (threadIdx.x == 0 && a.status) atomicOr(a.status, kStatusWaitTimeout);
+    mbar_wait(&bar, 0, a.wait_cycles);
+    return;
+  }
   const int team = threadIdx.x / P, lane = threadIdx.x % P;
   LineTw<N, P> tc;
   tc.init(s_tw, lane);
   for (int base = 0; base < NH; base += C::TEAMS_BC) {
-    const int li = base + team;
-    const int kx = li < NH ? (P == 8 ? pair_spread(li, NH) : spread_kx<NH>(li)) : 0;
-    fft_line<N, 1, P, 1>(tile + kx, NH, lane, s_tw, li < NH, &tc);
+    const int li = base + team;  // consecutive columns for the teams of a warp
+    fft_line<N, 1, P, 1>(tile + (li < NH ? li : 0), PC, lane, s_tw, li < NH, &tc);
   }
   __syncthreads();
 
@@ -855,8 +841,8 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC, SearchCfg<N>::MINB_C) k_s
     const int ja = 2 * pr, jb = 2 * pr + 1;
     const bool has_b = jb < w;
     const int ya = (ja - r + N) % N, yb = has_b ? (jb - r + N) % N : ya;
-    const float2* ra = tile + (size_t)lpos<1>(ya) * NH;
-    const float2* rb = tile + (size_t)lpos<1>(yb) * NH;
+    const float2* ra = tile + (size_t)lpos<1>(ya) * PC;
+    const float2* rb = tile + (size_t)lpos<1>(yb) * PC;
     // Hermitian extension of rows a and b packed as a + i b
     fft_line_in<N, 1, P, 1>(
         [&](int n) {

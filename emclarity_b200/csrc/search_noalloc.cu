@@ -193,7 +193,7 @@ emc_status emc_search_plain_noalloc(const float* d_ref, const float* d_mask, int
                 "emc_search_plain_noalloc: peak radius %d not in [1, %d]", peak_radius, EMC_NOALLOC_MAX_RADIUS);
   EMC_CHECK_ARG(interp >= 0 && interp <= 2, "emc_search_plain_noalloc: interp %d", interp);
   EMC_CHECK_ARG(energy > 0.0, "emc_search_plain_noalloc: energy must be > 0");
-  const size_t per_eval = sizeof(float2) * (s1_eval_elems(n) + (size_t)(n / 2 + 1) * n * (2 * peak_radius + 1));
+  const size_t per_eval = sizeof(float2) * (s1_eval_elems(n) + s2_plane_elems(n) * (2 * peak_radius + 1));
   const size_t avail = EMC_NOALLOC_SCRATCH_BYTES - kSpecOff;
   const int chunk = (int)std::min<size_t>(kMaxChunk, avail / per_eval);
   EMC_CHECK_ARG(chunk >= 1, "emc_search_plain_noalloc: box %d with radius %d needs %zu B of scratch per "
