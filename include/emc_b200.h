@@ -323,7 +323,7 @@ EMC_API emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* 
                                emc_search_hit* h_best, void* stream);
 /* No counterpart in the reference.  Synchronises `stream` and reports whether a device-side wait of
  * the handle's runs since the last check gave up (EMC_E_TIMEOUT; the results of those runs are
- * invalid), clearing the report.  The waits (for the bulk copies of the 64^3 and 96^3 z pass) are bounded
+ * invalid), clearing the report.  The waits (for the bulk copies of the z and peak passes) are bounded
  * at about a second, after which the CTA leaves without a result; the context stays usable. */
 EMC_API emc_status emc_search_status(emc_search_t s, void* stream);
 /* Test hook (no counterpart in the reference): waits of later runs give up after wait_cycles SM
