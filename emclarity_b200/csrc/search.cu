@@ -756,8 +756,16 @@ static emc_status search_run(emc_search_t s, const emc_particle_desc* particles,
       if (!cnt) continue;
       const int r = effective_radius(s, n);
       const size_t pe = emc::per_eval_scratch(n, r);
-      int e = s->chunk_evals > 0 ? s->chunk_evals : (int)std::max<size_t>(1, s->scratch_budget / pe);
+      const bool auto_size = s->chunk_evals <= 0;
+      int e = auto_size ? (int)std::max<size_t>(1, s->scratch_budget / pe) : s->chunk_evals;
       e = (int)std::min<long>(e, 65535);
+      if (auto_size) {
+        // chunks of equal size (520 + 20 evaluations left the second overlap slot idle), and at least
+        // two at 64^3, whose chunks overlap in pairs
+        long k = (cnt + e - 1) / e;
+        if (n <= 64 && s->overlap > 1 && cnt >= 64) k = std::max(k, 2L);
+        e = (int)((cnt + k - 1) / k);
+      }
       for (long off = 0; off < cnt; off += e) {
         Chunk c{n, dt, begin + off, (int)std::min<long>(e, cnt - off)};
         chunks.push_back(c);

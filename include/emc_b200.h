@@ -294,8 +294,9 @@ EMC_API emc_status emc_search_add_reference(emc_search_t s, const float* d_ref, 
 EMC_API emc_status emc_search_set_orientations(emc_search_t s, const double* phi_theta_psi, int n);
 /* Tuning knobs (0 = automatic / autotuned).  peak_radius: spherical peak mask radius in
  * voxels (the peakMask >= 0.95 region of BH_multi_xcf_Translational.m:34).  chunk_evals:
- * evaluations per launch of the three passes; 0 sizes chunks to 768 MiB of scratch (about 600
- * evaluations at 64^3), or an eighth of the free device memory at creation if less. */
+ * evaluations per launch of the three passes; 0 cuts each box's evaluations into equal chunks of
+ * at most 768 MiB of scratch (about 520 evaluations at 64^3), or an eighth of the free device
+ * memory at creation if less, and into at least two at 64^3 (whose chunks overlap in pairs). */
 EMC_API emc_status emc_search_configure(emc_search_t s, int peak_radius, int interp, int chunk_evals);
 /* Runs every (particle, orientation) pair.  d_cc / d_peak (optional, may be NULL):
  * per-pair outputs in pair order (particle-major, orientations in list order),
