@@ -339,6 +339,11 @@ struct emc_search_s {
   // device status word of bounded waits (emc::kStatusWaitTimeout), read and cleared by
   // emc_search_status and emc_search_run_host; the wait limit and the test hook's phantom bytes
   emc::DevBuf<unsigned> d_status;
+  // device outputs of emc_search_run_host, kept between calls (grown on demand) so that a repeated
+  // request replays its recorded graph
+  emc::DevBuf<float> host_cc;
+  emc::DevBuf<int> host_peak;
+  emc::DevBuf<emc_search_hit> host_best;
   long long wait_cycles = 1ll << 31;
   unsigned phantom_tx = 0;
   // Per-evaluation scratch of a chunk, one set per overlap slot: chunk i of a recorded run uses slot
@@ -904,14 +909,15 @@ emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particle
   cudaStream_t st = emc::as_stream(stream);
   long total = 0;
   for (int p = 0; p < np; ++p) total += particles[p].orient_count;
-  float* d_cc = nullptr;
-  int* d_peak = nullptr;
-  emc_search_hit* d_best = nullptr;
+  // the handle's output buffers: the stream's earlier work on them ended with the previous call's
+  // synchronisation, so growing them here frees nothing in use
   emc_status rs = EMC_OK;
-  if (h_cc && cudaMalloc(&d_cc, sizeof(float) * std::max<long>(total, 1)) != cudaSuccess) rs = EMC_E_OOM;
-  if (rs == EMC_OK && h_peak && cudaMalloc(&d_peak, sizeof(int) * 3 * std::max<long>(total, 1)) != cudaSuccess)
-    rs = EMC_E_OOM;
-  if (rs == EMC_OK && h_best && cudaMalloc(&d_best, sizeof(emc_search_hit) * np) != cudaSuccess) rs = EMC_E_OOM;
+  if (h_cc) rs = s->host_cc.reserve((size_t)std::max<long>(total, 1));
+  if (rs == EMC_OK && h_peak) rs = s->host_peak.reserve(3 * (size_t)std::max<long>(total, 1));
+  if (rs == EMC_OK && h_best) rs = s->host_best.reserve((size_t)np);
+  float* d_cc = h_cc ? s->host_cc.p : nullptr;
+  int* d_peak = h_peak ? s->host_peak.p : nullptr;
+  emc_search_hit* d_best = h_best ? s->host_best.p : nullptr;
   if (rs == EMC_OK) rs = emc_search_run(s, particles, np, d_cc, d_peak, d_best, stream);
   if (rs == EMC_OK && h_cc && cudaMemcpyAsync(h_cc, d_cc, sizeof(float) * total, cudaMemcpyDeviceToHost, st))
     rs = EMC_E_CUDA;
@@ -925,11 +931,6 @@ emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particle
   if (rs == EMC_E_OOM) emc::set_error("emc_search_run_host: device allocation failed");
   if (rs == EMC_E_CUDA) emc::set_error("emc_search_run_host: copy back failed");
   if (rs == EMC_OK) rs = take_status(s);
-  cudaFree(d_cc);
-  cudaFree(d_peak);
-  cudaFree(d_best);
-  // the graph was recorded with these temporary outputs: do not replay it
-  drop_graphs(s);
   return rs;
 }
 
@@ -1032,6 +1033,10 @@ emc_status emc_search_destroy(emc_search_t s) {
   s->d_dmat.release();
   s->d_results.release();
   s->d_best_keys.release();
+  s->d_status.release();
+  s->host_cc.release();
+  s->host_peak.release();
+  s->host_best.release();
   for (auto& sc : s->slot) sc.release();
   if (s->branch) cudaStreamDestroy(s->branch);
   if (s->fork_ev) cudaEventDestroy(s->fork_ev);

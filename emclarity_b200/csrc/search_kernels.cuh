@@ -357,7 +357,7 @@ __device__ __forceinline__ void gather_cells(const CellT<T>* __restrict__ cells,
                                              float ty, float tz, int z0, float* __restrict__ fplanes, double& s1,
                                              double& s2) {
   using C = SearchCfg<N, GG>;
-  constexpr int G = C::G, NT = C::NT_A, NH = C::NH;
+  constexpr int G = C::G, NT = C::NT_A;
   constexpr int SEG = N / 32;                     // row segments per lane
   constexpr int RU = SEG >= 3 ? 2 : 4 / SEG;      // rows per warp per step: U = RU * SEG loads in flight
   // (two rows at 96^3 / 128^3: 6 / 8 cells in flight; 128^3 pass A 149 us per 9 evaluations from 156)
