@@ -317,8 +317,10 @@ EMC_API emc_status emc_search_run(emc_search_t s, const emc_particle_desc* parti
 EMC_API emc_status emc_search_run_energies(emc_search_t s, const emc_particle_desc* particles,
                                    int n_particles, const double* d_energy, float* d_cc,
                                    int* d_peak, emc_search_hit* d_best, void* stream);
-/* Same as emc_search_run with host output buffers (copies inside, synchronises).  Returns
- * EMC_E_TIMEOUT when a device-side wait of the run gave up (see emc_search_status). */
+/* Same as emc_search_run with host output buffers (copies inside, synchronises).  The device
+ * staging buffers stay in the handle between calls (grown on demand), so repeating a request
+ * replays its recorded graph.  Returns EMC_E_TIMEOUT when a device-side wait of the run gave up
+ * (see emc_search_status). */
 EMC_API emc_status emc_search_run_host(emc_search_t s, const emc_particle_desc* particles,
                                int n_particles, float* h_cc, int* h_peak,
                                emc_search_hit* h_best, void* stream);
