@@ -1130,14 +1130,14 @@ def run_refine(args, n_part=None):
 def run_extras(args):
     """Keys of the default line beside the headline: the batched uneven configuration (2,000 particles,
     60/30/10 over 64^3 / 96^3 / 128^3, 256 local orientations each) with FP32 and with BF16 reference
-    storage (one warm-up and two timed runs each), and a bounded pose refinement (200 x 96^3)."""
+    storage (three warm-up and two timed runs each), and a bounded pose refinement (200 x 96^3)."""
     import torch
 
     from emclarity_b200 import synthetic
     grid = synthetic.local_grid(N_ORIENT, 8.0, 2.0)
     sizes, refs, parts = mixed_batch(2000)
-    out = {"mixed": mixed_entry(sizes, parts, refs, "f32", 2, 1, grid, args.overlap),
-           "mixed_bf16": mixed_entry(sizes, parts, refs, "bf16", 2, 1, grid, args.overlap)}
+    out = {"mixed": mixed_entry(sizes, parts, refs, "f32", 2, 3, grid, args.overlap),
+           "mixed_bf16": mixed_entry(sizes, parts, refs, "bf16", 2, 3, grid, args.overlap)}
     del parts, refs
     torch.cuda.empty_cache()
     out["refine"] = run_refine(args, n_part=200)
