@@ -281,7 +281,9 @@ struct SearchCfg {
   static constexpr int MINB_A = N <= 64 ? (G == 1 ? 5 : 0) : (SMEM_CTAS_A < 2 ? SMEM_CTAS_A : 2);
   // Pass B: a CTA transforms the z lines of one ky and one of KS_B parts of the kx columns (NHB
   // columns at most).  128^3 splits the columns in two: with the whole ky row a CTA needed 544
-  // threads and 95 registers (one CTA per SM, latency-bound); half rows fit three per SM.
+  // threads and 95 registers (one CTA per SM, latency-bound); half rows fit three per SM.  At 96^3
+  // two parts (four CTAs per SM instead of two) took pass B from 494 to 448 us per chunk, but pass A's
+  // stores of the second part, which starts at an odd column, from 965 to 1035 us.
   // Pass A writes S1 as pass B's shared-memory tiles: per (evaluation, ky, column part) a slab of PY
   // rows (row z at lpos<1>(z)) of TPB_K float2, which pass B fetches with one bulk copy.  The
   // particle spectrum and weight rows (the caller's layout) come in 16-byte cp.async pieces from the
