@@ -301,7 +301,9 @@ struct SearchCfg {
   // evaluations per pass-B CTA (grid y = ceil(items / EVALS_B)): four at 64^3, where the later ones
   // reuse the particle's spectrum and weight rows (pass B 321.5 -> 309.9 us per 534-evaluation chunk
   // with two, 302.1 with four); at 96^3 a second evaluation's registers cost more than the reuse gave
-  // (502 -> 509 us)
+  // (502 -> 509 us).  A second slab tile, the next evaluation's slab copied while the current one is
+  // transformed (66 KB, three CTAs per SM), took pass B from 295.6 to 307.0 us and the overlapped
+  // 64^3 run from 620 to 679 ms: pass A of the other chunk no longer fits beside three such CTAs.
   static constexpr int EVALS_B = N <= 64 ? 4 : 1;
   static constexpr int TPB_K = NHB + 1 + (NHB + 1) % 2;                 // >= NHB + 1, even
   static constexpr int QP_K = TPB_K;
