@@ -298,13 +298,15 @@ struct SearchCfg {
   static constexpr int NT_B = ((NHB * P + 31) / 32) * 32;
   static constexpr int TEAMS_B = NT_B / P;
   static constexpr int GRID_BX = N * KS_B;
-  // evaluations per pass-B CTA (grid y = ceil(items / EVALS_B)): four at 64^3 and 96^3, where the
-  // later ones reuse the particle's spectrum and weight rows (64^3: pass B 321.5 -> 309.9 us per
-  // 534-evaluation chunk with two, 302.1 with four; 96^3, 69 registers, still two CTAs per SM: 493.4 ->
-  // 505.6 us per 167-evaluation chunk with two, 485.3 with four).  A second slab tile, the next evaluation's slab copied while the current one is
+  // evaluations per pass-B CTA (grid y = ceil(items / EVALS_B)): four at 64^3 and 96^3, two at
+  // 128^3, where the later ones reuse the particle's spectrum (and weight) rows (64^3: pass B 321.5 ->
+  // 309.9 us per 534-evaluation chunk with two, 302.1 with four; 96^3, 69 registers, still two CTAs
+  // per SM: 493.4 -> 505.6 us per 167-evaluation chunk with two, 485.3 with four; 128^3, 56
+  // registers, three CTAs per SM: 446.4 -> 432.6 us per 72-evaluation chunk with two, 436.6 with
+  // four).  A second slab tile, the next evaluation's slab copied while the current one is
   // transformed (66 KB, three CTAs per SM), took pass B from 295.6 to 307.0 us and the overlapped
   // 64^3 run from 620 to 679 ms: pass A of the other chunk no longer fits beside three such CTAs.
-  static constexpr int EVALS_B = N <= 96 ? 4 : 1;
+  static constexpr int EVALS_B = N <= 96 ? 4 : 2;
   static constexpr int TPB_K = NHB + 1 + (NHB + 1) % 2;                 // >= NHB + 1, even
   static constexpr int QP_K = TPB_K;
   static constexpr int WP_K = ((NHB + 3 + 3) / 4) * 4;                   // >= NHB + 3, 16-byte rows
