@@ -502,7 +502,9 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
     constexpr int NPAIRS = G * N / 2;
     const bool has_line = team < C::TEAMS_LA;
     float2* buf = lines + (size_t)(has_line ? team : 0) * LP;
-    for (int base = 0; base < NPAIRS; base += C::TEAMS_LA) {
+    static_assert((C::TEAMS_LA * P) % 32 == 0, "line-buffer teams fill whole warps");
+    // warps without line buffers (96^3, 128^3: the second half of the CTA) skip the loop
+    for (int base = 0; base < NPAIRS && threadIdx.x < C::TEAMS_LA * P; base += C::TEAMS_LA) {
       const int q = base + ((team & ~3) | ((team & 1) << 1) | ((team >> 1) & 1));  // pairs 0, 2, 1, 3
       const bool active = has_line && q < NPAIRS;
       // rows 2q, 2q+1 of the slab (same plane, adjacent padded rows since 2q+1 is odd)
@@ -557,7 +559,10 @@ __global__ void __launch_bounds__(SearchCfg<N, GG>::NT_A, SearchCfg<N, GG>::MINB
   // 3. FFT along y for columns 0 .. N/2-1 of every plane (column 0 carries X(0) + i X(N/2))
   {
     constexpr int NLINES = G * (N / 2);
+    static_assert(NLINES % (32 / P) == 0, "a warp's teams are all active or all idle");
     for (int base = 0; base < NLINES; base += C::TEAMS_A) {
+      // a warp whose teams all lie past the last line (96^3: the second round) skips the round
+      if (base + (int)(threadIdx.x >> 5) * (32 / P) >= NLINES) continue;
       const int li = base + team;
       const bool active = li < NLINES;
       const int zl = active ? li / (N / 2) : 0, kx = active ? li % (N / 2) : 0;
@@ -838,6 +843,8 @@ __global__ void __launch_bounds__(SearchCfg<N>::NT_BC, SearchCfg<N>::MINB_C) k_s
   constexpr int c = N / 2;
 
   unsigned long long best = 0ull;
+  // (warps with no row pair run the C2R loop predicated off; letting them skip it measured slower:
+  // 74.2 -> 76-78 us per 64^3 chunk, a 4-byte spill and the branch against idle issue slots)
   const int npairs = (w + 1) / 2;
   const bool has_line = team < C::TEAMS_LC;
   float2* buf = lines + (size_t)(has_line ? team : 0) * C::LP;
